@@ -1,0 +1,322 @@
+"""Host-side mirror of droplet's public API over the C ABI.
+
+Same names, argument meaning and error behaviour as the TypeScript entry
+points (src/index.ts:16-38):
+
+  createDevice(opts)                       src/gpu/device.ts:27-41
+  Renderer(device, opts).render(...)       src/render/pipeline.ts:50-592
+  voxelize(device, data, opts)             src/voxel/voxelize.ts:59-248
+  BlockMaskBuffer                          src/voxel/block-mask-buffer.ts:23-64
+
+Every call goes through libdroplet_b200.so; a non-zero status raises
+DropletError (the TypeScript shim throws Error the same way).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import DropletError, check
+from .types import BackgroundRGBA, Bounds, RenderCamera, SplatData
+
+
+def _splats(d: SplatData) -> _lib.DlSplats:
+    s = _lib.DlSplats()
+    s.count = d.count
+    p = lambda a: None if a is None or a.size == 0 else a.ctypes.data
+    s.positions, s.rotations, s.log_scales = p(d.positions), p(d.rotations), p(d.logScales)
+    s.opacity_logits, s.colors_dc, s.colors_sh = p(d.opacityLogits), p(d.colorsDC), p(d.colorsSH)
+    s.sh_bands = d.shBands
+    s._keep = d
+    return s
+
+
+def _camera(c: RenderCamera) -> _lib.DlCamera:
+    cs = _lib.DlCamera()
+    cs.width, cs.height = int(c.width), int(c.height)
+    ctypes.memmove(cs.view, np.ascontiguousarray(c.viewMatrix, np.float32).ctypes.data, 64)
+    cs.fov_y, cs.near_plane, cs.far_plane = float(c.fovY), float(c.near), float(c.far)
+    cs.projection = _lib.DL_PINHOLE if (c.projection or "pinhole") == "pinhole" else _lib.DL_EQUIRECT
+    return cs
+
+
+def _bg(bg) -> ctypes.Array:
+    if bg is None:
+        bg = BackgroundRGBA()
+    if isinstance(bg, BackgroundRGBA):
+        vals = (bg.r, bg.g, bg.b, bg.a)
+    elif isinstance(bg, dict):
+        vals = (bg["r"], bg["g"], bg["b"], bg["a"])
+    else:
+        vals = tuple(bg)
+    return (ctypes.c_float * 4)(*[float(v) for v in vals])
+
+
+class Device:
+    """Opaque handle standing in for GPUDevice (one CUDA device + stream)."""
+
+    def __init__(self, handle: int, ordinal: int):
+        self._h = handle
+        self.ordinal = ordinal
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise DropletError(_lib.DL_E_INVALID_ARG, "device is closed")
+        return self._h
+
+    def destroy(self):
+        if self._h:
+            _lib.load().dl_device_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def createDevice(opts: Optional[dict] = None) -> Device:
+    """device.ts:27-41.  opts: {"device": Device} passes an existing device
+    through; {"ordinal": k} picks a CUDA device.  Raises if none is usable."""
+    opts = opts or {}
+    if opts.get("device") is not None:
+        return opts["device"]
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    ordinal = int(opts.get("ordinal", 0))
+    check(L.dl_device_open(ordinal, ctypes.byref(h)))
+    return Device(h.value, ordinal)
+
+
+class Scene:
+    """A device-resident copy of a SplatData (no reference counterpart)."""
+
+    def __init__(self, renderer: "Renderer", handle: int, count: int):
+        self._r = renderer
+        self._h = handle
+        self.count = count
+
+    def destroy(self):
+        if self._h:
+            _lib.load().dl_scene_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """pipeline.ts:50-592.  opts: {chunkCap, maxCoveragePerSplat}."""
+
+    STAGES = ("project", "depth_sort", "emit", "tile_offsets", "pair_sort", "rasterize")
+
+    def __init__(self, device: Device, opts: Optional[dict] = None, **kw):
+        opts = dict(opts or {}, **kw)
+        o = _lib.DlRendererOpts(int(opts.get("chunkCap") or 0), int(opts.get("maxCoveragePerSplat") or 0))
+        h = ctypes.c_void_p()
+        check(_lib.load().dl_renderer_create(device.handle, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h.value
+        self.device = device
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise DropletError(_lib.DL_E_INVALID_ARG, "renderer is destroyed")
+        return self._h
+
+    def render(self, data: SplatData, camera: RenderCamera, background=None) -> np.ndarray:
+        """pipeline.ts:181-426 — returns a fresh uint8 array of width*height*4 (RGBA8)."""
+        out = np.empty(int(camera.width) * int(camera.height) * 4, np.uint8)
+        check(_lib.load().dl_render(self.handle, ctypes.byref(_splats(data)), ctypes.byref(_camera(camera)),
+                                    _bg(background), out.ctypes.data if out.size else None, out.size))
+        return out
+
+    # ---- device-resident scenes and batches
+    def upload(self, data: SplatData, precision: str = "f32") -> Scene:
+        prec = {"f32": _lib.DL_PREC_F32, "f16": _lib.DL_PREC_F16, "bf16": _lib.DL_PREC_BF16}[precision]
+        h = ctypes.c_void_p()
+        check(_lib.load().dl_scene_upload(self.handle, ctypes.byref(_splats(data)), prec, ctypes.byref(h)))
+        return Scene(self, h.value, data.count)
+
+    def render_batch(self, scene: Scene, cameras: Sequence[RenderCamera], background=None, flags: int = 0,
+                     outs: Optional[Sequence[int]] = None) -> Optional[List[np.ndarray]]:
+        """Render len(cameras) views.  With outs (device pointers) the images stay
+        on the device (flag DL_BATCH_OUT_DEVICE is added); otherwise returns a list
+        of uint8 arrays."""
+        n = len(cameras)
+        cams = (_lib.DlCamera * n)(*[_camera(c) for c in cameras])
+        ptrs = (ctypes.c_void_p * n)()
+        host = None
+        if outs is None:
+            host = [np.empty(int(c.width) * int(c.height) * 4, np.uint8) for c in cameras]
+            for k, a in enumerate(host):
+                ptrs[k] = a.ctypes.data
+        else:
+            flags |= _lib.DL_BATCH_OUT_DEVICE
+            for k, p in enumerate(outs):
+                ptrs[k] = int(p)
+        check(_lib.load().dl_render_batch(self.handle, scene._h, cams, n, _bg(background), ptrs, flags))
+        return host
+
+    # ---- instrumentation
+    def set_stream(self, stream_ptr: Optional[int]):
+        check(_lib.load().dl_renderer_set_stream(self.handle, stream_ptr))
+
+    def set_debug(self, on: bool = True):
+        check(_lib.load().dl_renderer_set_debug(self.handle, 1 if on else 0))
+
+    def set_profiling(self, on: bool = True):
+        check(_lib.load().dl_renderer_set_profiling(self.handle, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        ms = (ctypes.c_double * 6)()
+        check(_lib.load().dl_renderer_stage_times(self.handle, ms, 6))
+        return dict(zip(self.STAGES, list(ms)))
+
+    def launch_count(self) -> int:
+        c = ctypes.c_uint64()
+        check(_lib.load().dl_renderer_launch_count(self.handle, ctypes.byref(c)))
+        return int(c.value)
+
+    def debug_get(self, name: str, dtype) -> np.ndarray:
+        L = _lib.load()
+        n = ctypes.c_size_t()
+        check(L.dl_renderer_debug_get(self.handle, name.encode(), None, 0, ctypes.byref(n)))
+        out = np.empty(n.value // np.dtype(dtype).itemsize, dtype)
+        if n.value:
+            check(L.dl_renderer_debug_get(self.handle, name.encode(), out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
+    def destroy(self):
+        """pipeline.ts:581-591."""
+        if self._h:
+            _lib.load().dl_renderer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- voxelize
+@dataclass
+class VoxelBlock:
+    """block-mask-buffer.ts:14-21."""
+    blockIdx: int
+    maskLo: int
+    maskHi: int
+
+
+def _popcount32(a: np.ndarray) -> int:
+    """block-mask-buffer.ts:60-64 (SWAR popcount), summed over an array."""
+    v = a.astype(np.uint64)
+    v = v - ((v >> 1) & 0x55555555)
+    v = (v & 0x33333333) + ((v >> 2) & 0x33333333)
+    v = (((v + (v >> 4)) & 0x0F0F0F0F) * 0x01010101) & 0xFFFFFFFF
+    return int(np.sum(v >> 24))
+
+
+class BlockMaskBuffer:
+    """block-mask-buffer.ts:23-58: sparse 4x4x4-voxel blocks, 2 x u32 masks each,
+    in insertion order; the masks are kept as numpy columns."""
+
+    def __init__(self, blockIdx=None, maskLo=None, maskHi=None):
+        self.blockIdx = np.asarray(blockIdx if blockIdx is not None else [], np.uint32)
+        self.maskLo = np.asarray(maskLo if maskLo is not None else [], np.uint32)
+        self.maskHi = np.asarray(maskHi if maskHi is not None else [], np.uint32)
+        self._index = None
+
+    def _map(self):
+        if self._index is None:
+            self._index = {int(b): i for i, b in enumerate(self.blockIdx.tolist())}
+        return self._index
+
+    def addBlock(self, blockIdx: int, maskLo: int, maskHi: int) -> None:
+        if maskLo == 0 and maskHi == 0:
+            return
+        m = self._map()
+        i = m.get(int(blockIdx))
+        if i is None:
+            m[int(blockIdx)] = len(self.blockIdx)
+            self.blockIdx = np.append(self.blockIdx, np.uint32(blockIdx))
+            self.maskLo = np.append(self.maskLo, np.uint32(maskLo))
+            self.maskHi = np.append(self.maskHi, np.uint32(maskHi))
+        else:
+            self.maskLo[i] |= np.uint32(maskLo)
+            self.maskHi[i] |= np.uint32(maskHi)
+
+    def get(self, blockIdx: int) -> Optional[VoxelBlock]:
+        i = self._map().get(int(blockIdx))
+        if i is None:
+            return None
+        return VoxelBlock(int(self.blockIdx[i]), int(self.maskLo[i]), int(self.maskHi[i]))
+
+    @property
+    def blocks(self) -> List[VoxelBlock]:
+        return [VoxelBlock(int(b), int(lo), int(hi)) for b, lo, hi in zip(self.blockIdx, self.maskLo, self.maskHi)]
+
+    def popcount(self) -> int:
+        return _popcount32(self.maskLo) + _popcount32(self.maskHi)
+
+    @property
+    def count(self) -> int:
+        return int(self.blockIdx.size)
+
+
+@dataclass
+class VoxelizeResult:
+    """voxelize.ts:38-45."""
+    buffer: BlockMaskBuffer
+    bounds: Bounds
+    voxelResolution: float
+    numBlocksX: float
+    numBlocksY: float
+    numBlocksZ: float
+
+
+def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> VoxelizeResult:
+    """voxelize.ts:59-248.  opts: {voxelResolution=0.05, opacityCutoff=0.1, bounds}."""
+    opts = opts or {}
+    o = _lib.DlVoxOpts()
+    res = opts.get("voxelResolution")
+    cut = opts.get("opacityCutoff")
+    o.voxel_resolution = 0.05 if res is None else float(res)
+    o.opacity_cutoff = 0.1 if cut is None else float(cut)
+    o.use_defaults = 0
+    b = opts.get("bounds")
+    if b is not None:
+        bmin, bmax = (b.min, b.max) if isinstance(b, Bounds) else (b["min"], b["max"])
+        o.has_bounds = 1
+        for k in range(3):
+            o.bounds_min[k] = float(bmin[k])
+            o.bounds_max[k] = float(bmax[k])
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    check(L.dl_voxelize(device.handle, ctypes.byref(_splats(data)), ctypes.byref(o), ctypes.byref(h)))
+    try:
+        bmin = (ctypes.c_double * 3)()
+        bmax = (ctypes.c_double * 3)()
+        dims = (ctypes.c_double * 3)()
+        cnt = ctypes.c_uint64()
+        check(L.dl_vox_result_info(h, bmin, bmax, dims, ctypes.byref(cnt)))
+        n = int(cnt.value)
+        idx = np.empty(n, np.uint32)
+        lo = np.empty(n, np.uint32)
+        hi = np.empty(n, np.uint32)
+        if n:
+            check(L.dl_vox_result_copy(h, idx.ctypes.data, lo.ctypes.data, hi.ctypes.data))
+    finally:
+        L.dl_vox_result_free(h)
+    return VoxelizeResult(BlockMaskBuffer(idx, lo, hi), Bounds(tuple(bmin), tuple(bmax)),
+                          o.voxel_resolution, dims[0], dims[1], dims[2])

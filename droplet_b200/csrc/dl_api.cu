@@ -1,0 +1,243 @@
+// dl_api.cu — the C ABI (include/droplet_b200.h): devices, renderers, scenes,
+// status codes and the thread-local error message.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dl_internal.h"
+
+static thread_local std::string g_last_error;
+
+void dl_set_error(const std::string& msg) { g_last_error = msg; }
+
+extern "C" const char* dl_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------- device
+extern "C" int dl_device_open(int ordinal, dl_device** out) {
+    if (!out) { dl_set_error("dl_device_open: out is NULL"); return DL_E_INVALID_ARG; }
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        dl_set_error("no CUDA device available");
+        return DL_E_NO_DEVICE;
+    }
+    if (ordinal < 0 || ordinal >= count) { dl_set_error("device ordinal out of range"); return DL_E_INVALID_ARG; }
+    DL_CK(cudaSetDevice(ordinal));
+    cudaDeviceProp prop;
+    DL_CK(cudaGetDeviceProperties(&prop, ordinal));
+    if (prop.major < 10) {
+        dl_set_error(std::string("device ") + prop.name + " is not sm_100 (B200); this library is built for sm_100a only");
+        return DL_E_NO_DEVICE;
+    }
+    dl_device* d = new dl_device();
+    d->ordinal = ordinal;
+    d->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete d;
+        dl_set_error("cudaStreamCreate failed");
+        return DL_E_CUDA;
+    }
+    *out = d;
+    return DL_OK;
+}
+
+extern "C" int dl_device_close(dl_device* d) {
+    if (!d) return DL_OK;
+    cudaSetDevice(d->ordinal);
+    if (d->stream) cudaStreamDestroy(d->stream);
+    delete d;
+    return DL_OK;
+}
+
+// ---------------------------------------------------------------- renderer
+extern "C" int dl_renderer_create(dl_device* dev, const dl_renderer_opts* opts, dl_renderer** out) {
+    if (!dev || !out) { dl_set_error("dl_renderer_create: NULL argument"); return DL_E_INVALID_ARG; }
+    DL_CK(cudaSetDevice(dev->ordinal));
+    dl_renderer* r = new dl_renderer();
+    r->dev = dev;
+    // src/render/pipeline.ts:76-81 defaults
+    r->chunk_cap = (opts && opts->chunk_cap) ? opts->chunk_cap : 200000u;
+    r->max_cov = (opts && opts->max_coverage_per_splat) ? opts->max_coverage_per_splat : 16384u;
+    r->stream = dev->stream;
+    r->own_scene.dev = dev;
+    for (auto& e : r->ev) cudaEventCreate(&e);
+    *out = r;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_destroy(dl_renderer* r) {
+    if (!r) return DL_OK;
+    cudaSetDevice(r->dev->ordinal);
+    cudaStreamSynchronize(r->stream);
+    DevBuf* bufs[] = {&r->views, &r->segStart, &r->segLen, &r->segTileBase, &r->scratch, &r->keys0, &r->keys1,
+                      &r->vals0, &r->vals1, &r->recA, &r->recBC, &r->recH, &r->bbox, &r->nvis, &r->depthHist,
+                      &r->sortStatus, &r->pairBase, &r->pairCap, &r->pkeys0, &r->pkeys1, &r->pvals0, &r->pvals1,
+                      &r->npairs, &r->emitStatus, &r->tileCount, &r->tileOff, &r->pairSegLen, &r->pairSegTileBase,
+                      &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->own_scene.mem};
+    for (DevBuf* b : bufs) b->release();
+    if (r->h_views) cudaFreeHost(r->h_views);
+    if (r->h_u64) cudaFreeHost(r->h_u64);
+    for (auto& e : r->ev) if (e) cudaEventDestroy(e);
+    delete r;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_set_stream(dl_renderer* r, void* s) {
+    if (!r) { dl_set_error("renderer is NULL"); return DL_E_INVALID_ARG; }
+    r->stream = s ? (cudaStream_t)s : r->dev->stream;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_set_profiling(dl_renderer* r, int on) {
+    if (!r) { dl_set_error("renderer is NULL"); return DL_E_INVALID_ARG; }
+    r->profiling = on != 0;
+    for (double& m : r->stage_ms) m = 0.0;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_stage_times(dl_renderer* r, double* ms, int n) {
+    if (!r || !ms) { dl_set_error("NULL argument"); return DL_E_INVALID_ARG; }
+    for (int i = 0; i < n && i < 6; i++) ms[i] = r->stage_ms[i];
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_launch_count(dl_renderer* r, uint64_t* count) {
+    if (!r || !count) { dl_set_error("NULL argument"); return DL_E_INVALID_ARG; }
+    *count = r->launches;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_set_debug(dl_renderer* r, int keep_intermediates) {
+    if (!r) { dl_set_error("renderer is NULL"); return DL_E_INVALID_ARG; }
+    r->keep_accum = keep_intermediates != 0;
+    return DL_OK;
+}
+
+static int check_camera(const dl_camera* cam) {
+    if (!cam) { dl_set_error("camera is NULL"); return DL_E_INVALID_ARG; }
+    return DL_OK;
+}
+
+// src/render/pipeline.ts:181-426 + composite :428-473
+extern "C" int dl_render(dl_renderer* r, const dl_splats* data, const dl_camera* cam, const float bg[4],
+                         uint8_t* out_rgba, size_t out_len) {
+    if (!r || !data) { dl_set_error("dl_render: NULL argument"); return DL_E_INVALID_ARG; }
+    DL_TRY(check_camera(cam));
+    const uint64_t pixels = (uint64_t)cam->width * cam->height;
+    if (pixels == 0) return DL_OK;
+    if (!out_rgba || out_len < pixels * 4) { dl_set_error("dl_render: output buffer smaller than width*height*4"); return DL_E_INVALID_ARG; }
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    DlView v;
+    DL_TRY(dl_make_view(cam, bg, r->max_cov, &v));
+    DL_TRY(dl_upload_scene(&r->own_scene, data, DL_PREC_F32, r->stream));
+    DL_TRY(r->rgba.ensure(pixels * 4));
+    uint32_t* outs[1] = {r->rgba.as<uint32_t>()};
+    DL_TRY(dl_render_views(r, r->own_scene.d, &v, 1, outs, 0));
+    DL_CK(cudaMemcpyAsync(out_rgba, r->rgba.p, pixels * 4, cudaMemcpyDeviceToHost, r->stream));
+    DL_CK(cudaStreamSynchronize(r->stream));
+    return DL_OK;
+}
+
+extern "C" int dl_scene_upload(dl_renderer* r, const dl_splats* data, int precision, dl_scene** out) {
+    if (!r || !data || !out) { dl_set_error("dl_scene_upload: NULL argument"); return DL_E_INVALID_ARG; }
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    dl_scene* s = new dl_scene();
+    s->dev = r->dev;
+    const int st = dl_upload_scene(s, data, precision, r->stream);
+    if (st != DL_OK) { s->mem.release(); delete s; return st; }
+    if (cudaStreamSynchronize(r->stream) != cudaSuccess) {
+        s->mem.release();
+        delete s;
+        dl_set_error("scene upload failed");
+        return DL_E_CUDA;
+    }
+    *out = s;
+    return DL_OK;
+}
+
+extern "C" int dl_scene_free(dl_scene* s) {
+    if (!s) return DL_OK;
+    cudaSetDevice(s->dev->ordinal);
+    s->mem.release();
+    delete s;
+    return DL_OK;
+}
+
+extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
+                               uint8_t* const* outs, uint32_t flags) {
+    if (!r || !s || !cams || !outs || n < 0) { dl_set_error("dl_render_batch: bad argument"); return DL_E_INVALID_ARG; }
+    if (n == 0) return DL_OK;
+    if (n > 4096) { dl_set_error("at most 4096 views per batch"); return DL_E_CAPACITY; }
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    std::vector<DlView> views((size_t)n);
+    uint64_t totalPix = 0;
+    for (int i = 0; i < n; i++) {
+        DL_TRY(dl_make_view(&cams[i], bg, r->max_cov, &views[i]));
+        if (!outs[i]) { dl_set_error("dl_render_batch: NULL output"); return DL_E_INVALID_ARG; }
+        totalPix += (uint64_t)views[i].W * views[i].H;
+    }
+    const bool outDev = (flags & DL_BATCH_OUT_DEVICE) != 0;
+    std::vector<uint32_t*> dOuts((size_t)n);
+    if (outDev) {
+        for (int i = 0; i < n; i++) dOuts[i] = (uint32_t*)outs[i];
+    } else {
+        DL_TRY(r->rgba.ensure(totalPix * 4));
+        uint64_t off = 0;
+        for (int i = 0; i < n; i++) { dOuts[i] = r->rgba.as<uint32_t>() + off; off += (uint64_t)views[i].W * views[i].H; }
+    }
+    uint64_t launches = 0;
+    if (flags & DL_BATCH_PLAIN) {
+        for (int i = 0; i < n; i++) {
+            if ((uint64_t)views[i].W * views[i].H == 0) continue;
+            DL_TRY(dl_render_views(r, s->d, &views[i], 1, &dOuts[i], flags & ~DL_BATCH_F16_RECORDS));
+            launches += r->launches;
+        }
+    } else {
+        DL_TRY(dl_render_views(r, s->d, views.data(), (uint32_t)n, dOuts.data(), flags));
+        launches = r->launches;
+    }
+    r->launches = launches;
+    if (!outDev) {
+        for (int i = 0; i < n; i++)
+            DL_CK(cudaMemcpyAsync(outs[i], dOuts[i], (uint64_t)views[i].W * views[i].H * 4, cudaMemcpyDeviceToHost, r->stream));
+    }
+    DL_CK(cudaStreamSynchronize(r->stream));
+    return DL_OK;
+}
+
+// ---------------------------------------------------------------- debug copies
+extern "C" int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst, size_t cap, size_t* bytes) {
+    if (!r || !name) { dl_set_error("NULL argument"); return DL_E_INVALID_ARG; }
+    const std::string s(name);
+    const void* src = nullptr;
+    size_t n = 0;
+    uint64_t scalar = 0;
+    bool host = false;
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    if (s == "nvis" || s == "npairs") {
+        if (s == "nvis") {
+            uint32_t v = 0;
+            DL_CK(cudaMemcpy(&v, r->nvis.p, 4, cudaMemcpyDeviceToHost));
+            scalar = v;
+        } else {
+            DL_CK(cudaMemcpy(&scalar, r->npairs.p, 8, cudaMemcpyDeviceToHost));
+        }
+        src = &scalar; n = 8; host = true;
+    } else if (s == "depth_keys") { src = r->keys0.p; n = 4ull * r->last_n; }
+    else if (s == "sorted_idx") { src = r->vals0.p; n = 4ull * r->last_n; }
+    else if (s == "recA") { src = r->recA.p; n = 16ull * r->last_n; }
+    else if (s == "recBC") { src = r->recBC.p; n = 32ull * r->last_n; }
+    else if (s == "recH") { src = r->recH.p; n = 16ull * r->last_n; }
+    else if (s == "bbox") { src = r->bbox.p; n = 8ull * r->last_n; }
+    else if (s == "tile_off") { src = r->tileOff.p; n = 4ull * (r->last_T + 1); }
+    else if (s == "pair_vals") { src = r->last_final_vals; n = 4ull * r->last_pairs_final; }
+    else if (s == "accum") { src = r->keep_accum ? r->accum.p : nullptr; n = src ? 16ull * r->last_W * r->last_H : 0; }
+    else { dl_set_error("unknown debug array: " + s); return DL_E_INVALID_ARG; }
+    if (bytes) *bytes = n;
+    if (!dst || n == 0) return DL_OK;
+    if (cap < n) { dl_set_error("debug_get: destination too small"); return DL_E_INVALID_ARG; }
+    if (host) std::memcpy(dst, src, n);
+    else DL_CK(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+    return DL_OK;
+}

@@ -1,0 +1,106 @@
+// dl_internal.h — host-side internals shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/droplet_b200.h"
+#include "dl_common.cuh"
+
+void dl_set_error(const std::string& msg);
+
+#define DL_CK(call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            dl_set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                \
+            return e_ == cudaErrorMemoryAllocation ? DL_E_OOM : DL_E_CUDA;                   \
+        }                                                                                    \
+    } while (0)
+
+#define DL_TRY(expr)                  \
+    do {                              \
+        int s_ = (expr);              \
+        if (s_ != DL_OK) return s_;   \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need) {
+        if (need <= bytes && p) return DL_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t alloc = need < 256 ? 256 : need;
+        cudaError_t e = cudaMalloc(&p, alloc);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            dl_set_error(std::string("cudaMalloc(") + std::to_string(alloc) + "): " + cudaGetErrorString(e));
+            return DL_E_OOM;
+        }
+        bytes = alloc;
+        return DL_OK;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct dl_device {
+    int ordinal = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+};
+
+struct dl_scene {
+    dl_device* dev = nullptr;
+    DevBuf mem;
+    DlSceneDev d{};
+    int precision = DL_PREC_F32;
+};
+
+// Host-side state of the tile-binned renderer.
+struct dl_renderer {
+    dl_device* dev = nullptr;
+    uint32_t chunk_cap = 200000;
+    uint32_t max_cov = 16384;
+    cudaStream_t stream = nullptr;      // effective stream
+    cudaStream_t own_stream = nullptr;
+
+    // frame buffers (grow-only)
+    DevBuf views, segStart, segLen, segTileBase, scratch;     // scratch: counters + error word
+    DevBuf keys0, keys1, vals0, vals1, recA, recBC, recH, bbox, nvis;
+    DevBuf depthHist, sortStatus;
+    DevBuf pairBase, pairCap, pkeys0, pkeys1, pvals0, pvals1, npairs, emitStatus;
+    DevBuf tileCount, tileOff, pairSegLen, pairSegTileBase, pairGlob, outs, accum, tileEvals, work;
+    dl_scene own_scene;                 // upload target of dl_render()
+
+    // host mirrors
+    DlView* h_views = nullptr;          // pinned
+    size_t h_views_cap = 0;
+    uint64_t* h_u64 = nullptr;          // pinned scratch
+    size_t h_u64_cap = 0;
+    uint64_t pair_cap_per_view = 0;
+
+    // last frame (single view) for debug copies
+    uint32_t last_n = 0, last_stride = 0, last_T = 0, last_W = 0, last_H = 0, last_pairs_final = 0;
+    int last_rec_kind = 0;
+    uint32_t* last_final_vals = nullptr;
+    DevBuf rgba;                        // device output of dl_render()
+    bool keep_accum = false;
+    bool keep_depth_keys = true;
+
+    // profiling
+    bool profiling = false;
+    cudaEvent_t ev[8] = {};
+    double stage_ms[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t launches = 0;
+};
+
+// dl_render.cu
+int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hviews, uint32_t V,
+                    uint32_t* const* d_outs, uint32_t flags);
+int dl_upload_scene(dl_scene* s, const dl_splats* data, int precision, cudaStream_t stream);
+int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlView* out);

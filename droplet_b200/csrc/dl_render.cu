@@ -1,0 +1,433 @@
+// dl_render.cu — host orchestration of the renderer's device pipeline.
+//
+// One frame (any number of views of one device-resident scene):
+//   project_k -> depth sort (4 onesweep passes) -> emit_k -> tile_offsets_k
+//   -> pair sort (1-3 onesweep passes) -> rasterize_k
+// No host synchronisation happens inside the frame: every size a later stage
+// needs (visible count, pair count, tile offsets) stays in device memory.
+// Pair buffers are sized from an upper bound; if a frame overflows them the
+// emit kernel flags it, the host grows the buffers and re-runs the pair stages.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "dl_internal.h"
+#include "dl_render_kernels.cuh"
+#include "dl_sort.cuh"
+
+namespace {
+
+constexpr int kScratchWords = 32;
+enum {
+    SC_DEPTH_CTR = 0,      // 4 counters
+    SC_EMIT_CTR = 4,
+    SC_PAIR_CTR = 5,       // 4 counters
+    SC_WORK_CTR = 9,
+    SC_ERR = 10,
+    SC_DEPTH_TILES = 11,
+    SC_PAIR_TILES = 12,
+    SC_OVF = 13
+};
+
+inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+int ensure_pinned(void** p, size_t* cap, size_t need) {
+    if (need <= *cap && *p) return DL_OK;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (cudaMallocHost(p, need) != cudaSuccess) {
+        *p = nullptr;
+        dl_set_error("cudaMallocHost failed");
+        return DL_E_OOM;
+    }
+    *cap = need;
+    return DL_OK;
+}
+
+template <int BITS>
+void launch_pass(const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
+    dlsort::pass_k<BITS><<<grid, dlsort::kThreads, 0, st>>>(p);
+}
+
+void launch_pass_bits(int bits, const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
+    if (bits == 8) launch_pass<8>(p, grid, st);
+    else if (bits == 7) launch_pass<7>(p, grid, st);
+    else launch_pass<6>(p, grid, st);
+}
+
+__global__ void sh_to_half_k(const float* in, uint16_t* out, uint64_t n, int kind) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float f = in[i];
+        out[i] = kind == 1 ? __half_as_ushort(__float2half_rn(f)) : __bfloat16_as_ushort(__float2bfloat16_rn(f));
+    }
+}
+
+void ev_record(dl_renderer* r, int i) {
+    if (r->profiling) cudaEventRecord(r->ev[i], r->stream);
+}
+
+}  // namespace
+
+int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlView* v) {
+    if (!cam) { dl_set_error("camera is NULL"); return DL_E_INVALID_ARG; }
+    if (cam->projection != DL_PINHOLE && cam->projection != DL_EQUIRECT) {
+        dl_set_error("camera.projection must be DL_PINHOLE or DL_EQUIRECT");
+        return DL_E_INVALID_ARG;
+    }
+    std::memset(v, 0, sizeof(*v));
+    std::memcpy(v->view, cam->view, sizeof(v->view));
+    // src/render/camera.ts:32-46 in f64, stored into the f32 uniform (pipeline.ts:490-497)
+    const double focal = (double)cam->height / (2.0 * std::tan(cam->fov_y / 2.0));
+    v->width = (float)cam->width;
+    v->height = (float)cam->height;
+    v->focal = (float)focal;
+    v->cx = (float)((double)cam->width / 2.0);
+    v->cy = (float)((double)cam->height / 2.0);
+    v->near_f = (float)cam->near_plane;
+    v->far_f = (float)cam->far_plane;
+    v->near_d = cam->near_plane;
+    v->far_d = cam->far_plane;
+    v->W = cam->width;
+    v->H = cam->height;
+    v->tilesX = (cam->width + DL_TILE - 1) / DL_TILE;
+    v->tilesY = (cam->height + DL_TILE - 1) / DL_TILE;
+    if (v->tilesX > 0xffffu || v->tilesY > 0xffffu || (uint64_t)v->tilesX * v->tilesY >= (1u << 20)) {
+        dl_set_error("image too large: at most 2^20 16x16 tiles and 65535 tiles per axis");
+        return DL_E_CAPACITY;
+    }
+    v->numTiles = v->tilesX * v->tilesY;
+    v->projection = cam->projection;
+    v->maxCoverage = maxCov;
+    const float dflt[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+    for (int k = 0; k < 4; k++) v->bg[k] = bg ? bg[k] : dflt[k];
+    return DL_OK;
+}
+
+int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t st) {
+    if (!d) { dl_set_error("splats is NULL"); return DL_E_INVALID_ARG; }
+    if (d->sh_bands < 0 || d->sh_bands > 3) { dl_set_error("sh_bands must be 0..3"); return DL_E_INVALID_ARG; }
+    if (d->count >= (1ull << 30)) { dl_set_error("at most 2^30 - 1 splats"); return DL_E_CAPACITY; }
+    const uint64_t n = d->count;
+    if (n > 0 && (!d->positions || !d->rotations || !d->log_scales || !d->opacity_logits || !d->colors_dc)) {
+        dl_set_error("splats: a required array is NULL");
+        return DL_E_INVALID_ARG;
+    }
+    if (precision < DL_PREC_F32 || precision > DL_PREC_BF16) { dl_set_error("bad precision"); return DL_E_INVALID_ARG; }
+    // SH coefficients absent: the reference packs zeros (preprocess.ts:127-135), which adds
+    // exactly zero to the colour, so the splats render as band 0.
+    const int bands = d->colors_sh ? d->sh_bands : 0;
+    const int M = bands == 0 ? 0 : bands == 1 ? 3 : bands == 2 ? 8 : 15;
+    const uint64_t a = 256;
+    const uint64_t oPos = 0, oRot = round_up(oPos + 12 * n, a), oLsc = round_up(oRot + 16 * n, a);
+    const uint64_t oOpl = round_up(oLsc + 12 * n, a), oDc = round_up(oOpl + 4 * n, a);
+    const uint64_t oSh = round_up(oDc + 12 * n, a);
+    const uint64_t shBytes = (uint64_t)3 * M * n * (precision == DL_PREC_F32 ? 4 : 2);
+    const uint64_t oTmp = round_up(oSh + shBytes, a);
+    const uint64_t total = (precision == DL_PREC_F32 || M == 0) ? oTmp : oTmp + (uint64_t)3 * M * n * 4;
+    DL_TRY(s->mem.ensure(total));
+    char* b = s->mem.as<char>();
+    if (n) {
+        DL_CK(cudaMemcpyAsync(b + oPos, d->positions, 12 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(b + oRot, d->rotations, 16 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(b + oLsc, d->log_scales, 12 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(b + oOpl, d->opacity_logits, 4 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(b + oDc, d->colors_dc, 12 * n, cudaMemcpyHostToDevice, st));
+        if (M) {
+            if (precision == DL_PREC_F32) {
+                DL_CK(cudaMemcpyAsync(b + oSh, d->colors_sh, shBytes, cudaMemcpyHostToDevice, st));
+            } else {
+                DL_CK(cudaMemcpyAsync(b + oTmp, d->colors_sh, (uint64_t)3 * M * n * 4, cudaMemcpyHostToDevice, st));
+                sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp), (uint16_t*)(b + oSh), (uint64_t)3 * M * n,
+                                                   precision);
+                DL_CK(cudaGetLastError());
+            }
+        }
+    }
+    s->precision = precision;
+    s->d.pos = (const float*)(b + oPos);
+    s->d.rot = (const float*)(b + oRot);
+    s->d.lsc = (const float*)(b + oLsc);
+    s->d.opl = (const float*)(b + oOpl);
+    s->d.dc = (const float*)(b + oDc);
+    s->d.sh = (M && precision == DL_PREC_F32) ? (const float*)(b + oSh) : nullptr;
+    s->d.sh16 = (M && precision != DL_PREC_F32) ? (const uint16_t*)(b + oSh) : nullptr;
+    s->d.n = (uint32_t)n;
+    s->d.bands = bands;
+    s->d.sh_kind = M ? precision : 0;
+    return DL_OK;
+}
+
+int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint32_t V, uint32_t* const* d_outs,
+                    uint32_t flags) {
+    cudaStream_t st = r->stream;
+    const uint32_t N = sc.n;
+    const uint64_t stride = round_up(std::max<uint32_t>(N, 1), 64);
+    const bool f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
+    const bool fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
+    uint32_t maxT = 1;
+    for (uint32_t v = 0; v < V; v++) maxT = std::max(maxT, hv[v].numTiles);
+    const uint32_t TS = maxT + 1;
+    const uint32_t depthTilesPerView = (uint32_t)((N + dlsort::kTile - 1) / dlsort::kTile);
+    const uint32_t emitTilesPerView = (uint32_t)((stride + dlr::kEmitRanks - 1) / dlr::kEmitRanks);
+    r->launches = 0;
+
+    // ---- buffers
+    DL_TRY(r->views.ensure(sizeof(DlView) * V));
+    DL_TRY(r->segStart.ensure(8ull * V));
+    DL_TRY(r->segLen.ensure(4ull * V));
+    DL_TRY(r->segTileBase.ensure(4ull * V));
+    DL_TRY(r->scratch.ensure(4ull * kScratchWords));
+    DL_TRY(r->keys0.ensure(4ull * V * stride));
+    DL_TRY(r->keys1.ensure(4ull * V * stride));
+    DL_TRY(r->vals0.ensure(4ull * V * stride));
+    DL_TRY(r->vals1.ensure(4ull * V * stride));
+    DL_TRY(r->recA.ensure(16ull * V * stride));
+    if (f16rec) DL_TRY(r->recH.ensure(16ull * V * stride));
+    else DL_TRY(r->recBC.ensure(32ull * V * stride));
+    DL_TRY(r->bbox.ensure(8ull * V * stride));
+    DL_TRY(r->nvis.ensure(4ull * V));
+    DL_TRY(r->depthHist.ensure(4ull * V * 4 * 256));
+    DL_TRY(r->outs.ensure(sizeof(uint32_t*) * V));
+    DL_TRY(r->tileCount.ensure(4ull * V * TS));
+    DL_TRY(r->tileOff.ensure(4ull * V * TS));
+    DL_TRY(r->pairBase.ensure(8ull * V));
+    DL_TRY(r->pairCap.ensure(8ull * V));
+    DL_TRY(r->npairs.ensure(8ull * V));
+    DL_TRY(r->pairSegLen.ensure(4ull * V));
+    DL_TRY(r->pairSegTileBase.ensure(4ull * V));
+    DL_TRY(r->pairGlob.ensure(4ull * V * 4 * 256));
+    DL_TRY(r->emitStatus.ensure(8ull * V * emitTilesPerView));
+    if (r->keep_accum && V == 1) DL_TRY(r->accum.ensure(16ull * hv[0].W * hv[0].H));
+
+    // ---- host-side tables (pinned staging), one upload
+    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + 8ull * V * 2 + sizeof(void*) * V;
+    DL_TRY(ensure_pinned((void**)&r->h_views, &r->h_views_cap, hbytes));
+    char* hb = (char*)r->h_views;
+    std::memcpy(hb, hv, sizeof(DlView) * V);
+    uint64_t* hSegStart = (uint64_t*)(hb + sizeof(DlView) * V);
+    uint32_t* hSegLen = (uint32_t*)(hSegStart + V);
+    for (uint32_t v = 0; v < V; v++) { hSegStart[v] = (uint64_t)v * stride; hSegLen[v] = N; }
+    void** hOuts = (void**)(hSegLen + V);
+    for (uint32_t v = 0; v < V; v++) hOuts[v] = d_outs[v];
+    DL_CK(cudaMemcpyAsync(r->views.p, hb, sizeof(DlView) * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(r->segStart.p, hSegStart, 8ull * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(r->segLen.p, hSegLen, 4ull * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(r->outs.p, hOuts, sizeof(void*) * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemsetAsync(r->scratch.p, 0, 4ull * kScratchWords, st));
+    DL_CK(cudaMemsetAsync(r->nvis.p, 0, 4ull * V, st));
+    uint32_t* scr = r->scratch.as<uint32_t>();
+
+    // ---- 1. project (+ f64 cull and depth keys)
+    ev_record(r, 0);
+    dlr::ProjectArgs pa;
+    pa.sc = sc;
+    pa.views = r->views.as<DlView>();
+    pa.num_views = V;
+    pa.view_stride = stride;
+    pa.keys = r->keys0.as<uint32_t>();
+    pa.recA = r->recA.as<float4>();
+    pa.recBC = f16rec ? nullptr : r->recBC.as<float4>();
+    pa.recH = f16rec ? r->recH.as<uint4>() : nullptr;
+    pa.bbox = r->bbox.as<uint2>();
+    pa.nvis = r->nvis.as<uint32_t>();
+    if (N) {
+        dlr::project_k<<<(N + 255) / 256, 256, 0, st>>>(pa);
+        r->launches++;
+    }
+    DL_CK(cudaGetLastError());
+    ev_record(r, 1);
+
+    // ---- 2. depth sort: stable LSD, 4 x 8-bit digits, one segment per view
+    dlsort::Segs ds;
+    ds.start = r->segStart.as<uint64_t>();
+    ds.len = r->segLen.as<uint32_t>();
+    ds.tile_base = r->segTileBase.as<uint32_t>();
+    ds.total_tiles = scr + SC_DEPTH_TILES;
+    ds.num = V;
+    const uint32_t depthGrid = std::max<uint32_t>(1, V * depthTilesPerView);
+    DL_TRY(r->sortStatus.ensure(4ull * 256 * depthGrid));
+    if (N) {
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ds);
+        DL_CK(cudaMemsetAsync(r->depthHist.p, 0, 4ull * V * 4 * 256, st));
+        dlsort::hist_k<8><<<std::min<uint32_t>(depthGrid, 4096), dlsort::kThreads, 0, st>>>(
+            r->keys0.as<uint32_t>(), ds, 4, 0, r->depthHist.as<uint32_t>());
+        dlsort::scan_hist_k<8><<<std::min<uint32_t>(4 * V, 1024), 256, 0, st>>>(r->depthHist.as<uint32_t>(), 4 * V);
+        r->launches += 3;
+        uint32_t* kin = r->keys0.as<uint32_t>();
+        uint32_t* kout = r->keys1.as<uint32_t>();
+        uint32_t* vin = nullptr;
+        uint32_t* vout = r->vals1.as<uint32_t>();
+        for (int p = 0; p < 4; p++) {
+            DL_CK(cudaMemsetAsync(r->sortStatus.p, 0, 4ull * 256 * depthGrid, st));
+            dlsort::Pass sp;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
+            sp.segs = ds; sp.glob_off = r->depthHist.as<uint32_t>();
+            sp.status = r->sortStatus.as<uint32_t>(); sp.counter = scr + SC_DEPTH_CTR + p; sp.err = scr + SC_ERR;
+            sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
+            launch_pass_bits(8, sp, depthGrid, st);
+            r->launches++;
+            std::swap(kin, kout);
+            vin = vout;
+            vout = (vout == r->vals1.as<uint32_t>()) ? r->vals0.as<uint32_t>() : r->vals1.as<uint32_t>();
+        }
+        DL_CK(cudaGetLastError());
+    }
+    ev_record(r, 2);
+    // after 4 passes: keys0 / vals0 hold the sorted keys / splat indices
+
+    // ---- 3.. pair stages (re-run if the pair buffers overflow)
+    int keyBits = 0;
+    while ((1u << keyBits) < maxT) keyBits++;
+    const int pbits = 8;
+    const int ppasses = (keyBits + pbits - 1) / pbits;
+    if (r->pair_cap_per_view == 0) r->pair_cap_per_view = std::max<uint64_t>(1u << 20, 4ull * N);
+    for (int attempt = 0; attempt < 3; attempt++) {
+        const uint64_t cap = r->pair_cap_per_view;
+        if (cap >= (1ull << 30)) { dl_set_error("more than 2^30 tile pairs in one view"); return DL_E_CAPACITY; }
+        DL_TRY(r->pkeys0.ensure(4ull * V * cap));
+        DL_TRY(r->pvals0.ensure(4ull * V * cap));
+        if (ppasses > 0) {
+            DL_TRY(r->pkeys1.ensure(4ull * V * cap));
+            DL_TRY(r->pvals1.ensure(4ull * V * cap));
+        }
+        const uint32_t pairGrid = std::max<uint32_t>(1, (uint32_t)(V * ((cap + dlsort::kTile - 1) / dlsort::kTile)));
+        DL_TRY(r->sortStatus.ensure(4ull * 256 * std::max(pairGrid, depthGrid)));
+        DL_TRY(ensure_pinned((void**)&r->h_u64, &r->h_u64_cap, 16ull * V + 64));
+        for (uint32_t v = 0; v < V; v++) { r->h_u64[v] = (uint64_t)v * cap; r->h_u64[V + v] = cap; }
+        DL_CK(cudaMemcpyAsync(r->pairBase.p, r->h_u64, 8ull * V, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(r->pairCap.p, r->h_u64 + V, 8ull * V, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemsetAsync(r->tileCount.p, 0, 4ull * V * TS, st));
+        DL_CK(cudaMemsetAsync(r->emitStatus.p, 0, 8ull * V * emitTilesPerView, st));
+        DL_CK(cudaMemsetAsync(scr + SC_EMIT_CTR, 0, 4ull * 6, st));   // emit + pair counters + work counter
+        DL_CK(cudaMemsetAsync(scr + SC_OVF, 0, 4, st));
+
+        ev_record(r, 3);
+        dlr::EmitArgs ea;
+        ea.sorted_vals = r->vals0.as<uint32_t>();
+        ea.bbox = r->bbox.as<uint2>();
+        ea.nvis = r->nvis.as<uint32_t>();
+        ea.views = r->views.as<DlView>();
+        ea.view_stride = stride;
+        ea.tiles_per_view = emitTilesPerView;
+        ea.pair_base = r->pairBase.as<uint64_t>();
+        ea.pair_cap = r->pairCap.as<uint64_t>();
+        ea.pair_keys = r->pkeys0.as<uint32_t>();
+        ea.pair_vals = r->pvals0.as<uint32_t>();
+        ea.npairs = r->npairs.as<unsigned long long>();
+        ea.tile_count = r->tileCount.as<uint32_t>();
+        ea.tile_stride = TS;
+        ea.status = r->emitStatus.as<unsigned long long>();
+        ea.counter = scr + SC_EMIT_CTR;
+        ea.err = scr + SC_ERR;
+        ea.ovf = scr + SC_OVF;
+        dlr::emit_k<<<V * emitTilesPerView, dlr::kEmitThreads, 0, st>>>(ea);
+        r->launches++;
+        DL_CK(cudaGetLastError());
+        ev_record(r, 4);
+
+        dlr::TileOffArgs ta;
+        ta.views = r->views.as<DlView>();
+        ta.tile_count = r->tileCount.as<uint32_t>();
+        ta.tile_off = r->tileOff.as<uint32_t>();
+        ta.tile_stride = TS;
+        ta.npairs = r->npairs.as<unsigned long long>();
+        ta.pair_cap = r->pairCap.as<uint64_t>();
+        ta.seg_len = r->pairSegLen.as<uint32_t>();
+        ta.glob_off = r->pairGlob.as<uint32_t>();
+        ta.bits = pbits;
+        ta.passes = ppasses;
+        dlr::tile_offsets_k<<<V, 1024, 0, st>>>(ta);
+        r->launches++;
+        DL_CK(cudaGetLastError());
+        ev_record(r, 5);
+
+        // pair sort by tile id (stable: depth-rank order kept inside each tile)
+        uint32_t* finalVals = r->pvals0.as<uint32_t>();
+        if (ppasses > 0) {
+            dlsort::Segs ps;
+            ps.start = r->pairBase.as<uint64_t>();
+            ps.len = r->pairSegLen.as<uint32_t>();
+            ps.tile_base = r->pairSegTileBase.as<uint32_t>();
+            ps.total_tiles = scr + SC_PAIR_TILES;
+            ps.num = V;
+            dlsort::prepare_k<<<1, 32, 0, st>>>(ps);
+            r->launches++;
+            uint32_t* kin = r->pkeys0.as<uint32_t>();
+            uint32_t* kout = r->pkeys1.as<uint32_t>();
+            uint32_t* vin = r->pvals0.as<uint32_t>();
+            uint32_t* vout = r->pvals1.as<uint32_t>();
+            for (int p = 0; p < ppasses; p++) {
+                DL_CK(cudaMemsetAsync(r->sortStatus.p, 0, 4ull * 256 * pairGrid, st));
+                dlsort::Pass sp;
+                sp.keys_in = kin; sp.vals_in = vin;
+                sp.keys_out = (p + 1 < ppasses) ? kout : nullptr;
+                sp.vals_out = vout;
+                sp.segs = ps; sp.glob_off = r->pairGlob.as<uint32_t>();
+                sp.status = r->sortStatus.as<uint32_t>(); sp.counter = scr + SC_PAIR_CTR + p; sp.err = scr + SC_ERR;
+                sp.shift = pbits * p; sp.pass = p; sp.passes = ppasses;
+                launch_pass_bits(pbits, sp, pairGrid, st);
+                r->launches++;
+                std::swap(kin, kout);
+                std::swap(vin, vout);
+            }
+            finalVals = vin;
+            DL_CK(cudaGetLastError());
+        }
+        ev_record(r, 6);
+
+        dlr::RasterArgs ra;
+        std::memset(&ra, 0, sizeof(ra));
+        ra.views = r->views.as<DlView>();
+        ra.tile_off = r->tileOff.as<uint32_t>();
+        ra.tile_stride = TS;
+        ra.pair_vals = finalVals;
+        ra.pair_base = r->pairBase.as<uint64_t>();
+        ra.recA = r->recA.as<float4>();
+        ra.recBC = f16rec ? nullptr : r->recBC.as<float4>();
+        ra.recH = f16rec ? r->recH.as<uint4>() : nullptr;
+        ra.view_stride = stride;
+        ra.outs = r->outs.as<uint32_t*>();
+        ra.accum = (r->keep_accum && V == 1) ? r->accum.as<float4>() : nullptr;
+        const dim3 rg(maxT, V);
+        if (fastExp) dlr::rasterize_k<false><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
+        else dlr::rasterize_k<true><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
+        r->launches++;
+        DL_CK(cudaGetLastError());
+        ev_record(r, 7);
+
+        // one sync per frame: error word and pair totals
+        DL_CK(cudaMemcpyAsync(r->h_u64, r->npairs.p, 8ull * V, cudaMemcpyDeviceToHost, st));
+        DL_CK(cudaMemcpyAsync(r->h_u64 + V, scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));
+        DL_CK(cudaMemcpyAsync(r->h_u64 + V + 1, scr + SC_OVF, 4, cudaMemcpyDeviceToHost, st));
+        DL_CK(cudaStreamSynchronize(st));
+        const uint32_t err = (uint32_t)(r->h_u64[V] & 0xffffffffu) | (uint32_t)(r->h_u64[V + 1] & 0xffffffffu);
+        if (r->profiling) {
+            float ms;
+            const int from[6] = {0, 1, 3, 4, 5, 6}, to[6] = {1, 2, 4, 5, 6, 7};
+            for (int k = 0; k < 6; k++)
+                if (cudaEventElapsedTime(&ms, r->ev[from[k]], r->ev[to[k]]) == cudaSuccess) r->stage_ms[k] += ms;
+        }
+        if (err & DL_DEVERR_TIMEOUT) {
+            dl_set_error("a bounded device-side wait timed out");
+            return DL_E_TIMEOUT;
+        }
+        uint64_t maxPairs = 0;
+        for (uint32_t v = 0; v < V; v++) maxPairs = std::max<uint64_t>(maxPairs, r->h_u64[v]);
+        if (err & DL_DEVERR_OVERFLOW) {
+            r->pair_cap_per_view = maxPairs + maxPairs / 4 + 4096;
+            continue;
+        }
+        r->last_n = N;
+        r->last_stride = (uint32_t)stride;
+        r->last_T = hv[0].numTiles;
+        r->last_W = hv[0].W;
+        r->last_H = hv[0].H;
+        r->last_pairs_final = (uint32_t)r->h_u64[0];
+        r->last_rec_kind = f16rec ? 1 : 0;
+        r->last_final_vals = finalVals;
+        return DL_OK;
+    }
+    dl_set_error("pair buffers overflowed repeatedly");
+    return DL_E_CAPACITY;
+}

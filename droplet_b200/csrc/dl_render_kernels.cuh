@@ -1,0 +1,669 @@
+// dl_render_kernels.cuh — CUDA kernels of the tile-binned forward renderer.
+//
+// Stage map (reference -> here):
+//   camera.ts:56-99 cull + radix-sort.ts key   -> project_k (f64 cull, depth key)
+//   project.ts:59-234 project                    -> project_k (same f32 op order)
+//   radix-sort.ts:65-117 CPU depth sort          -> dlsort passes (dl_sort.cuh)
+//   prefix-sum.ts + pipeline.ts:277-304 scan     -> emit_k (decoupled look-back)
+//   emit-pairs.ts:164-193 emit                    -> emit_k (load-balanced emission)
+//   pipeline.ts:544-578 stable pair sort          -> dlsort passes on tile ids
+//   find-boundaries.ts:17-99 tile offsets         -> tile_offsets_k (scan of per-tile counts)
+//   rasterize.ts:135-181 + finalize.ts:211-224    -> rasterize_k (fused)
+//
+// All f32 arithmetic that feeds an integer decision or an output byte is
+// written in the shaders' evaluation order and compiled with --fmad=false,
+// so results are bit-identical to the CPU restatement of the reference.
+#pragma once
+#include "dl_common.cuh"
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+namespace dlr {
+
+// ------------------------------------------------------------------ project
+struct ProjectArgs {
+    DlSceneDev sc;
+    const DlView* views;
+    uint32_t num_views;
+    uint64_t view_stride;     // elements between views' per-splat arrays (>= N)
+    uint32_t* keys;           // [V][stride] sortable depth key, 0xffffffff if culled
+    float4* recA;             // [V][stride] (screenX, screenY, radius, depth)
+    float4* recBC;            // [V][stride][2] (A, B, C, alpha), (r, g, b, 0)   (f32 records)
+    uint4* recH;              // [V][stride] half records: (A,B) (C,alpha) (r,g) (b,0)  (f16 records)
+    uint2* bbox;              // [V][stride] (minX | minY<<16, maxX | maxY<<16); empty if minX > maxX
+    uint32_t* nvis;           // [V] visible count
+};
+
+struct Cov3 { float c00, c01, c02, c11, c12, c22; };
+
+__device__ __forceinline__ void quat_rot(const float q[4], float vx, float vy, float vz, float o[3]) {
+    // project.ts:50-53 — t = 2*cross(q.yzw, v); v + q.x*t + cross(q.yzw, t)
+    const float qx = q[1], qy = q[2], qz = q[3];
+    const float c0 = qy * vz - qz * vy, c1 = qz * vx - qx * vz, c2 = qx * vy - qy * vx;
+    const float t0 = 2.0f * c0, t1 = 2.0f * c1, t2 = 2.0f * c2;
+    const float d0 = qy * t2 - qz * t1, d1 = qz * t0 - qx * t2, d2 = qx * t1 - qy * t0;
+    o[0] = (vx + q[0] * t0) + d0;
+    o[1] = (vy + q[0] * t1) + d1;
+    o[2] = (vz + q[0] * t2) + d2;
+}
+
+// project.ts:86-98 — view-independent, computed once per splat.
+__device__ __forceinline__ Cov3 make_cov3(const float rot[4], const float s[3]) {
+    float rx[3], ry[3], rz[3];
+    quat_rot(rot, 1.0f, 0.0f, 0.0f, rx);
+    quat_rot(rot, 0.0f, 1.0f, 0.0f, ry);
+    quat_rot(rot, 0.0f, 0.0f, 1.0f, rz);
+    for (int k = 0; k < 3; k++) { rx[k] = rx[k] * s[0]; ry[k] = ry[k] * s[1]; rz[k] = rz[k] * s[2]; }
+    Cov3 c;
+    c.c00 = (rx[0] * rx[0] + ry[0] * ry[0]) + rz[0] * rz[0];
+    c.c01 = (rx[0] * rx[1] + ry[0] * ry[1]) + rz[0] * rz[1];
+    c.c02 = (rx[0] * rx[2] + ry[0] * ry[2]) + rz[0] * rz[2];
+    c.c11 = (rx[1] * rx[1] + ry[1] * ry[1]) + rz[1] * rz[1];
+    c.c12 = (rx[1] * rx[2] + ry[1] * ry[2]) + rz[1] * rz[2];
+    c.c22 = (rx[2] * rx[2] + ry[2] * ry[2]) + rz[2] * rz[2];
+    return c;
+}
+
+__device__ __forceinline__ float sh_coef(const DlSceneDev& sc, uint64_t i) {
+    if (sc.sh_kind == 0) return __ldg(sc.sh + i);
+    const uint16_t b = __ldg(sc.sh16 + i);
+    if (sc.sh_kind == 1) return __half2float(__ushort_as_half(b));
+    return __bfloat162float(__ushort_as_bfloat16(b));
+}
+
+// project.ts:264-331 evalSH (channel-major coefficients, camera-space direction)
+__device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int M, float x, float y, float z,
+                                        float& r, float& g, float& b) {
+    const float SH1 = 0.4886025119029199f, nSH1 = -0.4886025119029199f;
+    const float b1[3] = {nSH1 * y, SH1 * z, nSH1 * x};
+    r = 0.0f; g = 0.0f; b = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r = r + b1[k] * sh_coef(sc, base + k);
+        g = g + b1[k] * sh_coef(sc, base + M + k);
+        b = b + b1[k] * sh_coef(sc, base + 2 * M + k);
+    }
+    if (sc.bands >= 2) {
+        const float xx = x * x, yy = y * y, zz = z * z;
+        const float xy = x * y, yz = y * z, xz = x * z;
+        const float b2[5] = {1.0925484305920792f * xy, -1.0925484305920792f * yz,
+                             0.31539156525252005f * (((2.0f * zz) - xx) - yy), -1.0925484305920792f * xz,
+                             0.5462742152960396f * (xx - yy)};
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            r = r + b2[k] * sh_coef(sc, base + 3 + k);
+            g = g + b2[k] * sh_coef(sc, base + M + 3 + k);
+            b = b + b2[k] * sh_coef(sc, base + 2 * M + 3 + k);
+        }
+        if (sc.bands >= 3) {
+            const float b3[7] = {(-0.5900435899266435f * y) * ((3.0f * xx) - yy),
+                                 (2.890611442640554f * xy) * z,
+                                 (-0.4570457994644658f * y) * (((4.0f * zz) - xx) - yy),
+                                 (0.3731763325901154f * z) * (((2.0f * zz) - (3.0f * xx)) - (3.0f * yy)),
+                                 (-0.4570457994644658f * x) * (((4.0f * zz) - xx) - yy),
+                                 (1.445305721320277f * z) * (xx - yy),
+                                 (-0.5900435899266435f * x) * (xx - (3.0f * yy))};
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                r = r + b3[k] * sh_coef(sc, base + 8 + k);
+                g = g + b3[k] * sh_coef(sc, base + M + 8 + k);
+                b = b + b3[k] * sh_coef(sc, base + 2 * M + 8 + k);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t pack_h2(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// One splat, all views.  Thread per splat, index order (coalesced SoA reads).
+__global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool inRange = g < a.sc.n;
+    float pos[3] = {0, 0, 0}, rot[4] = {1, 0, 0, 0}, s[3] = {1, 1, 1}, dc[3] = {0, 0, 0}, opl = 0.0f;
+    if (inRange) {
+        pos[0] = __ldg(a.sc.pos + 3ull * g); pos[1] = __ldg(a.sc.pos + 3ull * g + 1); pos[2] = __ldg(a.sc.pos + 3ull * g + 2);
+        const float4 q = __ldg(reinterpret_cast<const float4*>(a.sc.rot) + g);
+        rot[0] = q.x; rot[1] = q.y; rot[2] = q.z; rot[3] = q.w;
+        s[0] = dl_expf(__ldg(a.sc.lsc + 3ull * g));
+        s[1] = dl_expf(__ldg(a.sc.lsc + 3ull * g + 1));
+        s[2] = dl_expf(__ldg(a.sc.lsc + 3ull * g + 2));
+        opl = __ldg(a.sc.opl + g);
+        dc[0] = __ldg(a.sc.dc + 3ull * g); dc[1] = __ldg(a.sc.dc + 3ull * g + 1); dc[2] = __ldg(a.sc.dc + 3ull * g + 2);
+    }
+    const Cov3 cv = make_cov3(rot, s);
+    const float sig = dl_sigmoidf(opl);
+    const int M = a.sc.bands == 0 ? 0 : a.sc.bands == 1 ? 3 : a.sc.bands == 2 ? 8 : 15;
+    const uint64_t shBase = (uint64_t)g * 3 * M;
+
+    for (uint32_t v = 0; v < a.num_views; v++) {
+        const DlView& u = a.views[v];
+        const float* V = u.view;
+        const uint64_t o = (uint64_t)v * a.view_stride + g;
+        // ---- camera.ts:56-99: f64 cull and depth key
+        bool visible = false;
+        float depthKey = 0.0f;
+        if (inRange) {
+            const double x = pos[0], y = pos[1], z = pos[2];
+            if (u.projection == 0) {
+                const double cz = (((double)V[2] * x + (double)V[6] * y) + (double)V[10] * z) + (double)V[14];
+                const double depth = -cz;
+                visible = depth > u.near_d && depth < u.far_d;
+                depthKey = (float)depth;
+            } else {
+                const double cx = (((double)V[0] * x + (double)V[4] * y) + (double)V[8] * z) + (double)V[12];
+                const double cy = (((double)V[1] * x + (double)V[5] * y) + (double)V[9] * z) + (double)V[13];
+                const double cz = (((double)V[2] * x + (double)V[6] * y) + (double)V[10] * z) + (double)V[14];
+                const double r2 = (cx * cx + cy * cy) + cz * cz;
+                visible = r2 > u.near_d * u.near_d;
+                depthKey = (float)sqrt(r2);
+            }
+            a.keys[o] = visible ? dl_sortable_key(depthKey) : 0xffffffffu;
+        }
+        const uint32_t ballot = __ballot_sync(0xffffffffu, visible);
+        if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&a.nvis[v], (uint32_t)__popc(ballot));
+        if (!visible) continue;
+
+        // ---- project.ts:79-84
+        const float pcx = ((V[0] * pos[0] + V[4] * pos[1]) + V[8] * pos[2]) + V[12];
+        const float pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
+        const float pcz = ((V[2] * pos[0] + V[6] * pos[1]) + V[10] * pos[2]) + V[14];
+        const float depth = -pcz;
+        float screenX, screenY;
+        bool culled = false;
+        if (u.projection == 0) {
+            culled = depth <= u.near_f || depth >= u.far_f;
+            screenX = (pcx * u.focal) / -pcz + u.cx;
+            screenY = (-pcy * u.focal) / -pcz + u.cy;
+        } else {
+            const float r = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
+            culled = r <= u.near_f;
+            const float lon = dl_atan2f(pcx, -pcz);
+            const float lat = dl_asinf(pcy / r);
+            screenX = (lon / 6.2831853f + 0.5f) * u.width;
+            screenY = (0.5f - lat / 3.14159265f) * u.height;
+        }
+        float conicA = 0, conicB = 0, conicC = 0, radius = 0, radiusFade = 0, aaFactor = 0;
+        if (!culled) {
+            // Σ_cam = V Σ Vᵀ (project.ts:103-123)
+            const float v00 = V[0], v01 = V[4], v02 = V[8], v10 = V[1], v11 = V[5], v12 = V[9];
+            const float v20 = V[2], v21 = V[6], v22 = V[10];
+            const float a00 = (v00 * cv.c00 + v01 * cv.c01) + v02 * cv.c02;
+            const float a01 = (v00 * cv.c01 + v01 * cv.c11) + v02 * cv.c12;
+            const float a02 = (v00 * cv.c02 + v01 * cv.c12) + v02 * cv.c22;
+            const float a10 = (v10 * cv.c00 + v11 * cv.c01) + v12 * cv.c02;
+            const float a11 = (v10 * cv.c01 + v11 * cv.c11) + v12 * cv.c12;
+            const float a12 = (v10 * cv.c02 + v11 * cv.c12) + v12 * cv.c22;
+            const float a20 = (v20 * cv.c00 + v21 * cv.c01) + v22 * cv.c02;
+            const float a21 = (v20 * cv.c01 + v21 * cv.c11) + v22 * cv.c12;
+            const float a22 = (v20 * cv.c02 + v21 * cv.c12) + v22 * cv.c22;
+            const float cc00 = (a00 * v00 + a01 * v01) + a02 * v02;
+            const float cc01 = (a00 * v10 + a01 * v11) + a02 * v12;
+            const float cc02 = (a00 * v20 + a01 * v21) + a02 * v22;
+            const float cc11 = (a10 * v10 + a11 * v11) + a12 * v12;
+            const float cc12 = (a10 * v20 + a11 * v21) + a12 * v22;
+            const float cc22 = (a20 * v20 + a21 * v21) + a22 * v22;
+            // EWA Jacobian as written (project.ts:128-149)
+            const float invZ = 1.0f / pcz;
+            const float j00 = u.focal * invZ;
+            const float j02 = ((-u.focal * pcx) * invZ) * invZ;
+            const float j11 = u.focal * invZ;
+            const float j12 = ((-u.focal * pcy) * invZ) * invZ;
+            const float b00 = j00 * cc00 + j02 * cc02;
+            const float b01 = j00 * cc01 + j02 * cc12;
+            const float b02 = j00 * cc02 + j02 * cc22;
+            const float b11 = j11 * cc11 + j12 * cc12;
+            const float b12 = j11 * cc12 + j12 * cc22;
+            float c00 = b00 * j00 + b02 * j02;
+            const float c01 = b01 * j11 + b02 * j12;
+            float c11 = b11 * j11 + b12 * j12;
+            const float detOrig = c00 * c11 - c01 * c01;
+            c00 = c00 + DL_AA_DILATION;
+            c11 = c11 + DL_AA_DILATION;
+            const float det = c00 * c11 - c01 * c01;
+            aaFactor = sqrtf(fmaxf(detOrig / det, 0.0f));
+            if (det <= 1.0e-6f) {
+                culled = true;
+            } else {
+                const float invDet = 1.0f / det;
+                conicA = c11 * invDet;
+                conicB = -c01 * invDet;
+                conicC = c00 * invDet;
+                const float mid = 0.5f * (c00 + c11);
+                const float radiusEig = sqrtf(fmaxf(0.1f, mid * mid - det));
+                const float lambda1 = mid + radiusEig;
+                const float radiusRaw = DL_SIGMA_CUTOFF * sqrtf(lambda1);
+                const float fadeStart = DL_FADE_START_FRAC * u.height;
+                const float fadeEnd = DL_FADE_END_FRAC * u.height;
+                radiusFade = fminf(fmaxf((fadeEnd - radiusRaw) / (fadeEnd - fadeStart), 0.0f), 1.0f);
+                if (radiusFade <= 0.0f) culled = true;
+                else radius = ceilf(fminf(radiusRaw, fadeEnd));
+            }
+        }
+        if (culled) {
+            a.recA[o] = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
+            a.bbox[o] = make_uint2(0xffffu, 0u);
+            continue;
+        }
+        float col0 = dc[0], col1 = dc[1], col2 = dc[2];
+        if (a.sc.bands > 0) {
+            const float len = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
+            float sr, sg, sb;
+            eval_sh(a.sc, shBase, M, pcx / len, pcy / len, pcz / len, sr, sg, sb);
+            col0 = col0 + sr; col1 = col1 + sg; col2 = col2 + sb;
+        }
+        col0 = fmaxf(col0 + 0.5f, 0.0f);
+        col1 = fmaxf(col1 + 0.5f, 0.0f);
+        col2 = fmaxf(col2 + 0.5f, 0.0f);
+        const float alpha = (sig * radiusFade) * aaFactor;
+        a.recA[o] = make_float4(screenX, screenY, radius, depth);
+        if (a.recBC) {
+            a.recBC[2 * o] = make_float4(conicA, conicB, conicC, alpha);
+            a.recBC[2 * o + 1] = make_float4(col0, col1, col2, 0.0f);
+        } else {
+            a.recH[o] = make_uint4(pack_h2(conicA, conicB), pack_h2(conicC, alpha), pack_h2(col0, col1),
+                                   pack_h2(col2, 0.0f));
+        }
+        // project.ts:224-233 tile AABB (u32() saturates: off-screen left/top splats land in row/col 0)
+        const uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
+        const uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
+        const uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, floorf((screenX + radius) / 16.0f)));
+        const uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, floorf((screenY + radius) / 16.0f)));
+        if (maxTX >= minTX && maxTY >= minTY)
+            a.bbox[o] = make_uint2(minTX | (minTY << 16), maxTX | (maxTY << 16));
+        else
+            a.bbox[o] = make_uint2(0xffffu, 0u);
+    }
+}
+
+// ------------------------------------------------------------------ emit
+// Fused: gather tile counts in depth-rank order, exclusive scan with a
+// decoupled look-back across CTAs (replaces the two scan kernels and the host
+// block-sum scan), then write every pair of the CTA's contiguous output range
+// with consecutive threads on consecutive slots (load-balanced, coalesced).
+constexpr int kEmitThreads = 256;
+constexpr int kEmitItems = 4;
+constexpr int kEmitRanks = kEmitThreads * kEmitItems;   // 1024 ranks per CTA
+constexpr unsigned long long kEmitAgg = 1ull << 62;
+constexpr unsigned long long kEmitPrefix = 2ull << 62;
+constexpr unsigned long long kEmitMask = (1ull << 62) - 1;
+
+struct EmitArgs {
+    const uint32_t* sorted_vals;   // [V][stride] rank -> splat
+    const uint2* bbox;             // [V][stride]
+    const uint32_t* nvis;          // [V]
+    const DlView* views;
+    uint64_t view_stride;
+    uint32_t tiles_per_view;       // ceil(stride / kEmitRanks)
+    const uint64_t* pair_base;     // [V]
+    const uint64_t* pair_cap;      // [V]
+    uint32_t* pair_keys;
+    uint32_t* pair_vals;
+    unsigned long long* npairs;    // [V] out
+    uint32_t* tile_count;          // [V][tile_stride] (zeroed)
+    uint32_t tile_stride;
+    unsigned long long* status;    // [V][tiles_per_view] (zeroed)
+    uint32_t* counter;
+    uint32_t* err;                 // DL_DEVERR_TIMEOUT
+    uint32_t* ovf;                 // DL_DEVERR_OVERFLOW
+};
+
+__device__ __forceinline__ uint32_t bbox_count(uint2 bb, uint32_t maxCov) {
+    const uint32_t minX = bb.x & 0xffffu, minY = bb.x >> 16, maxX = bb.y & 0xffffu, maxY = bb.y >> 16;
+    if (maxX < minX || maxY < minY) return 0u;
+    const uint32_t c = (maxX - minX + 1u) * (maxY - minY + 1u);
+    return c > maxCov ? maxCov : c;
+}
+
+__global__ void __launch_bounds__(kEmitThreads) emit_k(EmitArgs a) {
+    __shared__ uint32_t s_excl[kEmitRanks + 1];
+    __shared__ uint32_t s_g[kEmitRanks];
+    __shared__ uint32_t s_min[kEmitRanks];
+    __shared__ uint16_t s_span[kEmitRanks];
+    __shared__ uint32_t s_wsum[kEmitThreads / 32];
+    __shared__ uint32_t s_tile;
+    __shared__ unsigned long long s_prefix;
+    __shared__ uint32_t s_skip;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t v = tile / a.tiles_per_view;
+    const uint32_t lt = tile - v * a.tiles_per_view;
+    const uint32_t n = a.nvis[v];
+    const uint32_t r0 = lt * kEmitRanks;
+    if (r0 >= n) {
+        if (lt == 0 && tid == 0) a.npairs[v] = 0ull;
+        return;
+    }
+    const DlView& u = a.views[v];
+    const uint64_t vo = (uint64_t)v * a.view_stride;
+
+    uint32_t cnt[kEmitItems], gs[kEmitItems], mins[kEmitItems], spans[kEmitItems];
+    uint32_t local = 0;
+#pragma unroll
+    for (int j = 0; j < kEmitItems; j++) {
+        const uint32_t r = r0 + tid * kEmitItems + j;
+        cnt[j] = 0; gs[j] = 0; mins[j] = 0; spans[j] = 1;
+        if (r < n) {
+            const uint32_t g = a.sorted_vals[vo + r];
+            const uint2 bb = a.bbox[vo + g];
+            gs[j] = g;
+            cnt[j] = bbox_count(bb, u.maxCoverage);
+            mins[j] = bb.x;
+            spans[j] = (bb.y & 0xffffu) - (bb.x & 0xffffu) + 1u;
+        }
+        local += cnt[j];
+    }
+    // block exclusive scan of per-thread sums
+    uint32_t inc = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    uint32_t wpre = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kEmitThreads / 32; w++) { if (w < warp) wpre += s_wsum[w]; total += s_wsum[w]; }
+    uint32_t run = wpre + inc - local;
+#pragma unroll
+    for (int j = 0; j < kEmitItems; j++) {
+        const int i = tid * kEmitItems + j;
+        s_excl[i] = run;
+        s_g[i] = gs[j];
+        s_min[i] = mins[j];
+        s_span[i] = (uint16_t)spans[j];
+        run += cnt[j];
+    }
+    if (tid == 0) s_excl[kEmitRanks] = total;
+
+    // decoupled look-back over this view's earlier CTAs
+    if (tid == 0) {
+        unsigned long long* st = a.status + (uint64_t)v * a.tiles_per_view;
+        unsigned long long excl = 0;
+        if (lt == 0) {
+            dl_st_volatile64(&st[0], kEmitPrefix | (unsigned long long)total);
+        } else {
+            __threadfence();
+            dl_st_volatile64(&st[lt], kEmitAgg | (unsigned long long)total);
+            int64_t q = (int64_t)lt - 1;
+            uint32_t spins = 0;
+            while (q >= 0) {
+                const unsigned long long s = dl_ld_volatile64(&st[q]);
+                const unsigned long long flag = s & ~kEmitMask;
+                if (flag == 0ull) {
+                    if (++spins > DL_SPIN_LIMIT) { atomicOr(a.err, DL_DEVERR_TIMEOUT); break; }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += s & kEmitMask;
+                if (flag == kEmitPrefix) break;
+                q--;
+            }
+            __threadfence();
+            dl_st_volatile64(&st[lt], kEmitPrefix | ((excl + total) & kEmitMask));
+        }
+        s_prefix = excl;
+        if (r0 + kEmitRanks >= n) a.npairs[v] = excl + total;    // last CTA of the view
+        const bool over = excl + total > a.pair_cap[v];
+        if (over) atomicOr(a.ovf, DL_DEVERR_OVERFLOW);
+        s_skip = over ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s_skip) return;
+    const uint64_t outBase = a.pair_base[v] + s_prefix;
+    uint32_t* tc = a.tile_count + (uint64_t)v * a.tile_stride;
+    for (uint32_t o = tid; o < total; o += kEmitThreads) {
+        // last rank slot whose exclusive offset is <= o
+        uint32_t lo = 0, hi = kEmitRanks;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_excl[mid] <= o) lo = mid; else hi = mid;
+        }
+        const uint32_t w = o - s_excl[lo];
+        const uint32_t span = s_span[lo];
+        const uint32_t mn = s_min[lo];
+        const uint32_t ty = (mn >> 16) + w / span;
+        const uint32_t tx = (mn & 0xffffu) + w % span;
+        const uint32_t tileId = ty * u.tilesX + tx;
+        a.pair_keys[outBase + o] = tileId;
+        a.pair_vals[outBase + o] = s_g[lo];
+        atomicAdd(&tc[tileId], 1u);
+    }
+}
+
+// ------------------------------------------------------------------ tile offsets
+// tileOffsets[t] = number of pairs with tile < t (find-boundaries.ts semantics,
+// including start == end for empty tiles and tileOffsets[T] = numPairs), plus
+// the pair sort's per-view digit offsets and segment lengths.  One CTA per view.
+struct TileOffArgs {
+    const DlView* views;
+    const uint32_t* tile_count;    // [V][tile_stride]
+    uint32_t* tile_off;            // [V][tile_stride] (T+1 used)
+    uint32_t tile_stride;
+    const unsigned long long* npairs;
+    const uint64_t* pair_cap;
+    uint32_t* seg_len;             // [V] pair-sort segment lengths (0 on overflow)
+    uint32_t* glob_off;            // [V][passes][radix]
+    int bits, passes;
+};
+
+__global__ void __launch_bounds__(1024) tile_offsets_k(TileOffArgs a) {
+    __shared__ uint32_t s_hist[4 * 256];
+    __shared__ uint32_t s_wsum[32];
+    __shared__ uint32_t s_carry;
+    const uint32_t v = blockIdx.x;
+    const uint32_t T = a.views[v].numTiles;
+    const uint32_t* tc = a.tile_count + (uint64_t)v * a.tile_stride;
+    uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    const int radix = 1 << a.bits;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < 4 * 256; i += blockDim.x) s_hist[i] = 0;
+    if (tid == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < T; base += blockDim.x) {
+        const uint32_t t = base + tid;
+        const uint32_t c = t < T ? tc[t] : 0u;
+        if (c) {
+            for (int p = 0; p < a.passes; p++) atomicAdd(&s_hist[p * 256 + ((t >> (p * a.bits)) & (radix - 1))], c);
+        }
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += x;
+        }
+        if (lane == 31) s_wsum[warp] = inc;
+        __syncthreads();
+        uint32_t wpre = 0, tot = 0;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) { if (w < warp) wpre += s_wsum[w]; tot += s_wsum[w]; }
+        if (t < T) to[t] = s_carry + wpre + inc - c;
+        __syncthreads();
+        if (tid == 0) s_carry += tot;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        to[T] = s_carry;
+        const bool ok = a.npairs[v] <= a.pair_cap[v];
+        a.seg_len[v] = ok ? (uint32_t)a.npairs[v] : 0u;
+    }
+    for (int p = 0; p < a.passes; p++) {
+        if (tid == 0) {
+            uint32_t acc = 0;
+            for (int d = 0; d < radix; d++) {
+                const uint32_t x = s_hist[p * 256 + d];
+                a.glob_off[((uint64_t)v * a.passes + p) * radix + d] = acc;
+                acc += x;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ rasterize
+// One CTA per (view, 16x16 tile), one thread per pixel.  The tile's slice is
+// walked in batches of 256 pairs staged in shared memory; a staging thread
+// drops pairs whose screen box cannot reach any pixel centre of the tile
+// (conservative by one pixel, so no pixel's per-pixel box test could pass),
+// keeping order.  Each pixel then runs rasterize.ts:161-178 verbatim, and the
+// finalize shader (finalize.ts:211-224) is fused as the epilogue.
+struct RasterArgs {
+    const DlView* views;
+    const uint32_t* tile_off;      // [V][tile_stride]
+    uint32_t tile_stride;
+    const uint32_t* pair_vals;     // sorted by tile, rank order within a tile
+    const uint64_t* pair_base;     // [V]
+    const float4* recA;            // [V][view_stride]
+    const float4* recBC;           // f32 records, or
+    const uint4* recH;             // f16 records
+    uint64_t view_stride;
+    uint32_t* const* outs;         // [V] packed RGBA8 per pixel
+    float4* accum;                 // optional [W*H] (single view debug)
+    const uint32_t* work;          // optional persistent work list: (v << 20) | tile
+    uint32_t num_work;
+    uint32_t* work_counter;
+    const float* pixel_cost;       // unused placeholder for cost logging
+    uint32_t* tile_evals;          // optional [V][tile_stride] per-tile evaluated-pair counts
+};
+
+constexpr int kRasterThreads = 256;
+
+template <bool kExactExp>
+__device__ __forceinline__ float raster_exp(float p) {
+    if (kExactExp) return dl_expf(p);
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(p * 1.4426950408889634f));
+    return y;
+}
+
+template <bool kExactExp>
+__device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uint32_t tile,
+                                            float4* s_a, float4* s_b, float2* s_c, uint32_t* s_wc) {
+    const DlView& u = a.views[v];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
+    const uint32_t x = tx * DL_TILE + (tid & 15), y = ty * DL_TILE + (tid >> 4);
+    const bool inImage = x < u.W && y < u.H;
+    const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+    const float tx0 = (float)(tx * DL_TILE) + 0.5f - 1.0f, tx1 = (float)(tx * DL_TILE + DL_TILE - 1) + 0.5f + 1.0f;
+    const float ty0 = (float)(ty * DL_TILE) + 0.5f - 1.0f, ty1 = (float)(ty * DL_TILE + DL_TILE - 1) + 0.5f + 1.0f;
+    const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    const uint32_t start = to[tile], end = to[tile + 1];
+    const uint32_t* vals = a.pair_vals + a.pair_base[v];
+    const uint64_t vo = (uint64_t)v * a.view_stride;
+
+    float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
+    bool done = !inImage;
+    uint32_t evals = 0;
+    for (uint32_t b = start; b < end; b += kRasterThreads) {
+        // ---- stage: load, conservative tile-box filter, ordered compaction
+        const uint32_t e = b + tid;
+        bool keep = false;
+        float4 ra = make_float4(0, 0, 0, 0);
+        uint32_t g = 0;
+        if (e < end) {
+            g = vals[e];
+            ra = __ldg(a.recA + vo + g);
+            const float r = ra.z;
+            keep = r > 0.0f && !(ra.x - r > tx1) && !(ra.x + r < tx0) && !(ra.y - r > ty1) && !(ra.y + r < ty0);
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_wc[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, nsurv = 0;
+#pragma unroll
+        for (int w = 0; w < kRasterThreads / 32; w++) { if (w < warp) before += s_wc[w]; nsurv += s_wc[w]; }
+        if (keep) {
+            const uint32_t slot = before + __popc(bal & dl_lanemask_lt());
+            float A, B, C, al, cr, cg, cb;
+            if (a.recBC) {
+                const float4 p = __ldg(a.recBC + 2 * (vo + g));
+                const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
+                A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
+            } else {
+                const uint4 h = __ldg(a.recH + vo + g);
+                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&h.x));
+                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&h.y));
+                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&h.z));
+                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&h.w));
+                A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+            }
+            s_a[slot] = make_float4(ra.x, ra.y, ra.z, A);
+            s_b[slot] = make_float4(2.0f * B, C, al, cr);
+            s_c[slot] = make_float2(cg, cb);
+        }
+        __syncthreads();
+        // ---- per-pixel front-to-back compositing (rasterize.ts:161-178)
+        if (!done) {
+            for (uint32_t j = 0; j < nsurv; j++) {
+                const float4 sa = s_a[j];
+                const float dx = px - sa.x;
+                const float dy = py - sa.y;
+                if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
+                const float4 sb = s_b[j];
+                evals++;
+                const float power = -0.5f * ((((sa.w * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
+                if (power > 0.0f) continue;
+                const float alpha = fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
+                if (alpha < DL_MIN_ALPHA) continue;
+                const float w = T * alpha;
+                const float2 sc = s_c[j];
+                c0 = c0 + w * sb.w;
+                c1 = c1 + w * sc.x;
+                c2 = c2 + w * sc.y;
+                T = T * (1.0f - alpha);
+                if (T < DL_MIN_T) { done = true; break; }
+            }
+        }
+        if (__syncthreads_count(!done) == 0) break;
+    }
+    if (a.tile_evals) {
+        uint32_t s = evals;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0 && s) atomicAdd(&a.tile_evals[(uint64_t)v * a.tile_stride + tile], s);
+    }
+    if (inImage) {
+        // finalize.ts:211-224
+        const float rr = fminf(fmaxf(c0 + T * u.bg[0], 0.0f), 1.0f);
+        const float gg = fminf(fmaxf(c1 + T * u.bg[1], 0.0f), 1.0f);
+        const float bb = fminf(fmaxf(c2 + T * u.bg[2], 0.0f), 1.0f);
+        const float aa = fminf(fmaxf((1.0f - T) + T * u.bg[3], 0.0f), 1.0f);
+        const uint32_t out = dl_sat_u32(rr * 255.0f + 0.5f) | (dl_sat_u32(gg * 255.0f + 0.5f) << 8) |
+                             (dl_sat_u32(bb * 255.0f + 0.5f) << 16) | (dl_sat_u32(aa * 255.0f + 0.5f) << 24);
+        a.outs[v][(uint64_t)y * u.W + x] = out;
+        if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c0, c1, c2, T);
+    }
+}
+
+template <bool kExactExp>
+__global__ void __launch_bounds__(kRasterThreads) rasterize_k(RasterArgs a) {
+    __shared__ float4 s_a[kRasterThreads];
+    __shared__ float4 s_b[kRasterThreads];
+    __shared__ float2 s_c[kRasterThreads];
+    __shared__ uint32_t s_wc[kRasterThreads / 32];
+    __shared__ uint32_t s_item;
+    if (a.work == nullptr) {
+        const uint32_t v = blockIdx.y;
+        if (blockIdx.x >= a.views[v].numTiles) return;
+        raster_tile<kExactExp>(a, v, blockIdx.x, s_a, s_b, s_c, s_wc);
+        return;
+    }
+    // persistent: pull (view, tile) items in the order of the work list
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(a.work_counter, 1u);
+        __syncthreads();
+        const uint32_t i = s_item;
+        __syncthreads();
+        if (i >= a.num_work) return;
+        const uint32_t w = a.work[i];
+        raster_tile<kExactExp>(a, w >> 20, w & 0xfffffu, s_a, s_b, s_c, s_wc);
+        __syncthreads();
+    }
+}
+
+}  // namespace dlr

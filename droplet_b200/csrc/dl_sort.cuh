@@ -1,0 +1,239 @@
+// dl_sort.cuh — stable LSD radix sort of u32 keys with u32 values
+// ("onesweep": one histogram pass, then one scatter pass per digit whose
+// tile offsets come from a decoupled look-back; Adinets & Merrill, 2022).
+//
+// Replaces two reference stages with one device primitive:
+//   * the CPU depth sort (src/spatial/radix-sort.ts:65-117: stable LSD,
+//     4 x 8-bit digits over the order-preserving u32 depth key);
+//   * the CPU stable counting sort of tile pairs (src/render/pipeline.ts:544-578),
+//     itself a replacement for the unstable GPU sorter (src/gpu/radix-sort.ts).
+// Stability is what both callers rely on: ties keep input order, so equal
+// depths stay in index order and each tile's pairs stay in depth-rank order.
+//
+// Batched use: the key array holds S independent segments (one per view);
+// every pass sorts each segment separately in the same launch.  Segment
+// lengths live in device memory so a whole frame can run without a host sync.
+//
+// Every look-back wait is bounded (DL_SPIN_LIMIT polls); on expiry the CTA
+// sets DL_DEVERR_TIMEOUT in the error word, assumes a zero prefix and
+// finishes, so the host reports an error instead of the GPU hanging.
+#pragma once
+#include "dl_common.cuh"
+
+namespace dlsort {
+
+constexpr int kThreads = 256;
+constexpr int kItems = 15;
+constexpr int kTile = kThreads * kItems;     // 3840 keys per CTA tile
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1;
+
+struct Segs {
+    const uint64_t* start;       // element offset of each segment
+    const uint32_t* len;         // element count of each segment (device)
+    uint32_t* tile_base;         // first global tile of each segment (filled by prepare_k)
+    uint32_t* total_tiles;       // sum of tiles (filled by prepare_k)
+    uint32_t num;
+};
+
+// Global tile -> segment (tile_base is ascending; few segments).
+__device__ __forceinline__ uint32_t seg_of_tile(const Segs& s, uint32_t tile) {
+    uint32_t lo = 0, hi = s.num;            // find last seg with tile_base <= tile
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s.tile_base[mid] <= tile) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+static __global__ void prepare_k(Segs s) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t acc = 0;
+    for (uint32_t i = 0; i < s.num; i++) {
+        s.tile_base[i] = acc;
+        acc += (s.len[i] + kTile - 1) / kTile;
+    }
+    *s.total_tiles = acc;
+}
+
+// Digit histograms of all passes: hist[seg][pass][radix] (must be zeroed).
+template <int BITS>
+__global__ void __launch_bounds__(kThreads) hist_k(const uint32_t* __restrict__ keys, Segs s, int passes,
+                                                   int first_shift, uint32_t* __restrict__ hist) {
+    constexpr int RADIX = 1 << BITS;
+    __shared__ uint32_t sh[4 * RADIX];
+    const uint32_t total = *s.total_tiles;
+    for (uint32_t tile = blockIdx.x; tile < total; tile += gridDim.x) {
+        for (int i = threadIdx.x; i < passes * RADIX; i += kThreads) sh[i] = 0;
+        __syncthreads();
+        const uint32_t seg = seg_of_tile(s, tile);
+        const uint32_t lt = tile - s.tile_base[seg];
+        const uint32_t len = s.len[seg];
+        const uint64_t base = s.start[seg];
+        for (int j = 0; j < kItems; j++) {
+            const uint32_t e = lt * kTile + j * kThreads + threadIdx.x;
+            if (e < len) {
+                const uint32_t k = keys[base + e];
+                for (int p = 0; p < passes; p++)
+                    atomicAdd(&sh[p * RADIX + ((k >> (first_shift + p * BITS)) & (RADIX - 1))], 1u);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < passes * RADIX; i += kThreads)
+            if (sh[i]) atomicAdd(&hist[(size_t)seg * passes * RADIX + i], sh[i]);
+        __syncthreads();
+    }
+}
+
+// Exclusive scan of each (segment, pass) histogram row in place.
+template <int BITS>
+__global__ void scan_hist_k(uint32_t* hist, uint32_t rows) {
+    constexpr int RADIX = 1 << BITS;
+    __shared__ uint32_t sh[RADIX];
+    for (uint32_t row = blockIdx.x; row < rows; row += gridDim.x) {
+        uint32_t* h = hist + (size_t)row * RADIX;
+        for (int i = threadIdx.x; i < RADIX; i += blockDim.x) sh[i] = h[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int i = 0; i < RADIX; i++) { const uint32_t v = sh[i]; sh[i] = acc; acc += v; }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < RADIX; i += blockDim.x) h[i] = sh[i];
+        __syncthreads();
+    }
+}
+
+struct Pass {
+    const uint32_t* keys_in;
+    const uint32_t* vals_in;     // NULL: values are the element index within the segment
+    uint32_t* keys_out;          // NULL on a last pass whose keys nobody reads
+    uint32_t* vals_out;
+    Segs segs;
+    const uint32_t* glob_off;    // [seg][passes][radix] exclusive digit offsets
+    uint32_t* status;            // [tile][radix] look-back words, zeroed before the pass
+    uint32_t* counter;           // dynamic tile counter, zeroed before the pass
+    uint32_t* err;
+    int shift, pass, passes;
+};
+
+template <int BITS>
+__global__ void __launch_bounds__(kThreads) pass_k(Pass p) {
+    constexpr int RADIX = 1 << BITS;
+    constexpr int WARPS = kThreads / 32;
+    constexpr uint32_t MASK = RADIX - 1;
+    __shared__ uint32_t s_keys[kTile];
+    __shared__ uint32_t s_vals[kTile];
+    __shared__ uint32_t s_hist[WARPS][RADIX];
+    __shared__ uint32_t s_toff[RADIX];
+    __shared__ uint32_t s_glob[RADIX];
+    __shared__ uint32_t s_wsum[WARPS];
+    __shared__ uint32_t s_tile;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(p.counter, 1u);
+    for (int i = lane; i < RADIX; i += 32) s_hist[warp][i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile >= *p.segs.total_tiles) return;
+    const uint32_t seg = seg_of_tile(p.segs, tile);
+    const uint32_t lt = tile - p.segs.tile_base[seg];
+    const uint32_t len = p.segs.len[seg];
+    const uint64_t base = p.segs.start[seg];
+    const uint32_t t0 = lt * kTile;
+    const uint32_t nValid = min((uint32_t)kTile, len - t0);
+
+    // load (warp-striped) and rank within the warp, in element order
+    uint32_t key[kItems], val[kItems], rank[kItems];
+    int dig[kItems];
+    const uint32_t lmask = dl_lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t e = warp * 32 * kItems + j * 32 + lane;
+        const bool ok = e < nValid;
+        key[j] = ok ? p.keys_in[base + t0 + e] : 0u;
+        val[j] = ok ? (p.vals_in ? p.vals_in[base + t0 + e] : t0 + e) : 0u;
+        dig[j] = ok ? (int)((key[j] >> p.shift) & MASK) : RADIX;
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        const uint32_t peers = __match_any_sync(0xffffffffu, dig[j]);
+        const uint32_t before = (dig[j] < RADIX) ? s_hist[warp][dig[j]] : 0u;
+        __syncwarp();
+        const int leader = 31 - __clz(peers);
+        if (lane == leader && dig[j] < RADIX) s_hist[warp][dig[j]] = before + __popc(peers);
+        __syncwarp();
+        rank[j] = before + __popc(peers & lmask);
+    }
+    __syncthreads();
+
+    // per digit: warp-exclusive offsets and the tile count; publish the aggregate
+    uint32_t cnt = 0;
+    if (tid < RADIX) {
+        for (int w = 0; w < WARPS; w++) { const uint32_t c = s_hist[w][tid]; s_hist[w][tid] = cnt; cnt += c; }
+        uint32_t* st = p.status + (size_t)tile * RADIX + tid;
+        __threadfence();
+        dl_st_volatile(st, (lt == 0 ? kFlagPrefix : kFlagAgg) | cnt);
+    }
+    // exclusive scan of the tile's digit counts -> position of each digit run in the tile
+    {
+        uint32_t v = (tid < RADIX) ? cnt : 0u, inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        if (lane == 31) s_wsum[warp] = inc;
+        __syncthreads();
+        uint32_t wpre = 0;
+        for (int w = 0; w < warp; w++) wpre += s_wsum[w];
+        if (tid < RADIX) s_toff[tid] = wpre + inc - v;
+    }
+    // decoupled look-back for this digit's prefix over earlier tiles of the segment
+    if (tid < RADIX) {
+        uint32_t excl = 0;
+        if (lt > 0) {
+            int64_t q = (int64_t)tile - 1;
+            const int64_t first = (int64_t)p.segs.tile_base[seg];
+            uint32_t spins = 0;
+            while (q >= first) {
+                const uint32_t s = dl_ld_volatile(p.status + (size_t)q * RADIX + tid);
+                const uint32_t flag = s & ~kValMask;
+                if (flag == 0u) {
+                    if (++spins > DL_SPIN_LIMIT) { atomicOr(p.err, DL_DEVERR_TIMEOUT); break; }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += s & kValMask;
+                if (flag == kFlagPrefix) break;
+                q--;
+            }
+            __threadfence();
+            dl_st_volatile(p.status + (size_t)tile * RADIX + tid, kFlagPrefix | ((excl + cnt) & kValMask));
+        }
+        s_glob[tid] = p.glob_off[((size_t)seg * p.passes + p.pass) * RADIX + tid] + excl;
+    }
+    __syncthreads();
+
+    // scatter into shared memory in sorted-within-tile order
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        if (dig[j] < RADIX) {
+            const uint32_t pos = s_toff[dig[j]] + s_hist[warp][dig[j]] + rank[j];
+            s_keys[pos] = key[j];
+            s_vals[pos] = val[j];
+        }
+    }
+    __syncthreads();
+    // coalesced write-out: consecutive threads write consecutive slots of a digit run
+    for (uint32_t i = tid; i < nValid; i += kThreads) {
+        const uint32_t k = s_keys[i];
+        const uint32_t d = (k >> p.shift) & MASK;
+        const uint64_t dst = base + s_glob[d] + (i - s_toff[d]);
+        if (p.keys_out) p.keys_out[dst] = k;
+        p.vals_out[dst] = s_vals[i];
+    }
+}
+
+}  // namespace dlsort

@@ -1,0 +1,155 @@
+/* droplet_b200.h — C ABI of libdroplet_b200.so, the B200 (sm_100a) engine
+ * behind droplet's TypeScript API.
+ *
+ * The TypeScript surface stays as it is (src/index.ts:16-38); a thin shim
+ * calls these entry points through bun:ffi.  Each entry
+ * point cites the reference interface it replaces.  Paths are relative to the
+ * droplet repository.
+ *
+ * Conventions
+ *   - Every function returns an int status: DL_OK (0) or a DL_E_* code; the
+ *     message of the last failure on the calling thread is dl_last_error().
+ *     The shim turns a non-zero status into `throw new Error(msg)`, which is
+ *     how the reference reports setup failures (src/gpu/device.ts:27-41).
+ *   - Host arrays are borrowed read-only for the duration of a call
+ *     (src/render/preprocess.ts:90-138 copies them the same way); outputs are
+ *     written into caller-allocated memory.
+ *   - Handles are not thread-safe: one caller at a time per handle (the
+ *     reference's Renderer shares scratch between calls the same way,
+ *     src/render/pipeline.ts:5-8); distinct handles are independent.
+ */
+#ifndef DROPLET_B200_H
+#define DROPLET_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    DL_OK = 0,
+    DL_E_INVALID_ARG = 1,   /* bad pointer, size or option */
+    DL_E_OOM = 2,           /* device or pinned allocation failed */
+    DL_E_CUDA = 3,          /* a CUDA runtime call failed */
+    DL_E_TIMEOUT = 4,       /* a bounded device-side wait gave up (no hang) */
+    DL_E_CAPACITY = 5,      /* a size exceeds a documented limit */
+    DL_E_NO_DEVICE = 6      /* no usable CUDA device */
+};
+
+enum { DL_PINHOLE = 0, DL_EQUIRECT = 1 };              /* src/types.ts:70 Projection */
+enum { DL_PREC_F32 = 0, DL_PREC_F16 = 1, DL_PREC_BF16 = 2 };
+
+typedef struct dl_device dl_device;
+typedef struct dl_renderer dl_renderer;
+typedef struct dl_scene dl_scene;
+typedef struct dl_vox_result dl_vox_result;
+
+/* src/types.ts:23-32 SplatData: struct of arrays, all float32, N = count.
+ * colors_sh: per Gaussian 3*M channel-major terms (R[M], G[M], B[M]),
+ * M = 0/3/8/15 for sh_bands 0..3 (src/types.ts:35-37); may be NULL. */
+typedef struct dl_splats {
+    uint64_t count;
+    const float* positions;       /* 3N xyz */
+    const float* rotations;       /* 4N [w, x, y, z] */
+    const float* log_scales;      /* 3N */
+    const float* opacity_logits;  /* N */
+    const float* colors_dc;       /* 3N */
+    const float* colors_sh;       /* 3MN or NULL */
+    int32_t sh_bands;             /* 0..3 */
+} dl_splats;
+
+/* src/types.ts:74-82 RenderCamera (JS numbers are f64 here). */
+typedef struct dl_camera {
+    uint32_t width, height;
+    float view[16];               /* world->camera, column-major (Float32Array) */
+    double fov_y, near_plane, far_plane;
+    int32_t projection;           /* DL_PINHOLE or DL_EQUIRECT */
+} dl_camera;
+
+/* src/render/pipeline.ts:43-48 RendererOptions; 0 selects the default. */
+typedef struct dl_renderer_opts {
+    uint32_t chunk_cap;               /* default 200000; results never depend on it */
+    uint32_t max_coverage_per_splat;  /* default 16384 */
+} dl_renderer_opts;
+
+/* src/voxel/voxelize.ts:29-36 VoxelizeOptions. */
+typedef struct dl_vox_opts {
+    double voxel_resolution;      /* default 0.05 when <= 0 is passed with use_defaults */
+    double opacity_cutoff;        /* default 0.1 */
+    int32_t use_defaults;         /* 1: ignore the two fields above */
+    int32_t has_bounds;           /* 1: use bounds_min/bounds_max (opts.bounds) */
+    double bounds_min[3];
+    double bounds_max[3];
+} dl_vox_opts;
+
+/* ---- errors ------------------------------------------------------------ */
+/* Message of the last failure on this thread ("" if none). */
+const char* dl_last_error(void);
+
+/* ---- device: src/gpu/device.ts:27-41 createDevice ---------------------- */
+int dl_device_open(int ordinal, dl_device** out);
+int dl_device_close(dl_device* dev);
+
+/* ---- renderer: src/render/pipeline.ts:76-84 constructor, :581-591 destroy */
+int dl_renderer_create(dl_device* dev, const dl_renderer_opts* opts, dl_renderer** out);
+int dl_renderer_destroy(dl_renderer* r);
+/* Run the renderer's kernels on a caller-provided cudaStream_t (NULL: the
+ * renderer's own stream).  Lets a caller time kernels with its own events. */
+int dl_renderer_set_stream(dl_renderer* r, void* cuda_stream);
+
+/* src/render/pipeline.ts:181-426 Renderer.render(data, camera, background):
+ * writes width*height RGBA8 pixels (finalize.ts packing) into out_rgba.
+ * bg = (r, g, b, a) in [0, 1]; NULL means (0, 0, 0, 1). */
+int dl_render(dl_renderer* r, const dl_splats* data, const dl_camera* cam, const float bg[4],
+              uint8_t* out_rgba, size_t out_len);
+
+/* ---- device-resident scenes and batched views (no reference counterpart:
+ * the reference re-uploads SplatData on every render, pipeline.ts:221-228) */
+int dl_scene_upload(dl_renderer* r, const dl_splats* data, int sh_precision, dl_scene** out);
+int dl_scene_free(dl_scene* s);
+
+enum {
+    DL_BATCH_OUT_DEVICE = 1,      /* outs[i] are device pointers */
+    DL_BATCH_PLAIN = 2,           /* one launch sequence per view, f32 records, static schedule */
+    DL_BATCH_F16_RECORDS = 4,     /* projected conic/alpha/colour stored as f16 */
+    DL_BATCH_NO_GRAPH = 8,        /* launch directly instead of replaying a CUDA graph */
+    DL_BATCH_STATIC = 16,         /* rasterize tiles in launch order, not cost order */
+    DL_BATCH_FAST_EXP = 32        /* hardware ex2 in the rasterizer (+-1 LSB) */
+};
+/* Render n views of one resident scene; outs[i] receives cams[i].width *
+ * cams[i].height RGBA8 pixels (host or device memory, per flags). */
+int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
+                    uint8_t* const* outs, uint32_t flags);
+
+/* ---- voxelizer: src/voxel/voxelize.ts:59-248 voxelize(device, data, opts) */
+int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_opts* opts, dl_vox_result** out);
+/* VoxelizeResult {bounds, numBlocksX/Y/Z} (voxelize.ts:38-45) and the block
+ * count of its BlockMaskBuffer (block-mask-buffer.ts:57).  dims may be
+ * -Infinity for an empty input, as in the reference. */
+int dl_vox_result_info(const dl_vox_result* res, double bounds_min[3], double bounds_max[3],
+                       double dims[3], uint64_t* block_count);
+/* BlockMaskBuffer.blocks (block-mask-buffer.ts:27) in the reference's order:
+ * flat block index, low 32 voxel bits, high 32 voxel bits. */
+int dl_vox_result_copy(const dl_vox_result* res, uint32_t* block_idx, uint32_t* mask_lo, uint32_t* mask_hi);
+int dl_vox_result_free(dl_vox_result* res);
+
+/* ---- instrumentation (no reference counterpart) ------------------------ */
+/* Copy a named device array of the last single-view render into dst (cap
+ * bytes); *bytes receives its size.  Names: "depth_keys", "sorted_idx",
+ * "recA", "recBC", "bbox", "tile_off", "pair_vals", "accum", "nvis", "npairs". */
+int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst, size_t cap, size_t* bytes);
+/* Per-stage device time (ms) accumulated while profiling is on, in the order
+ * project, depth_sort, emit, tile_offsets, pair_sort, rasterize. */
+int dl_renderer_set_profiling(dl_renderer* r, int on);
+int dl_renderer_stage_times(dl_renderer* r, double* ms, int n);
+/* Kernel launches issued by the last render call. */
+int dl_renderer_launch_count(dl_renderer* r, uint64_t* count);
+/* Keep the last single-view frame's f32 accumulator (r, g, b, T) for "accum". */
+int dl_renderer_set_debug(dl_renderer* r, int keep_intermediates);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DROPLET_B200_H */

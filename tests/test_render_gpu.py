@@ -1,0 +1,168 @@
+"""GPU parity of the renderer against the oracle, through the C ABI.
+
+Integer stages (depth keys, depth order, tile counts, tile offsets, per-tile
+pair lists) must be bit-exact, and so must the projected records, the f32
+accumulator and the RGBA8 bytes: the kernels evaluate the shaders' f32
+expressions in the same order with FMA contraction off and share dl_math.h's
+exp/atan2/asin with the oracle.  Variants that trade exactness for speed (f16
+records, hardware exp) are held to the stated tolerance: RGBA8 within +-1 LSB
+on >= 99.9% of pixels."""
+import math
+
+import numpy as np
+import pytest
+
+import droplet_b200 as dl
+from droplet_b200 import _lib, synth
+from droplet_b200.types import RenderCamera, SplatData, mat4LookAt
+from oracle import oracle as O
+from parity import ORACLE_FIELDS, assert_render_parity, gpu_render_debug
+
+pytestmark = pytest.mark.gpu
+
+
+def nonblack(rgba):
+    p = rgba.reshape(-1, 4)
+    return int(((p[:, 0] > 5) | (p[:, 1] > 5) | (p[:, 2] > 5)).sum())
+
+
+def check(renderer, data, cam, bg=(0.0, 0.0, 0.0, 1.0), max_cov=16384):
+    g = gpu_render_debug(renderer, data, cam, bg)
+    o = O.render(data, cam, bg, maxCoverage=max_cov, chunkCap=1 << 30, fields=ORACLE_FIELDS)
+    assert_render_parity(g, o, max_cov)
+    return g, o
+
+
+# ---- the reference's browser tests (examples/browser/test.ts), on the GPU path
+def test_empty_scene(renderer):
+    rgba = renderer.render(SplatData.empty(), synth.front_camera())
+    assert nonblack(rgba) == 0 and rgba.reshape(-1, 4)[0, 3] == 255
+
+
+def test_one_splat(renderer):
+    g, o = check(renderer, synth.one_splat((0, 0, 0)), synth.front_camera())
+    img = g["rgba"].reshape(128, 128, 4)[..., 0]
+    assert img[64, 64] > 100 and abs(int(img[64, 54]) - int(img[64, 74])) < 10
+
+
+def test_three_splats_and_occlusion(renderer):
+    d = SplatData(3, [0, 0, 1, 0.5, 0, 0.8, -0.5, 0.3, 0.8], [1, 0, 0, 0] * 3, [-2.5] * 9, [3, 3, 3],
+                  [0.5, -0.5, -0.5, -0.5, 0.5, -0.5, -0.5, -0.5, 0.5])
+    check(renderer, d, synth.front_camera(256, 256))
+    d2 = SplatData(2, [0, 0, 1, 0, 0, -1], [1, 0, 0, 0] * 2, [-2.5] * 6, [4, 4], [0.5, -0.5, -0.5, -0.5, 0.5, -0.5])
+    g, _ = check(renderer, d2, synth.front_camera())
+    px = g["rgba"].reshape(128, 128, 4)[64, 64]
+    assert px[0] > 200 and px[1] < 50
+
+
+def test_sphere_disc(renderer):
+    g, _ = check(renderer, synth.many_splats(5000, "sphere"), synth.front_camera(256, 256))
+    assert 10000 < nonblack(g["rgba"]) < 30000
+
+
+def test_chunk_cap_has_no_effect(device):
+    d = synth.many_splats(200_000, "random")
+    a = dl.Renderer(device).render(d, synth.front_camera(64, 64))
+    b = dl.Renderer(device, {"chunkCap": 50_000}).render(d, synth.front_camera(64, 64))
+    o = O.render(d, synth.front_camera(64, 64), chunkCap=50_000)
+    assert np.array_equal(a, b) and np.array_equal(a, o["rgba"])
+
+
+def test_dense_large_splats(renderer):
+    n = 200_000
+    rng = np.random.default_rng(7)
+    pos = ((rng.random((n, 3)) - 0.5) * 0.1).astype(np.float32)
+    rot = np.zeros((n, 4), np.float32); rot[:, 0] = 1
+    dc = np.zeros((n, 3), np.float32); dc[:, 0] = 0.5
+    d = SplatData(n, pos, rot, np.full((n, 3), -2.5, np.float32), np.zeros(n, np.float32), dc)
+    g, _ = check(renderer, d, synth.front_camera(256, 256))
+    assert nonblack(g["rgba"]) > 100
+
+
+def test_one_million_random(renderer):
+    g, _ = check(renderer, synth.many_splats(1_000_000, "random"), synth.front_camera(256, 256))
+    assert nonblack(g["rgba"]) > 1000
+
+
+# ---- seeded workloads
+def test_plain_100k_720p_full_size(renderer):
+    check(renderer, synth.plain_100k(), synth.plain_100k_camera(), bg=(0.1, 0.2, 0.3, 0.5))
+
+
+@pytest.mark.parametrize("bands", [1, 2, 3])
+def test_sh_bands_1080p(renderer, bands):
+    d = synth.cluster_scene(150_000, seed=20 + bands, clusters=32, extent=10.0, bands=bands)
+    check(renderer, d, synth.pinhole(1920, 1080, (0.0, 2.0, 12.0)))
+
+
+def test_equirect(renderer):
+    d = synth.cluster_scene(150_000, seed=31, clusters=32, extent=10.0, bands=3)
+    check(renderer, d, synth.sh3_3m_cameras()[1])
+
+
+def test_max_coverage_truncation(device):
+    r = dl.Renderer(device, {"maxCoveragePerSplat": 7})
+    d = synth.cluster_scene(20_000, seed=4, clusters=4, extent=1.0, log_lo=0.05, log_hi=0.3)
+    check(r, d, synth.pinhole(640, 360, (0.0, 0.0, 3.0)), max_cov=7)
+
+
+def test_offscreen_left_top_splats_bin_to_edge_tiles(renderer):
+    # u32() saturation in project.ts:224-227: off-screen splats to the left/top
+    # still count tiles in column/row 0; the pair lists must reproduce that.
+    rng = np.random.default_rng(3)
+    n = 5000
+    pos = np.c_[rng.uniform(-30, 30, n), rng.uniform(-30, 30, n), rng.uniform(-5, 1, n)].astype(np.float32)
+    rot = np.zeros((n, 4), np.float32); rot[:, 0] = 1
+    d = SplatData(n, pos, rot, np.full((n, 3), -2.0, np.float32), np.ones(n, np.float32),
+                  rng.normal(0, .5, (n, 3)).astype(np.float32))
+    g, o = check(renderer, d, synth.pinhole(320, 240, (0.0, 0.0, 4.0)))
+    assert o["n_pairs"] > 0
+
+
+def test_near_far_and_degenerate(renderer):
+    rng = np.random.default_rng(9)
+    n = 4000
+    pos = np.c_[rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(3.0, 5.0, n)].astype(np.float32)
+    q = rng.normal(0, 1, (n, 4)); q /= np.linalg.norm(q, axis=1, keepdims=True)
+    ls = rng.uniform(-12, 1, (n, 3)).astype(np.float32)          # needles, sub-pixel and screen-filling
+    d = SplatData(n, pos, q.astype(np.float32), ls, rng.normal(0, 3, n).astype(np.float32),
+                  rng.normal(0, .5, (n, 3)).astype(np.float32))
+    cam = RenderCamera(300, 200, mat4LookAt((0, 0, 4), (0, 0, 0), (0, 1, 0)), math.pi / 3, 0.5, 3.9)
+    check(renderer, d, cam)
+
+
+def test_odd_sizes(renderer):
+    d = synth.plain_100k(30_000)
+    for w, h in ((1, 1), (17, 33), (255, 1), (1000, 7)):
+        check(renderer, d, synth.pinhole(w, h, (0.0, 0.0, 4.0)))
+
+
+# ---- batched path: same pixels as the single-view path
+def test_batch_matches_single_views(device, renderer):
+    d = synth.cluster_scene(200_000, seed=12, clusters=64, extent=10.0, bands=3)
+    cams = synth.ring_cameras(6, resolutions=[(320, 180), (640, 360), (500, 400)])
+    single = [renderer.render(d, c) for c in cams]
+    r2 = dl.Renderer(device)
+    sc = r2.upload(d)
+    plain = r2.render_batch(sc, cams, flags=_lib.DL_BATCH_PLAIN)
+    batched = r2.render_batch(sc, cams)
+    for a, b, c in zip(single, plain, batched):
+        assert np.array_equal(a, b) and np.array_equal(a, c)
+
+
+def _lsb_share(a, b):
+    diff = np.abs(a.astype(np.int16) - b.astype(np.int16)).reshape(-1, 4).max(axis=1)
+    return float((diff <= 1).mean()), int(diff.max())
+
+
+@pytest.mark.parametrize("flags,prec", [(_lib.DL_BATCH_F16_RECORDS, "f32"), (_lib.DL_BATCH_F16_RECORDS, "f16"),
+                                        (_lib.DL_BATCH_F16_RECORDS, "bf16"), (_lib.DL_BATCH_FAST_EXP, "f32")])
+def test_precision_variants_within_one_lsb(device, flags, prec):
+    d = synth.cluster_scene(200_000, seed=13, clusters=64, extent=10.0, bands=3)
+    cam = synth.pinhole(960, 540, (0.0, 2.0, 12.0))
+    o = O.render(d, cam)["rgba"]
+    r = dl.Renderer(device)
+    sc = r.upload(d, prec)
+    got = r.render_batch(sc, [cam], flags=flags)[0]
+    share, worst = _lsb_share(got, o)
+    assert share >= 0.999, (share, worst)
