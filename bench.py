@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: Mpix/s of the batched renderer on the 64-view ring workload.
+
+Workload (one "step"): 64 cameras on a ring of radius 12 at height 2 looking at
+the origin, resolutions cycling 640x360 / 1280x720 / 1920x1080 / 2560x1440
+(110.6 Mpix), rendering one device-resident 3M-Gaussian SH-band-3 scene (256
+seeded clusters in [-10, 10]^3).  Synthetic, seeded data (numpy PCG64).
+
+  value  Mpix/s of the batched path with the scene resident in HBM and images
+         written to device memory, timed with CUDA events on the launching
+         stream, max over ranks.
+  e2e    the same metric through the reference-facing call (dl_render_many:
+         SplatData from pinned host memory uploaded every step, all views
+         rendered, every RGBA8 image copied back to pinned host memory).
+  plain  the plain path (one launch sequence per view, f32 records, exact exp)
+         on the same GPU, reported beside value for the headline ratio.
+
+--impl reference times the reference's algorithm on the host cores instead:
+the C++ restatement of droplet's CPU stages and WGSL shaders (oracle/), since
+the reference itself only runs on WebGPU, which this machine does not have.
+Multi-GPU (torchrun): every rank renders the full batch (views are
+independent, no collective on the data path); scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpix/s @3M splats 1080p SH3, batched+learned vs plain, same B200, ≤1 LSB"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--views", type=int, default=64)
+    p.add_argument("--splats", type=int, default=3_000_000)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    from droplet_b200 import synth
+    data = synth.sh3_3m(args.splats)
+    cams = synth.ring_cameras(args.views)
+    return data, cams
+
+
+def config(args, cams, extra=None):
+    pix = sum(c.width * c.height for c in cams)
+    c = {"workload": f"ring{len(cams)}: {len(cams)} views cycling 640x360/1280x720/1920x1080/2560x1440 "
+                     f"({pix / 1e6:.1f} Mpix) of a {args.splats / 1e6:g}M-Gaussian SH3 scene",
+         "splats": args.splats, "views": len(cams), "pixels_per_step": pix, "sh_bands": 3, "tile": "16x16",
+         "l2": "inputs larger than L2 (scene 708 MB, per-view intermediates > 1 GB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)                  # let the sampler start before the timed region
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return None
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the rasterizer from the committed ncu summary."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "rasterize_ring64.json"))).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(data, cams):
+    """Bounded sample on the host cores: the oracle renders the 1920x1080 view."""
+    from oracle import oracle as O
+    cam = next(c for c in cams if c.width == 1920)
+    t = time.perf_counter()
+    O.render(data, cam)
+    dt = time.perf_counter() - t
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": cam.width * cam.height / dt / 1e6, "unit": "Mpix/s", "cores": cores, "kind": "port",
+            "sample": f"oracle (C++ restatement, OpenMP) renders 1 view {cam.width}x{cam.height} of the "
+                      f"{data.count}-Gaussian SH3 scene in {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    data, cams = workload(args)
+    order = list(cams[:4])            # one view of each resolution, cycled
+
+    def step(k):
+        c = order[k % len(order)]
+        O.render(data, c)
+        return c.width * c.height
+
+    for k in range(args.warmup):
+        step(k)
+    t = time.perf_counter()
+    pix = sum(step(args.warmup + k) for k in range(args.steps))
+    dt = time.perf_counter() - t
+    v = pix / dt / 1e6
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {"metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "impl": "reference",
+            "config": config(args, cams, {"sample": "each step renders one view, cycling 640x360, 1280x720, "
+                                                    "1920x1080, 2560x1440"}),
+            "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": cores, "kind": "port",
+                             "sample": "the oracle (C++ restatement of droplet's TS CPU stages + WGSL shaders; "
+                                       "WebGPU unavailable on this box), one view per step"},
+            "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import droplet_b200 as dl
+    from droplet_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    data, cams = workload(args)
+    pix = sum(c.width * c.height for c in cams)
+    dev = dl.createDevice({"ordinal": local_rank})
+    r = dl.Renderer(dev)
+    stream = torch.cuda.current_stream()
+    r.set_stream(stream.cuda_stream)
+    FAST = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
+    scene = r.upload(data, "f16")
+    outs = [torch.empty(c.width * c.height * 4, dtype=torch.uint8, device="cuda") for c in cams]
+    ptrs = [o.data_ptr() for o in outs]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    batched = lambda: r.render_batch(scene, cams, flags=FAST, outs=ptrs)
+    for _ in range(args.warmup):
+        batched()
+    with ClockSampler(local_rank) as clk:
+        ms = timed(batched, args.steps)
+    clocks = clk.summary()
+    launches = r.launch_count() * args.steps
+    value = world * pix * args.steps / (ms / 1e3) / 1e6
+
+    # per-stage device times and the rasterizer's work (outside the timed region)
+    r.set_profiling(True)
+    batched()
+    stages = r.stage_times()
+    r.set_profiling(False)
+    r.render_batch(scene, cams, flags=FAST | _lib.DL_BATCH_COUNT_EVALS, outs=ptrs)
+    evals = int(r.debug_get("evals", np.uint64)[0])
+    npairs = int(r.debug_get("npairs", np.uint64).sum())
+
+    plain_value = exact_value = None
+    if not args.no_plain:
+        half = max(1, args.steps // 2)
+        plain = lambda: r.render_batch(scene32, cams, flags=_lib.DL_BATCH_PLAIN, outs=ptrs)
+        exact = lambda: r.render_batch(scene32, cams, flags=0, outs=ptrs)
+        scene32 = r.upload(data, "f32")
+        plain()
+        plain_value = world * pix * half / (timed(plain, half) / 1e3) / 1e6
+        exact()
+        exact_value = world * pix * half / (timed(exact, half) / 1e3) / 1e6
+        scene32.destroy()
+
+    e2e = None
+    if not args.no_e2e:
+        # host SplatData in pinned memory, images back into pinned memory, every step
+        keep, fields = [], {}
+        for k in ("positions", "rotations", "logScales", "opacityLogits", "colorsDC", "colorsSH"):
+            t = torch.from_numpy(np.ascontiguousarray(getattr(data, k))).pin_memory()
+            keep.append(t)
+            fields[k] = t.numpy()
+        hdata = dl.SplatData(data.count, shBands=data.shBands, **fields)
+        houts = [torch.empty(c.width * c.height * 4, dtype=torch.uint8).pin_memory() for c in cams]
+        hptrs = [h.data_ptr() for h in houts]
+        r2 = dl.Renderer(dev)
+        r2.set_stream(stream.cuda_stream)
+        many = lambda: r2.render_many(hdata, cams, flags=FAST, outs=hptrs)
+        many()
+        half = max(1, args.steps // 2)
+        ems = timed(many, half)
+        h2d = sum(a.nbytes for a in fields.values())
+        e2e = {"value": world * pix * half / (ems / 1e3) / 1e6, "unit": "Mpix/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(pix * 4),
+               "call": "dl_render_many (host SplatData -> host RGBA8)"}
+        r2.destroy()
+
+    if rank != 0:
+        return
+    pk = peaks()
+    rast_ms = stages["rasterize"]
+    rec_bytes = 4 + 16 + 16                    # pair value + f32 screen record + f16 conic/alpha/colour
+    alg_bytes = npairs * rec_bytes + pix * 4
+    achieved = alg_bytes / (rast_ms / 1e3) / 1e9
+    hbm = pk["hbm_gbs"] if pk else 6650.0
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    flops = evals * 20
+    roof = {"kernel": "rasterize_k (fused finalize)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": profile_traffic(),
+            "peak_source": "measured" if pk else "fallback",
+            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": rast_ms,
+            "compute": {"evaluated_pairs": evals, "flops_per_eval": 20,
+                        "achieved_tflops": flops / (rast_ms / 1e3) / 1e12, "fp32_peak_tflops_at_clock": fp32_peak,
+                        "frac": flops / (rast_ms / 1e3) / 1e12 / fp32_peak}}
+    line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "config": config(args, cams, {"mode": "batched: one launch per stage for all views, f16 scene SH "
+                                                  "and records, hardware exp2 (+-1 LSB)",
+                                          "parallelism": f"views replicated per GPU x{world}"}),
+            "plain_value": plain_value, "exact_value": exact_value,
+            "vs_plain": (value / plain_value) if plain_value else None,
+            "stage_ms": stages, "pairs_per_step": npairs, "gpu_launches": launches, "clocks": clocks,
+            "roofline": roof, "e2e": e2e}
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(data, cams)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -21,6 +21,7 @@ DL_BATCH_F16_RECORDS = 4
 DL_BATCH_NO_GRAPH = 8
 DL_BATCH_STATIC = 16
 DL_BATCH_FAST_EXP = 32
+DL_BATCH_COUNT_EVALS = 64
 
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = [
@@ -28,7 +29,7 @@ EXPORTS = [
     "dl_renderer_set_stream", "dl_render", "dl_scene_upload", "dl_scene_free", "dl_render_batch",
     "dl_voxelize", "dl_vox_result_info", "dl_vox_result_copy", "dl_vox_result_free",
     "dl_renderer_debug_get", "dl_renderer_set_profiling", "dl_renderer_stage_times",
-    "dl_renderer_launch_count", "dl_renderer_set_debug",
+    "dl_renderer_launch_count", "dl_renderer_set_debug", "dl_render_many",
 ]
 
 
@@ -84,6 +85,7 @@ def load():
         "dl_scene_upload": [vp, P(DlSplats), i, P(vp)],
         "dl_scene_free": [vp],
         "dl_render_batch": [vp, vp, P(DlCamera), i, P(ctypes.c_float), P(vp), ctypes.c_uint32],
+        "dl_render_many": [vp, P(DlSplats), P(DlCamera), i, P(ctypes.c_float), P(vp), ctypes.c_uint32],
         "dl_voxelize": [vp, P(DlSplats), P(DlVoxOpts), P(vp)],
         "dl_vox_result_info": [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_uint64)],
         "dl_vox_result_copy": [vp, vp, vp, vp],

@@ -140,6 +140,23 @@ class Renderer:
                                     _bg(background), out.ctypes.data if out.size else None, out.size))
         return out
 
+    def render_many(self, data: SplatData, cameras: Sequence[RenderCamera], background=None, flags: int = 0,
+                    outs: Optional[Sequence[int]] = None) -> Optional[List[np.ndarray]]:
+        """render() for several cameras of one SplatData in one call (one upload,
+        one batched frame).  outs: optional host pointers (e.g. pinned buffers)."""
+        n = len(cameras)
+        cams = (_lib.DlCamera * n)(*[_camera(c) for c in cameras])
+        ptrs = (ctypes.c_void_p * n)()
+        host = None
+        if outs is None:
+            host = [np.empty(int(c.width) * int(c.height) * 4, np.uint8) for c in cameras]
+            outs = [a.ctypes.data for a in host]
+        for k, p in enumerate(outs):
+            ptrs[k] = int(p)
+        check(_lib.load().dl_render_many(self.handle, ctypes.byref(_splats(data)), cams, n, _bg(background), ptrs,
+                                         flags))
+        return host
+
     # ---- device-resident scenes and batches
     def upload(self, data: SplatData, precision: str = "f32") -> Scene:
         prec = {"f32": _lib.DL_PREC_F32, "f16": _lib.DL_PREC_F16, "bf16": _lib.DL_PREC_BF16}[precision]

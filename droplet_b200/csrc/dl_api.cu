@@ -74,7 +74,7 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
                       &r->vals0, &r->vals1, &r->recA, &r->recBC, &r->recH, &r->bbox, &r->nvis, &r->depthHist,
                       &r->sortStatus, &r->pairBase, &r->pairCap, &r->pkeys0, &r->pkeys1, &r->pvals0, &r->pvals1,
                       &r->npairs, &r->emitStatus, &r->tileCount, &r->tileOff, &r->pairSegLen, &r->pairSegTileBase,
-                      &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->own_scene.mem};
+                      &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->evalCount, &r->own_scene.mem};
     for (DevBuf* b : bufs) b->release();
     if (r->h_views) cudaFreeHost(r->h_views);
     if (r->h_u64) cudaFreeHost(r->h_u64);
@@ -165,6 +165,17 @@ extern "C" int dl_scene_free(dl_scene* s) {
 }
 
 extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
+                               uint8_t* const* outs, uint32_t flags);
+
+extern "C" int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
+                              uint8_t* const* outs, uint32_t flags) {
+    if (!r || !data) { dl_set_error("dl_render_many: NULL argument"); return DL_E_INVALID_ARG; }
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    DL_TRY(dl_upload_scene(&r->own_scene, data, DL_PREC_F32, r->stream));
+    return dl_render_batch(r, &r->own_scene, cams, n, bg, outs, flags & ~(uint32_t)DL_BATCH_OUT_DEVICE);
+}
+
+extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
                                uint8_t* const* outs, uint32_t flags) {
     if (!r || !s || !cams || !outs || n < 0) { dl_set_error("dl_render_batch: bad argument"); return DL_E_INVALID_ARG; }
     if (n == 0) return DL_OK;
@@ -215,16 +226,15 @@ extern "C" int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst
     uint64_t scalar = 0;
     bool host = false;
     DL_CK(cudaSetDevice(r->dev->ordinal));
-    if (s == "nvis" || s == "npairs") {
-        if (s == "nvis") {
-            uint32_t v = 0;
-            DL_CK(cudaMemcpy(&v, r->nvis.p, 4, cudaMemcpyDeviceToHost));
-            scalar = v;
-        } else {
-            DL_CK(cudaMemcpy(&scalar, r->npairs.p, 8, cudaMemcpyDeviceToHost));
-        }
+    if (s == "nvis") {
+        uint32_t v = 0;
+        DL_CK(cudaMemcpy(&v, r->nvis.p, 4, cudaMemcpyDeviceToHost));
+        scalar = v;
         src = &scalar; n = 8; host = true;
-    } else if (s == "depth_keys") { src = r->keys0.p; n = 4ull * r->last_n; }
+    } else if (s == "evals") {
+        if (r->evalCount.p) DL_CK(cudaMemcpy(&scalar, r->evalCount.p, 8, cudaMemcpyDeviceToHost));
+        src = &scalar; n = 8; host = true;
+    } else if (s == "npairs") { src = r->npairs.p; n = 8ull * r->last_V;    } else if (s == "depth_keys") { src = r->keys0.p; n = 4ull * r->last_n; }
     else if (s == "sorted_idx") { src = r->vals0.p; n = 4ull * r->last_n; }
     else if (s == "recA") { src = r->recA.p; n = 16ull * r->last_n; }
     else if (s == "recBC") { src = r->recBC.p; n = 32ull * r->last_n; }

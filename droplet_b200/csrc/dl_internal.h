@@ -88,6 +88,8 @@ struct dl_renderer {
     uint32_t last_n = 0, last_stride = 0, last_T = 0, last_W = 0, last_H = 0, last_pairs_final = 0;
     int last_rec_kind = 0;
     uint32_t* last_final_vals = nullptr;
+    uint32_t last_V = 0;
+    DevBuf evalCount;
     DevBuf rgba;                        // device output of dl_render()
     bool keep_accum = false;
     bool keep_depth_keys = true;

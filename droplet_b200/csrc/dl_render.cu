@@ -165,6 +165,11 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     const uint64_t stride = round_up(std::max<uint32_t>(N, 1), 64);
     const bool f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
     const bool fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
+    const bool countEvals = (flags & DL_BATCH_COUNT_EVALS) != 0;
+    if (countEvals) {
+        DL_TRY(r->evalCount.ensure(8));
+        DL_CK(cudaMemsetAsync(r->evalCount.p, 0, 8, st));
+    }
     uint32_t maxT = 1;
     for (uint32_t v = 0; v < V; v++) maxT = std::max(maxT, hv[v].numTiles);
     const uint32_t TS = maxT + 1;
@@ -389,6 +394,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         ra.view_stride = stride;
         ra.outs = r->outs.as<uint32_t*>();
         ra.accum = (r->keep_accum && V == 1) ? r->accum.as<float4>() : nullptr;
+        ra.eval_count = countEvals ? r->evalCount.as<unsigned long long>() : nullptr;
         const dim3 rg(maxT, V);
         if (fastExp) dlr::rasterize_k<false><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
         else dlr::rasterize_k<true><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
@@ -426,6 +432,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         r->last_pairs_final = (uint32_t)r->h_u64[0];
         r->last_rec_kind = f16rec ? 1 : 0;
         r->last_final_vals = finalVals;
+        r->last_V = V;
         return DL_OK;
     }
     dl_set_error("pair buffers overflowed repeatedly");

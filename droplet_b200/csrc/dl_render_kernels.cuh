@@ -526,7 +526,7 @@ struct RasterArgs {
     const uint32_t* work;          // optional persistent work list: (v << 20) | tile
     uint32_t num_work;
     uint32_t* work_counter;
-    const float* pixel_cost;       // unused placeholder for cost logging
+    unsigned long long* eval_count;   // optional: total evaluated (pixel, splat) pairs
     uint32_t* tile_evals;          // optional [V][tile_stride] per-tile evaluated-pair counts
 };
 
@@ -621,11 +621,14 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uin
         }
         if (__syncthreads_count(!done) == 0) break;
     }
-    if (a.tile_evals) {
+    if (a.tile_evals || a.eval_count) {
         uint32_t s = evals;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0 && s) atomicAdd(&a.tile_evals[(uint64_t)v * a.tile_stride + tile], s);
+        if (lane == 0 && s) {
+            if (a.tile_evals) atomicAdd(&a.tile_evals[(uint64_t)v * a.tile_stride + tile], s);
+            if (a.eval_count) atomicAdd(a.eval_count, (unsigned long long)s);
+        }
     }
     if (inImage) {
         // finalize.ts:211-224

@@ -116,12 +116,20 @@ enum {
     DL_BATCH_F16_RECORDS = 4,     /* projected conic/alpha/colour stored as f16 */
     DL_BATCH_NO_GRAPH = 8,        /* launch directly instead of replaying a CUDA graph */
     DL_BATCH_STATIC = 16,         /* rasterize tiles in launch order, not cost order */
-    DL_BATCH_FAST_EXP = 32        /* hardware ex2 in the rasterizer (+-1 LSB) */
+    DL_BATCH_FAST_EXP = 32,       /* hardware ex2 in the rasterizer (+-1 LSB) */
+    DL_BATCH_COUNT_EVALS = 64     /* count evaluated (pixel, splat) pairs ("evals") */
 };
 /* Render n views of one resident scene; outs[i] receives cams[i].width *
  * cams[i].height RGBA8 pixels (host or device memory, per flags). */
 int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
                     uint8_t* const* outs, uint32_t flags);
+
+/* Renderer.render(data, camera, bg) (src/render/pipeline.ts:181-426) for n
+ * cameras of one host SplatData in one call: the splats are uploaded into the
+ * renderer's own grow-only scene buffer, all views are rendered as one batch,
+ * and each RGBA8 image is copied to outs[i] (host memory). */
+int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
+                   uint8_t* const* outs, uint32_t flags);
 
 /* ---- voxelizer: src/voxel/voxelize.ts:59-248 voxelize(device, data, opts) */
 int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_opts* opts, dl_vox_result** out);
@@ -138,7 +146,8 @@ int dl_vox_result_free(dl_vox_result* res);
 /* ---- instrumentation (no reference counterpart) ------------------------ */
 /* Copy a named device array of the last single-view render into dst (cap
  * bytes); *bytes receives its size.  Names: "depth_keys", "sorted_idx",
- * "recA", "recBC", "bbox", "tile_off", "pair_vals", "accum", "nvis", "npairs". */
+ * "recA", "recBC", "bbox", "tile_off", "pair_vals", "accum", "nvis", "npairs"
+ * (one u64 per view of the last frame), "evals" (u64, with DL_BATCH_COUNT_EVALS). */
 int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst, size_t cap, size_t* bytes);
 /* Per-stage device time (ms) accumulated while profiling is on, in the order
  * project, depth_sort, emit, tile_offsets, pair_sort, rasterize. */
