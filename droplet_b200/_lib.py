@@ -30,6 +30,7 @@ EXPORTS = [
     "dl_voxelize", "dl_vox_result_info", "dl_vox_result_copy", "dl_vox_result_free",
     "dl_renderer_debug_get", "dl_renderer_set_profiling", "dl_renderer_stage_times",
     "dl_renderer_launch_count", "dl_renderer_set_debug", "dl_render_many",
+    "dl_render_static",
 ]
 
 
@@ -86,6 +87,7 @@ def load():
         "dl_scene_free": [vp],
         "dl_render_batch": [vp, vp, P(DlCamera), i, P(ctypes.c_float), P(vp), ctypes.c_uint32],
         "dl_render_many": [vp, P(DlSplats), P(DlCamera), i, P(ctypes.c_float), P(vp), ctypes.c_uint32],
+        "dl_render_static": [P(DlSplats), P(DlCamera), P(ctypes.c_float), ctypes.c_uint32, vp, ctypes.c_size_t],
         "dl_voxelize": [vp, P(DlSplats), P(DlVoxOpts), P(vp)],
         "dl_vox_result_info": [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_uint64)],
         "dl_vox_result_copy": [vp, vp, vp, vp],

@@ -438,3 +438,258 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     dl_set_error("pair buffers overflowed repeatedly");
     return DL_E_CAPACITY;
 }
+
+// ============================================================================
+// dl_render_static: the single-view render with every piece of device scratch
+// taken from one fixed, file-scope device array instead of cudaMalloc.
+//
+// Who needs it: code that runs inside a host application which owns all of
+// the GPU's memory (an engine or framework that reserves the device up front
+// with its own allocator and forbids foreign cudaMalloc/cudaFree), or a
+// real-time loop that may not allocate after start-up.  Such callers can still
+// render a small scene: this path allocates nothing, neither device memory nor
+// pinned host memory; it only copies the caller's host arrays into the array
+// below and the finished image back out.
+//
+// Limits (checked before anything runs, DL_E_CAPACITY with a message):
+//   at most kStaticMaxSplats Gaussians, kStaticMaxPixels output pixels,
+//   kStaticMaxTiles 16x16 tiles and kStaticMaxPairs tile pairs.
+// The array is kStaticBytes (16 MiB) on every GPU that loads this library,
+// held until the process exits.
+//
+// Sharing: every call on a device uses the same array and leaves the last
+// call's contents in it; everything a call reads is written or cleared by that
+// call first.  Calls whose GPU work overlaps (two host threads, or calls on
+// different streams of one device) race on the array and must be serialised
+// by the caller.  The first call on each device looks up the array's device
+// address (cudaGetSymbolAddress) with that device current; make that first
+// call before any stream capture on the device.
+// ============================================================================
+namespace {
+
+constexpr uint32_t kStaticMaxSplats = 16384;
+constexpr uint64_t kStaticMaxPixels = 1280ull * 720ull;
+constexpr uint32_t kStaticMaxTiles = 4096;
+constexpr uint64_t kStaticMaxPairs = 1ull << 18;
+constexpr size_t kStaticBytes = 16ull << 20;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+constexpr int kStaticMaxDevices = 64;
+unsigned char* g_static_addr[kStaticMaxDevices] = {};
+
+// Carves 256-byte-aligned pieces out of the array, in call order.
+struct Carver {
+    unsigned char* base;
+    size_t off = 0;
+    template <typename T> T* take(size_t bytes) {
+        T* p = reinterpret_cast<T*>(base + off);
+        off = (off + bytes + 255) / 256 * 256;
+        return p;
+    }
+};
+
+}  // namespace
+
+extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg[4],
+                                uint32_t max_coverage, uint8_t* out_rgba, size_t out_len) {
+    if (!data || !cam) { dl_set_error("dl_render_static: NULL argument"); return DL_E_INVALID_ARG; }
+    const uint64_t pixels = (uint64_t)cam->width * cam->height;
+    if (pixels == 0) return DL_OK;
+    if (!out_rgba || out_len < pixels * 4) {
+        dl_set_error("dl_render_static: output buffer smaller than width*height*4");
+        return DL_E_INVALID_ARG;
+    }
+    if (data->count > kStaticMaxSplats) {
+        dl_set_error("dl_render_static: at most " + std::to_string(kStaticMaxSplats) + " Gaussians (got " +
+                     std::to_string(data->count) + ")");
+        return DL_E_CAPACITY;
+    }
+    if (pixels > kStaticMaxPixels) {
+        dl_set_error("dl_render_static: at most " + std::to_string(kStaticMaxPixels) + " pixels per image");
+        return DL_E_CAPACITY;
+    }
+    DlView v;
+    DL_TRY(dl_make_view(cam, bg, max_coverage ? max_coverage : 16384u, &v));
+    if (v.numTiles > kStaticMaxTiles) {
+        dl_set_error("dl_render_static: at most " + std::to_string(kStaticMaxTiles) + " 16x16 tiles per image");
+        return DL_E_CAPACITY;
+    }
+    if (data->sh_bands < 0 || data->sh_bands > 3) { dl_set_error("sh_bands must be 0..3"); return DL_E_INVALID_ARG; }
+    const uint64_t n = data->count;
+    if (n > 0 && (!data->positions || !data->rotations || !data->log_scales || !data->opacity_logits || !data->colors_dc)) {
+        dl_set_error("splats: a required array is NULL");
+        return DL_E_INVALID_ARG;
+    }
+    int dev = 0;
+    DL_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices) { dl_set_error("dl_render_static: device ordinal too large"); return DL_E_CAPACITY; }
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        DL_CK(cudaGetSymbolAddress(&p, g_static_scratch));
+        g_static_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    cudaStream_t st = 0;
+
+    // ---- carve the array (same layout on every call)
+    const int bands = data->colors_sh ? data->sh_bands : 0;
+    const int M = bands == 0 ? 0 : bands == 1 ? 3 : bands == 2 ? 8 : 15;
+    const uint32_t N = (uint32_t)n;
+    const uint64_t stride = round_up(std::max<uint32_t>(N, 1), 64);
+    const uint32_t TS = v.numTiles + 1;
+    Carver c{g_static_addr[dev]};
+    float* dPos = c.take<float>(12ull * kStaticMaxSplats);
+    float* dRot = c.take<float>(16ull * kStaticMaxSplats);
+    float* dLsc = c.take<float>(12ull * kStaticMaxSplats);
+    float* dOpl = c.take<float>(4ull * kStaticMaxSplats);
+    float* dDc = c.take<float>(12ull * kStaticMaxSplats);
+    float* dSh = c.take<float>(180ull * kStaticMaxSplats);
+    DlView* dView = c.take<DlView>(sizeof(DlView));
+    uint64_t* dSegStart = c.take<uint64_t>(8);
+    uint32_t* dSegLen = c.take<uint32_t>(4);
+    uint32_t* dSegTileBase = c.take<uint32_t>(4);
+    uint32_t* scr = c.take<uint32_t>(4ull * kScratchWords);
+    uint32_t* keys0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    uint32_t* keys1 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    uint32_t* vals0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    uint32_t* vals1 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    float4* recA = c.take<float4>(16ull * kStaticMaxSplats);
+    float4* recBC = c.take<float4>(32ull * kStaticMaxSplats);
+    uint2* bbox = c.take<uint2>(8ull * kStaticMaxSplats);
+    uint32_t* nvis = c.take<uint32_t>(4);
+    uint32_t* depthHist = c.take<uint32_t>(4ull * 4 * 256);
+    const uint32_t maxSortTiles = (uint32_t)((kStaticMaxPairs + dlsort::kTile - 1) / dlsort::kTile);
+    uint32_t* sortStatus = c.take<uint32_t>(4ull * 256 * maxSortTiles);
+    uint32_t** dOuts = c.take<uint32_t*>(sizeof(void*));
+    uint32_t* tileCount = c.take<uint32_t>(4ull * (kStaticMaxTiles + 1));
+    uint32_t* tileOff = c.take<uint32_t>(4ull * (kStaticMaxTiles + 1));
+    uint64_t* pairBase = c.take<uint64_t>(8);
+    uint64_t* pairCap = c.take<uint64_t>(8);
+    unsigned long long* npairs = c.take<unsigned long long>(8);
+    uint32_t* pairSegLen = c.take<uint32_t>(4);
+    uint32_t* pairSegTileBase = c.take<uint32_t>(4);
+    uint32_t* pairGlob = c.take<uint32_t>(4ull * 4 * 256);
+    const uint32_t emitTiles = (uint32_t)((stride + dlr::kEmitRanks - 1) / dlr::kEmitRanks);
+    unsigned long long* emitStatus = c.take<unsigned long long>(8ull * ((kStaticMaxSplats + dlr::kEmitRanks - 1) / dlr::kEmitRanks));
+    uint32_t* pkeys0 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    uint32_t* pkeys1 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    uint32_t* pvals0 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    uint32_t* pvals1 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    uint32_t* rgba = c.take<uint32_t>(4ull * kStaticMaxPixels);
+    if (c.off > kStaticBytes) { dl_set_error("dl_render_static: scratch layout exceeds the array"); return DL_E_CAPACITY; }
+
+    // ---- inputs (pageable host copies are staged by the driver; nothing is allocated here)
+    if (n) {
+        DL_CK(cudaMemcpyAsync(dPos, data->positions, 12 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(dRot, data->rotations, 16 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(dLsc, data->log_scales, 12 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(dOpl, data->opacity_logits, 4 * n, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(dDc, data->colors_dc, 12 * n, cudaMemcpyHostToDevice, st));
+        if (M) DL_CK(cudaMemcpyAsync(dSh, data->colors_sh, 12ull * M * n, cudaMemcpyHostToDevice, st));
+    }
+    const uint64_t segStart = 0;
+    const uint32_t segLen = N;
+    uint32_t* outPtr = rgba;
+    const uint64_t pairBaseH = 0, pairCapH = kStaticMaxPairs;
+    DL_CK(cudaMemcpyAsync(dView, &v, sizeof(DlView), cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(dSegStart, &segStart, 8, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(dSegLen, &segLen, 4, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(dOuts, &outPtr, sizeof(void*), cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(pairBase, &pairBaseH, 8, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(pairCap, &pairCapH, 8, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemsetAsync(scr, 0, 4ull * kScratchWords, st));
+    DL_CK(cudaMemsetAsync(nvis, 0, 4, st));
+    DL_CK(cudaMemsetAsync(tileCount, 0, 4ull * TS, st));
+    DL_CK(cudaMemsetAsync(emitStatus, 0, 8ull * emitTiles, st));
+
+    DlSceneDev sc{};
+    sc.pos = dPos; sc.rot = dRot; sc.lsc = dLsc; sc.opl = dOpl; sc.dc = dDc;
+    sc.sh = M ? dSh : nullptr; sc.sh16 = nullptr; sc.n = N; sc.bands = bands; sc.sh_kind = 0;
+
+    // ---- project
+    dlr::ProjectArgs pa;
+    pa.sc = sc; pa.views = dView; pa.num_views = 1; pa.view_stride = stride; pa.keys = keys0; pa.recA = recA;
+    pa.recBC = recBC; pa.recH = nullptr; pa.bbox = bbox; pa.nvis = nvis;
+    if (N) dlr::project_k<<<(N + 255) / 256, 256, 0, st>>>(pa);
+    DL_CK(cudaGetLastError());
+
+    // ---- depth sort (4 x 8-bit stable passes)
+    dlsort::Segs ds;
+    ds.start = dSegStart; ds.len = dSegLen; ds.tile_base = dSegTileBase; ds.total_tiles = scr + SC_DEPTH_TILES; ds.num = 1;
+    const uint32_t depthGrid = std::max<uint32_t>(1, (N + dlsort::kTile - 1) / dlsort::kTile);
+    if (N) {
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ds);
+        DL_CK(cudaMemsetAsync(depthHist, 0, 4ull * 4 * 256, st));
+        dlsort::hist_k<8><<<depthGrid, dlsort::kThreads, 0, st>>>(keys0, ds, 4, 0, depthHist);
+        dlsort::scan_hist_k<8><<<4, 256, 0, st>>>(depthHist, 4);
+        uint32_t *kin = keys0, *kout = keys1, *vin = nullptr, *vout = vals1;
+        for (int p = 0; p < 4; p++) {
+            DL_CK(cudaMemsetAsync(sortStatus, 0, 4ull * 256 * depthGrid, st));
+            dlsort::Pass sp;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
+            sp.segs = ds; sp.glob_off = depthHist; sp.status = sortStatus; sp.counter = scr + SC_DEPTH_CTR + p;
+            sp.err = scr + SC_ERR; sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
+            launch_pass_bits(8, sp, depthGrid, st);
+            std::swap(kin, kout);
+            vin = vout;
+            vout = (vout == vals1) ? vals0 : vals1;
+        }
+        DL_CK(cudaGetLastError());
+    }
+
+    // ---- emit, tile offsets, pair sort (pair capacity is fixed: overflow is an error)
+    int keyBits = 0;
+    while ((1u << keyBits) < std::max<uint32_t>(v.numTiles, 1)) keyBits++;
+    const int pbits = 8, ppasses = (keyBits + pbits - 1) / pbits;
+    dlr::EmitArgs ea;
+    ea.sorted_vals = vals0; ea.bbox = bbox; ea.nvis = nvis; ea.views = dView; ea.view_stride = stride;
+    ea.tiles_per_view = emitTiles; ea.pair_base = pairBase; ea.pair_cap = pairCap; ea.pair_keys = pkeys0;
+    ea.pair_vals = pvals0; ea.npairs = npairs; ea.tile_count = tileCount; ea.tile_stride = TS;
+    ea.status = emitStatus; ea.counter = scr + SC_EMIT_CTR; ea.err = scr + SC_ERR; ea.ovf = scr + SC_OVF;
+    dlr::emit_k<<<emitTiles, dlr::kEmitThreads, 0, st>>>(ea);
+    dlr::TileOffArgs ta;
+    ta.views = dView; ta.tile_count = tileCount; ta.tile_off = tileOff; ta.tile_stride = TS; ta.npairs = npairs;
+    ta.pair_cap = pairCap; ta.seg_len = pairSegLen; ta.glob_off = pairGlob; ta.bits = pbits; ta.passes = ppasses;
+    dlr::tile_offsets_k<<<1, 1024, 0, st>>>(ta);
+    DL_CK(cudaGetLastError());
+    uint32_t* finalVals = pvals0;
+    if (ppasses > 0) {
+        dlsort::Segs ps;
+        ps.start = pairBase; ps.len = pairSegLen; ps.tile_base = pairSegTileBase; ps.total_tiles = scr + SC_PAIR_TILES;
+        ps.num = 1;
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ps);
+        uint32_t *kin = pkeys0, *kout = pkeys1, *vin = pvals0, *vout = pvals1;
+        for (int p = 0; p < ppasses; p++) {
+            DL_CK(cudaMemsetAsync(sortStatus, 0, 4ull * 256 * maxSortTiles, st));
+            dlsort::Pass sp;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = (p + 1 < ppasses) ? kout : nullptr; sp.vals_out = vout;
+            sp.segs = ps; sp.glob_off = pairGlob; sp.status = sortStatus; sp.counter = scr + SC_PAIR_CTR + p;
+            sp.err = scr + SC_ERR; sp.shift = pbits * p; sp.pass = p; sp.passes = ppasses;
+            launch_pass_bits(pbits, sp, maxSortTiles, st);
+            std::swap(kin, kout);
+            std::swap(vin, vout);
+        }
+        finalVals = vin;
+        DL_CK(cudaGetLastError());
+    }
+
+    // ---- rasterize + finalize (exact exp, f32 records: same pixels as dl_render)
+    dlr::RasterArgs ra;
+    std::memset(&ra, 0, sizeof(ra));
+    ra.views = dView; ra.tile_off = tileOff; ra.tile_stride = TS; ra.pair_vals = finalVals; ra.pair_base = pairBase;
+    ra.recA = recA; ra.recBC = recBC; ra.recH = nullptr; ra.view_stride = stride; ra.outs = dOuts;
+    dlr::rasterize_k<true><<<dim3(v.numTiles, 1), dlr::kRasterThreads, 0, st>>>(ra);
+    DL_CK(cudaGetLastError());
+
+    uint32_t flagsH[2] = {0, 0};
+    DL_CK(cudaMemcpyAsync(&flagsH[0], scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));
+    DL_CK(cudaMemcpyAsync(&flagsH[1], scr + SC_OVF, 4, cudaMemcpyDeviceToHost, st));
+    DL_CK(cudaMemcpyAsync(out_rgba, rgba, pixels * 4, cudaMemcpyDeviceToHost, st));
+    DL_CK(cudaStreamSynchronize(st));
+    if (flagsH[0] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return DL_E_TIMEOUT; }
+    if (flagsH[1] & DL_DEVERR_OVERFLOW) {
+        dl_set_error("dl_render_static: more than " + std::to_string(kStaticMaxPairs) + " tile pairs in this view");
+        return DL_E_CAPACITY;
+    }
+    return DL_OK;
+}

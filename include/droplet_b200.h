@@ -131,6 +131,20 @@ int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, c
 int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
                    uint8_t* const* outs, uint32_t flags);
 
+/* No counterpart in the reference.  For callers that cannot allocate GPU
+ * memory (an application that owns the whole device through its own
+ * allocator, or a real-time loop that may not allocate after start-up): the
+ * single-view render of dl_render with no renderer handle, on the current CUDA
+ * device and its default stream, with all device scratch taken from one
+ * 16 MiB array that the library reserves statically on every GPU that loads
+ * it.  Limits: 16384 Gaussians, 921600 pixels (e.g. 1280x720), 4096 16x16
+ * tiles, 262144 tile pairs; beyond them it returns DL_E_CAPACITY.  Calls that
+ * overlap on one GPU race on the shared array.  The first call on a device
+ * looks the array up and should come before any stream capture there.
+ * max_coverage 0 selects the default 16384. */
+int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg[4], uint32_t max_coverage,
+                     uint8_t* out_rgba, size_t out_len);
+
 /* ---- voxelizer: src/voxel/voxelize.ts:59-248 voxelize(device, data, opts) */
 int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_opts* opts, dl_vox_result** out);
 /* VoxelizeResult {bounds, numBlocksX/Y/Z} (voxelize.ts:38-45) and the block
