@@ -1,8 +1,8 @@
 // dl_render.cu — host orchestration of the renderer's device pipeline.
 //
 // One frame (any number of views of one device-resident scene):
-//   project_k -> depth sort (4 onesweep passes) -> emit_k -> tile_offsets_k
-//   -> pair sort (1-3 onesweep passes) -> rasterize_k
+//   project_k -> depth sort (4 onesweep passes) -> emit_k -> pair_digits_k
+//   -> pair sort (1-3 onesweep passes) -> boundaries_k -> rasterize_k
 // No host synchronisation happens inside the frame: every size a later stage
 // needs (visible count, pair count, tile offsets) stays in device memory.
 // Pair buffers are sized from an upper bound; if a frame overflows them the
@@ -63,9 +63,6 @@ __global__ void sh_to_half_k(const float* in, uint16_t* out, uint64_t n, int kin
     }
 }
 
-void ev_record(dl_renderer* r, int i) {
-    if (r->profiling) cudaEventRecord(r->ev[i], r->stream);
-}
 
 }  // namespace
 
@@ -158,23 +155,237 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
     return DL_OK;
 }
 
+namespace {
+
+// Device pointers of one frame's working set (renderer buffers or the static array).
+struct FramePtrs {
+    DlView* views;
+    uint64_t* segStart;
+    uint32_t* segLen;
+    uint32_t* segTileBase;
+    uint32_t* scr;
+    uint32_t *keys0, *keys1, *vals0, *vals1;
+    float4* recA;
+    float4* recBC;
+    uint4* recH;
+    uint2* bbox;
+    uint32_t* nvis;
+    uint32_t* depthHist;
+    uint32_t* sortStatus;
+    uint32_t** outs;
+    uint32_t* tileOff;
+    uint64_t *pairBase, *pairCap;
+    unsigned long long* npairs;
+    uint32_t *pairSegLen, *pairSegTileBase, *pairGlob, *pairHist;
+    unsigned long long* emitStatus;
+    uint32_t *pkeys0, *pkeys1, *pvals0, *pvals1;
+    float4* accum;
+    unsigned long long* evalCount;
+};
+
+struct FrameDims {
+    uint32_t V = 1, N = 0, maxT = 1, TS = 2;
+    uint64_t stride = 64, cap = 0;
+    uint32_t depthGrid = 1, emitTilesPerView = 1, pairGrid = 1;
+    int pbits = 8, ppasses = 0;
+    bool f16rec = false, fastExp = false;
+};
+
+FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uint32_t flags) {
+    FrameDims d;
+    d.V = V;
+    d.N = N;
+    d.stride = round_up(std::max<uint32_t>(N, 1), 64);
+    for (uint32_t v = 0; v < V; v++) d.maxT = std::max(d.maxT, hv[v].numTiles);
+    d.TS = d.maxT + 1;
+    d.depthGrid = std::max<uint32_t>(1, V * (uint32_t)((N + dlsort::kTile - 1) / dlsort::kTile));
+    d.emitTilesPerView = (uint32_t)((d.stride + dlr::kEmitRanks - 1) / dlr::kEmitRanks);
+    int keyBits = 0;
+    while ((1u << keyBits) < d.maxT) keyBits++;
+    d.ppasses = (keyBits + d.pbits - 1) / d.pbits;
+    d.cap = cap;
+    d.pairGrid = std::max<uint32_t>(1, (uint32_t)(V * ((cap + dlsort::kTile - 1) / dlsort::kTile)));
+    d.f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
+    d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
+    return d;
+}
+
+inline void rec_event(cudaEvent_t* ev, int i, cudaStream_t st) {
+    if (ev) cudaEventRecord(ev[i], st);
+}
+
+// project + depth sort.  Expects views, segment tables, nvis and scratch words
+// already uploaded / cleared on the stream.
+int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cudaStream_t st, cudaEvent_t* ev,
+                 uint64_t* launches) {
+    rec_event(ev, 0, st);
+    dlr::ProjectArgs pa;
+    pa.sc = sc;
+    pa.views = f.views;
+    pa.num_views = d.V;
+    pa.view_stride = d.stride;
+    pa.keys = f.keys0;
+    pa.recA = f.recA;
+    pa.recBC = d.f16rec ? nullptr : f.recBC;
+    pa.recH = d.f16rec ? f.recH : nullptr;
+    pa.bbox = f.bbox;
+    pa.nvis = f.nvis;
+    if (d.N) {
+        dlr::project_k<<<(d.N + 255) / 256, 256, 0, st>>>(pa);
+        (*launches)++;
+    }
+    DL_CK(cudaGetLastError());
+    rec_event(ev, 1, st);
+    // depth sort: stable LSD, 4 x 8-bit digits, one segment per view
+    if (d.N) {
+        dlsort::Segs ds;
+        ds.start = f.segStart; ds.len = f.segLen; ds.tile_base = f.segTileBase;
+        ds.total_tiles = f.scr + SC_DEPTH_TILES; ds.num = d.V;
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ds);
+        DL_CK(cudaMemsetAsync(f.depthHist, 0, 4ull * d.V * 4 * 256, st));
+        dlsort::hist_k<8><<<std::min<uint32_t>(d.depthGrid, 4096), dlsort::kThreads, 0, st>>>(f.keys0, ds, 4, 0,
+                                                                                               f.depthHist);
+        dlsort::scan_hist_k<8><<<std::min<uint32_t>(4 * d.V, 1024), 256, 0, st>>>(f.depthHist, 4 * d.V);
+        *launches += 3;
+        uint32_t *kin = f.keys0, *kout = f.keys1, *vin = nullptr, *vout = f.vals1;
+        for (int p = 0; p < 4; p++) {
+            DL_CK(cudaMemsetAsync(f.sortStatus, 0, 4ull * 256 * d.depthGrid, st));
+            dlsort::Pass sp;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
+            sp.segs = ds; sp.glob_off = f.depthHist;
+            sp.status = f.sortStatus; sp.counter = f.scr + SC_DEPTH_CTR + p; sp.err = f.scr + SC_ERR;
+            sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
+            launch_pass_bits(8, sp, d.depthGrid, st);
+            (*launches)++;
+            std::swap(kin, kout);
+            vin = vout;
+            vout = (vout == f.vals1) ? f.vals0 : f.vals1;
+        }
+        DL_CK(cudaGetLastError());
+    }
+    rec_event(ev, 2, st);
+    // after 4 passes keys0 / vals0 hold the sorted keys / splat indices
+    return DL_OK;
+}
+
+// emit -> pair digits -> pair sort -> boundaries -> rasterize.  Expects
+// pairBase / pairCap uploaded.  *finalVals receives the sorted pair values.
+int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEvent_t* ev, uint64_t* launches,
+                uint32_t** finalVals) {
+    DL_CK(cudaMemsetAsync(f.pairHist, 0, 4ull * d.V * 4 * 256, st));
+    DL_CK(cudaMemsetAsync(f.emitStatus, 0, 8ull * d.V * d.emitTilesPerView, st));
+    DL_CK(cudaMemsetAsync(f.scr + SC_EMIT_CTR, 0, 4ull * 6, st));   // emit + pair counters + work counter
+    DL_CK(cudaMemsetAsync(f.scr + SC_OVF, 0, 4, st));
+    rec_event(ev, 3, st);
+    dlr::EmitArgs ea;
+    ea.sorted_vals = f.vals0;
+    ea.bbox = f.bbox;
+    ea.nvis = f.nvis;
+    ea.views = f.views;
+    ea.view_stride = d.stride;
+    ea.tiles_per_view = d.emitTilesPerView;
+    ea.pair_base = f.pairBase;
+    ea.pair_cap = f.pairCap;
+    ea.pair_keys = f.pkeys0;
+    ea.pair_vals = f.pvals0;
+    ea.npairs = f.npairs;
+    ea.digit_hist = f.pairHist;
+    ea.bits = d.pbits;
+    ea.passes = d.ppasses;
+    ea.status = f.emitStatus;
+    ea.counter = f.scr + SC_EMIT_CTR;
+    ea.err = f.scr + SC_ERR;
+    ea.ovf = f.scr + SC_OVF;
+    dlr::emit_k<<<d.V * d.emitTilesPerView, dlr::kEmitThreads, 0, st>>>(ea);
+    (*launches)++;
+    DL_CK(cudaGetLastError());
+    rec_event(ev, 4, st);
+
+    dlr::PairDigitArgs pd;
+    pd.digit_hist = f.pairHist;
+    pd.glob_off = f.pairGlob;
+    pd.npairs = f.npairs;
+    pd.pair_cap = f.pairCap;
+    pd.seg_len = f.pairSegLen;
+    pd.bits = d.pbits;
+    pd.passes = d.ppasses;
+    dlr::pair_digits_k<<<d.V, 32, 0, st>>>(pd);
+    (*launches)++;
+    DL_CK(cudaGetLastError());
+    rec_event(ev, 5, st);
+
+    // pair sort by tile id (stable: depth-rank order kept inside each tile)
+    uint32_t* vals = f.pvals0;
+    uint32_t* keys = f.pkeys0;
+    if (d.ppasses > 0) {
+        dlsort::Segs ps;
+        ps.start = f.pairBase; ps.len = f.pairSegLen; ps.tile_base = f.pairSegTileBase;
+        ps.total_tiles = f.scr + SC_PAIR_TILES; ps.num = d.V;
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ps);
+        (*launches)++;
+        uint32_t *kin = f.pkeys0, *kout = f.pkeys1, *vin = f.pvals0, *vout = f.pvals1;
+        for (int p = 0; p < d.ppasses; p++) {
+            DL_CK(cudaMemsetAsync(f.sortStatus, 0, 4ull * 256 * d.pairGrid, st));
+            dlsort::Pass sp;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
+            sp.segs = ps; sp.glob_off = f.pairGlob;
+            sp.status = f.sortStatus; sp.counter = f.scr + SC_PAIR_CTR + p; sp.err = f.scr + SC_ERR;
+            sp.shift = d.pbits * p; sp.pass = p; sp.passes = d.ppasses;
+            launch_pass_bits(d.pbits, sp, d.pairGrid, st);
+            (*launches)++;
+            std::swap(kin, kout);
+            std::swap(vin, vout);
+        }
+        keys = kin;
+        vals = vin;
+        DL_CK(cudaGetLastError());
+    }
+    dlr::BoundArgs ba;
+    ba.views = f.views;
+    ba.keys = keys;
+    ba.pair_base = f.pairBase;
+    ba.seg_len = f.pairSegLen;
+    ba.tile_off = f.tileOff;
+    ba.tile_stride = d.TS;
+    const uint32_t bgrid = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((d.cap + 256) / 256, 1), 2048);
+    dlr::boundaries_k<<<dim3(bgrid, d.V), 256, 0, st>>>(ba);
+    (*launches)++;
+    DL_CK(cudaGetLastError());
+    rec_event(ev, 6, st);
+
+    dlr::RasterArgs ra;
+    std::memset(&ra, 0, sizeof(ra));
+    ra.views = f.views;
+    ra.tile_off = f.tileOff;
+    ra.tile_stride = d.TS;
+    ra.pair_vals = vals;
+    ra.pair_base = f.pairBase;
+    ra.recA = f.recA;
+    ra.recBC = d.f16rec ? nullptr : f.recBC;
+    ra.recH = d.f16rec ? f.recH : nullptr;
+    ra.view_stride = d.stride;
+    ra.outs = f.outs;
+    ra.accum = f.accum;
+    ra.eval_count = f.evalCount;
+    const dim3 rg(d.maxT, d.V);
+    if (d.fastExp) dlr::rasterize_k<false><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
+    else dlr::rasterize_k<true><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
+    (*launches)++;
+    DL_CK(cudaGetLastError());
+    rec_event(ev, 7, st);
+    *finalVals = vals;
+    return DL_OK;
+}
+
+}  // namespace
+
 int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint32_t V, uint32_t* const* d_outs,
                     uint32_t flags) {
     cudaStream_t st = r->stream;
     const uint32_t N = sc.n;
-    const uint64_t stride = round_up(std::max<uint32_t>(N, 1), 64);
-    const bool f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
-    const bool fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
+    if (r->pair_cap_per_view == 0) r->pair_cap_per_view = std::max<uint64_t>(1u << 20, 4ull * N);
+    FrameDims d = frame_dims(hv, V, N, r->pair_cap_per_view, flags);
     const bool countEvals = (flags & DL_BATCH_COUNT_EVALS) != 0;
-    if (countEvals) {
-        DL_TRY(r->evalCount.ensure(8));
-        DL_CK(cudaMemsetAsync(r->evalCount.p, 0, 8, st));
-    }
-    uint32_t maxT = 1;
-    for (uint32_t v = 0; v < V; v++) maxT = std::max(maxT, hv[v].numTiles);
-    const uint32_t TS = maxT + 1;
-    const uint32_t depthTilesPerView = (uint32_t)((N + dlsort::kTile - 1) / dlsort::kTile);
-    const uint32_t emitTilesPerView = (uint32_t)((stride + dlr::kEmitRanks - 1) / dlr::kEmitRanks);
     r->launches = 0;
 
     // ---- buffers
@@ -183,229 +394,103 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     DL_TRY(r->segLen.ensure(4ull * V));
     DL_TRY(r->segTileBase.ensure(4ull * V));
     DL_TRY(r->scratch.ensure(4ull * kScratchWords));
-    DL_TRY(r->keys0.ensure(4ull * V * stride));
-    DL_TRY(r->keys1.ensure(4ull * V * stride));
-    DL_TRY(r->vals0.ensure(4ull * V * stride));
-    DL_TRY(r->vals1.ensure(4ull * V * stride));
-    DL_TRY(r->recA.ensure(16ull * V * stride));
-    if (f16rec) DL_TRY(r->recH.ensure(16ull * V * stride));
-    else DL_TRY(r->recBC.ensure(32ull * V * stride));
-    DL_TRY(r->bbox.ensure(8ull * V * stride));
+    DL_TRY(r->keys0.ensure(4ull * V * d.stride));
+    DL_TRY(r->keys1.ensure(4ull * V * d.stride));
+    DL_TRY(r->vals0.ensure(4ull * V * d.stride));
+    DL_TRY(r->vals1.ensure(4ull * V * d.stride));
+    DL_TRY(r->recA.ensure(16ull * V * d.stride));
+    if (d.f16rec) DL_TRY(r->recH.ensure(16ull * V * d.stride));
+    else DL_TRY(r->recBC.ensure(32ull * V * d.stride));
+    DL_TRY(r->bbox.ensure(8ull * V * d.stride));
     DL_TRY(r->nvis.ensure(4ull * V));
     DL_TRY(r->depthHist.ensure(4ull * V * 4 * 256));
     DL_TRY(r->outs.ensure(sizeof(uint32_t*) * V));
-    DL_TRY(r->tileCount.ensure(4ull * V * TS));
-    DL_TRY(r->tileOff.ensure(4ull * V * TS));
+    DL_TRY(r->tileOff.ensure(4ull * V * d.TS));
     DL_TRY(r->pairBase.ensure(8ull * V));
     DL_TRY(r->pairCap.ensure(8ull * V));
     DL_TRY(r->npairs.ensure(8ull * V));
     DL_TRY(r->pairSegLen.ensure(4ull * V));
     DL_TRY(r->pairSegTileBase.ensure(4ull * V));
     DL_TRY(r->pairGlob.ensure(4ull * V * 4 * 256));
-    DL_TRY(r->emitStatus.ensure(8ull * V * emitTilesPerView));
+    DL_TRY(r->tileCount.ensure(4ull * V * 4 * 256));          // tile-id digit histograms of the pair sort
+    DL_TRY(r->emitStatus.ensure(8ull * V * d.emitTilesPerView));
+    DL_TRY(r->sortStatus.ensure(4ull * 256 * d.depthGrid));
     if (r->keep_accum && V == 1) DL_TRY(r->accum.ensure(16ull * hv[0].W * hv[0].H));
+    if (countEvals) DL_TRY(r->evalCount.ensure(8));
+
+    FramePtrs f;
+    std::memset(&f, 0, sizeof(f));
+    f.views = r->views.as<DlView>();
+    f.segStart = r->segStart.as<uint64_t>();
+    f.segLen = r->segLen.as<uint32_t>();
+    f.segTileBase = r->segTileBase.as<uint32_t>();
+    f.scr = r->scratch.as<uint32_t>();
+    f.keys0 = r->keys0.as<uint32_t>(); f.keys1 = r->keys1.as<uint32_t>();
+    f.vals0 = r->vals0.as<uint32_t>(); f.vals1 = r->vals1.as<uint32_t>();
+    f.recA = r->recA.as<float4>();
+    f.recBC = d.f16rec ? nullptr : r->recBC.as<float4>();
+    f.recH = d.f16rec ? r->recH.as<uint4>() : nullptr;
+    f.bbox = r->bbox.as<uint2>();
+    f.nvis = r->nvis.as<uint32_t>();
+    f.depthHist = r->depthHist.as<uint32_t>();
+    f.outs = r->outs.as<uint32_t*>();
+    f.tileOff = r->tileOff.as<uint32_t>();
+    f.pairBase = r->pairBase.as<uint64_t>();
+    f.pairCap = r->pairCap.as<uint64_t>();
+    f.npairs = r->npairs.as<unsigned long long>();
+    f.pairSegLen = r->pairSegLen.as<uint32_t>();
+    f.pairSegTileBase = r->pairSegTileBase.as<uint32_t>();
+    f.pairGlob = r->pairGlob.as<uint32_t>();
+    f.pairHist = r->tileCount.as<uint32_t>();
+    f.emitStatus = r->emitStatus.as<unsigned long long>();
+    f.accum = (r->keep_accum && V == 1) ? r->accum.as<float4>() : nullptr;
+    f.evalCount = countEvals ? r->evalCount.as<unsigned long long>() : nullptr;
 
     // ---- host-side tables (pinned staging), one upload
-    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + 8ull * V * 2 + sizeof(void*) * V;
+    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + sizeof(void*) * V + 64;
     DL_TRY(ensure_pinned((void**)&r->h_views, &r->h_views_cap, hbytes));
     char* hb = (char*)r->h_views;
     std::memcpy(hb, hv, sizeof(DlView) * V);
     uint64_t* hSegStart = (uint64_t*)(hb + sizeof(DlView) * V);
     uint32_t* hSegLen = (uint32_t*)(hSegStart + V);
-    for (uint32_t v = 0; v < V; v++) { hSegStart[v] = (uint64_t)v * stride; hSegLen[v] = N; }
-    void** hOuts = (void**)(hSegLen + V);
+    for (uint32_t v = 0; v < V; v++) { hSegStart[v] = (uint64_t)v * d.stride; hSegLen[v] = N; }
+    void** hOuts = (void**)(hSegLen + V + (V & 1));
     for (uint32_t v = 0; v < V; v++) hOuts[v] = d_outs[v];
-    DL_CK(cudaMemcpyAsync(r->views.p, hb, sizeof(DlView) * V, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(r->segStart.p, hSegStart, 8ull * V, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(r->segLen.p, hSegLen, 4ull * V, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(r->outs.p, hOuts, sizeof(void*) * V, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemsetAsync(r->scratch.p, 0, 4ull * kScratchWords, st));
-    DL_CK(cudaMemsetAsync(r->nvis.p, 0, 4ull * V, st));
-    uint32_t* scr = r->scratch.as<uint32_t>();
+    DL_CK(cudaMemcpyAsync(f.views, hb, sizeof(DlView) * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.segStart, hSegStart, 8ull * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.segLen, hSegLen, 4ull * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.outs, hOuts, sizeof(void*) * V, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemsetAsync(f.scr, 0, 4ull * kScratchWords, st));
+    DL_CK(cudaMemsetAsync(f.nvis, 0, 4ull * V, st));
+    if (f.evalCount) DL_CK(cudaMemsetAsync(f.evalCount, 0, 8, st));
+    cudaEvent_t* ev = r->profiling ? r->ev : nullptr;
 
-    // ---- 1. project (+ f64 cull and depth keys)
-    ev_record(r, 0);
-    dlr::ProjectArgs pa;
-    pa.sc = sc;
-    pa.views = r->views.as<DlView>();
-    pa.num_views = V;
-    pa.view_stride = stride;
-    pa.keys = r->keys0.as<uint32_t>();
-    pa.recA = r->recA.as<float4>();
-    pa.recBC = f16rec ? nullptr : r->recBC.as<float4>();
-    pa.recH = f16rec ? r->recH.as<uint4>() : nullptr;
-    pa.bbox = r->bbox.as<uint2>();
-    pa.nvis = r->nvis.as<uint32_t>();
-    if (N) {
-        dlr::project_k<<<(N + 255) / 256, 256, 0, st>>>(pa);
-        r->launches++;
-    }
-    DL_CK(cudaGetLastError());
-    ev_record(r, 1);
+    f.sortStatus = r->sortStatus.as<uint32_t>();
+    DL_TRY(launch_front(f, d, sc, st, ev, &r->launches));
 
-    // ---- 2. depth sort: stable LSD, 4 x 8-bit digits, one segment per view
-    dlsort::Segs ds;
-    ds.start = r->segStart.as<uint64_t>();
-    ds.len = r->segLen.as<uint32_t>();
-    ds.tile_base = r->segTileBase.as<uint32_t>();
-    ds.total_tiles = scr + SC_DEPTH_TILES;
-    ds.num = V;
-    const uint32_t depthGrid = std::max<uint32_t>(1, V * depthTilesPerView);
-    DL_TRY(r->sortStatus.ensure(4ull * 256 * depthGrid));
-    if (N) {
-        dlsort::prepare_k<<<1, 32, 0, st>>>(ds);
-        DL_CK(cudaMemsetAsync(r->depthHist.p, 0, 4ull * V * 4 * 256, st));
-        dlsort::hist_k<8><<<std::min<uint32_t>(depthGrid, 4096), dlsort::kThreads, 0, st>>>(
-            r->keys0.as<uint32_t>(), ds, 4, 0, r->depthHist.as<uint32_t>());
-        dlsort::scan_hist_k<8><<<std::min<uint32_t>(4 * V, 1024), 256, 0, st>>>(r->depthHist.as<uint32_t>(), 4 * V);
-        r->launches += 3;
-        uint32_t* kin = r->keys0.as<uint32_t>();
-        uint32_t* kout = r->keys1.as<uint32_t>();
-        uint32_t* vin = nullptr;
-        uint32_t* vout = r->vals1.as<uint32_t>();
-        for (int p = 0; p < 4; p++) {
-            DL_CK(cudaMemsetAsync(r->sortStatus.p, 0, 4ull * 256 * depthGrid, st));
-            dlsort::Pass sp;
-            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
-            sp.segs = ds; sp.glob_off = r->depthHist.as<uint32_t>();
-            sp.status = r->sortStatus.as<uint32_t>(); sp.counter = scr + SC_DEPTH_CTR + p; sp.err = scr + SC_ERR;
-            sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
-            launch_pass_bits(8, sp, depthGrid, st);
-            r->launches++;
-            std::swap(kin, kout);
-            vin = vout;
-            vout = (vout == r->vals1.as<uint32_t>()) ? r->vals0.as<uint32_t>() : r->vals1.as<uint32_t>();
-        }
-        DL_CK(cudaGetLastError());
-    }
-    ev_record(r, 2);
-    // after 4 passes: keys0 / vals0 hold the sorted keys / splat indices
-
-    // ---- 3.. pair stages (re-run if the pair buffers overflow)
-    int keyBits = 0;
-    while ((1u << keyBits) < maxT) keyBits++;
-    const int pbits = 8;
-    const int ppasses = (keyBits + pbits - 1) / pbits;
-    if (r->pair_cap_per_view == 0) r->pair_cap_per_view = std::max<uint64_t>(1u << 20, 4ull * N);
     for (int attempt = 0; attempt < 3; attempt++) {
         const uint64_t cap = r->pair_cap_per_view;
         if (cap >= (1ull << 30)) { dl_set_error("more than 2^30 tile pairs in one view"); return DL_E_CAPACITY; }
+        d = frame_dims(hv, V, N, cap, flags);
         DL_TRY(r->pkeys0.ensure(4ull * V * cap));
         DL_TRY(r->pvals0.ensure(4ull * V * cap));
-        if (ppasses > 0) {
-            DL_TRY(r->pkeys1.ensure(4ull * V * cap));
-            DL_TRY(r->pvals1.ensure(4ull * V * cap));
-        }
-        const uint32_t pairGrid = std::max<uint32_t>(1, (uint32_t)(V * ((cap + dlsort::kTile - 1) / dlsort::kTile)));
-        DL_TRY(r->sortStatus.ensure(4ull * 256 * std::max(pairGrid, depthGrid)));
+        DL_TRY(r->pkeys1.ensure(4ull * V * cap));
+        DL_TRY(r->pvals1.ensure(4ull * V * cap));
+        DL_TRY(r->sortStatus.ensure(4ull * 256 * std::max(d.pairGrid, d.depthGrid)));
+        f.sortStatus = r->sortStatus.as<uint32_t>();
+        f.pkeys0 = r->pkeys0.as<uint32_t>(); f.pkeys1 = r->pkeys1.as<uint32_t>();
+        f.pvals0 = r->pvals0.as<uint32_t>(); f.pvals1 = r->pvals1.as<uint32_t>();
         DL_TRY(ensure_pinned((void**)&r->h_u64, &r->h_u64_cap, 16ull * V + 64));
         for (uint32_t v = 0; v < V; v++) { r->h_u64[v] = (uint64_t)v * cap; r->h_u64[V + v] = cap; }
-        DL_CK(cudaMemcpyAsync(r->pairBase.p, r->h_u64, 8ull * V, cudaMemcpyHostToDevice, st));
-        DL_CK(cudaMemcpyAsync(r->pairCap.p, r->h_u64 + V, 8ull * V, cudaMemcpyHostToDevice, st));
-        DL_CK(cudaMemsetAsync(r->tileCount.p, 0, 4ull * V * TS, st));
-        DL_CK(cudaMemsetAsync(r->emitStatus.p, 0, 8ull * V * emitTilesPerView, st));
-        DL_CK(cudaMemsetAsync(scr + SC_EMIT_CTR, 0, 4ull * 6, st));   // emit + pair counters + work counter
-        DL_CK(cudaMemsetAsync(scr + SC_OVF, 0, 4, st));
-
-        ev_record(r, 3);
-        dlr::EmitArgs ea;
-        ea.sorted_vals = r->vals0.as<uint32_t>();
-        ea.bbox = r->bbox.as<uint2>();
-        ea.nvis = r->nvis.as<uint32_t>();
-        ea.views = r->views.as<DlView>();
-        ea.view_stride = stride;
-        ea.tiles_per_view = emitTilesPerView;
-        ea.pair_base = r->pairBase.as<uint64_t>();
-        ea.pair_cap = r->pairCap.as<uint64_t>();
-        ea.pair_keys = r->pkeys0.as<uint32_t>();
-        ea.pair_vals = r->pvals0.as<uint32_t>();
-        ea.npairs = r->npairs.as<unsigned long long>();
-        ea.tile_count = r->tileCount.as<uint32_t>();
-        ea.tile_stride = TS;
-        ea.status = r->emitStatus.as<unsigned long long>();
-        ea.counter = scr + SC_EMIT_CTR;
-        ea.err = scr + SC_ERR;
-        ea.ovf = scr + SC_OVF;
-        dlr::emit_k<<<V * emitTilesPerView, dlr::kEmitThreads, 0, st>>>(ea);
-        r->launches++;
-        DL_CK(cudaGetLastError());
-        ev_record(r, 4);
-
-        dlr::TileOffArgs ta;
-        ta.views = r->views.as<DlView>();
-        ta.tile_count = r->tileCount.as<uint32_t>();
-        ta.tile_off = r->tileOff.as<uint32_t>();
-        ta.tile_stride = TS;
-        ta.npairs = r->npairs.as<unsigned long long>();
-        ta.pair_cap = r->pairCap.as<uint64_t>();
-        ta.seg_len = r->pairSegLen.as<uint32_t>();
-        ta.glob_off = r->pairGlob.as<uint32_t>();
-        ta.bits = pbits;
-        ta.passes = ppasses;
-        dlr::tile_offsets_k<<<V, 1024, 0, st>>>(ta);
-        r->launches++;
-        DL_CK(cudaGetLastError());
-        ev_record(r, 5);
-
-        // pair sort by tile id (stable: depth-rank order kept inside each tile)
-        uint32_t* finalVals = r->pvals0.as<uint32_t>();
-        if (ppasses > 0) {
-            dlsort::Segs ps;
-            ps.start = r->pairBase.as<uint64_t>();
-            ps.len = r->pairSegLen.as<uint32_t>();
-            ps.tile_base = r->pairSegTileBase.as<uint32_t>();
-            ps.total_tiles = scr + SC_PAIR_TILES;
-            ps.num = V;
-            dlsort::prepare_k<<<1, 32, 0, st>>>(ps);
-            r->launches++;
-            uint32_t* kin = r->pkeys0.as<uint32_t>();
-            uint32_t* kout = r->pkeys1.as<uint32_t>();
-            uint32_t* vin = r->pvals0.as<uint32_t>();
-            uint32_t* vout = r->pvals1.as<uint32_t>();
-            for (int p = 0; p < ppasses; p++) {
-                DL_CK(cudaMemsetAsync(r->sortStatus.p, 0, 4ull * 256 * pairGrid, st));
-                dlsort::Pass sp;
-                sp.keys_in = kin; sp.vals_in = vin;
-                sp.keys_out = (p + 1 < ppasses) ? kout : nullptr;
-                sp.vals_out = vout;
-                sp.segs = ps; sp.glob_off = r->pairGlob.as<uint32_t>();
-                sp.status = r->sortStatus.as<uint32_t>(); sp.counter = scr + SC_PAIR_CTR + p; sp.err = scr + SC_ERR;
-                sp.shift = pbits * p; sp.pass = p; sp.passes = ppasses;
-                launch_pass_bits(pbits, sp, pairGrid, st);
-                r->launches++;
-                std::swap(kin, kout);
-                std::swap(vin, vout);
-            }
-            finalVals = vin;
-            DL_CK(cudaGetLastError());
-        }
-        ev_record(r, 6);
-
-        dlr::RasterArgs ra;
-        std::memset(&ra, 0, sizeof(ra));
-        ra.views = r->views.as<DlView>();
-        ra.tile_off = r->tileOff.as<uint32_t>();
-        ra.tile_stride = TS;
-        ra.pair_vals = finalVals;
-        ra.pair_base = r->pairBase.as<uint64_t>();
-        ra.recA = r->recA.as<float4>();
-        ra.recBC = f16rec ? nullptr : r->recBC.as<float4>();
-        ra.recH = f16rec ? r->recH.as<uint4>() : nullptr;
-        ra.view_stride = stride;
-        ra.outs = r->outs.as<uint32_t*>();
-        ra.accum = (r->keep_accum && V == 1) ? r->accum.as<float4>() : nullptr;
-        ra.eval_count = countEvals ? r->evalCount.as<unsigned long long>() : nullptr;
-        const dim3 rg(maxT, V);
-        if (fastExp) dlr::rasterize_k<false><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
-        else dlr::rasterize_k<true><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
-        r->launches++;
-        DL_CK(cudaGetLastError());
-        ev_record(r, 7);
+        DL_CK(cudaMemcpyAsync(f.pairBase, r->h_u64, 8ull * V, cudaMemcpyHostToDevice, st));
+        DL_CK(cudaMemcpyAsync(f.pairCap, r->h_u64 + V, 8ull * V, cudaMemcpyHostToDevice, st));
+        uint32_t* finalVals = nullptr;
+        DL_TRY(launch_back(f, d, st, ev, &r->launches, &finalVals));
 
         // one sync per frame: error word and pair totals
-        DL_CK(cudaMemcpyAsync(r->h_u64, r->npairs.p, 8ull * V, cudaMemcpyDeviceToHost, st));
-        DL_CK(cudaMemcpyAsync(r->h_u64 + V, scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));
-        DL_CK(cudaMemcpyAsync(r->h_u64 + V + 1, scr + SC_OVF, 4, cudaMemcpyDeviceToHost, st));
+        DL_CK(cudaMemcpyAsync(r->h_u64, f.npairs, 8ull * V, cudaMemcpyDeviceToHost, st));
+        DL_CK(cudaMemcpyAsync(r->h_u64 + V, f.scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));
+        DL_CK(cudaMemcpyAsync(r->h_u64 + V + 1, f.scr + SC_OVF, 4, cudaMemcpyDeviceToHost, st));
         DL_CK(cudaStreamSynchronize(st));
         const uint32_t err = (uint32_t)(r->h_u64[V] & 0xffffffffu) | (uint32_t)(r->h_u64[V + 1] & 0xffffffffu);
         if (r->profiling) {
@@ -425,12 +510,12 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             continue;
         }
         r->last_n = N;
-        r->last_stride = (uint32_t)stride;
+        r->last_stride = (uint32_t)d.stride;
         r->last_T = hv[0].numTiles;
         r->last_W = hv[0].W;
         r->last_H = hv[0].H;
         r->last_pairs_final = (uint32_t)r->h_u64[0];
-        r->last_rec_kind = f16rec ? 1 : 0;
+        r->last_rec_kind = d.f16rec ? 1 : 0;
         r->last_final_vals = finalVals;
         r->last_V = V;
         return DL_OK;
@@ -535,8 +620,7 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     const int bands = data->colors_sh ? data->sh_bands : 0;
     const int M = bands == 0 ? 0 : bands == 1 ? 3 : bands == 2 ? 8 : 15;
     const uint32_t N = (uint32_t)n;
-    const uint64_t stride = round_up(std::max<uint32_t>(N, 1), 64);
-    const uint32_t TS = v.numTiles + 1;
+    const FrameDims d = frame_dims(&v, 1, N, kStaticMaxPairs, 0);
     Carver c{g_static_addr[dev]};
     float* dPos = c.take<float>(12ull * kStaticMaxSplats);
     float* dRot = c.take<float>(16ull * kStaticMaxSplats);
@@ -544,37 +628,38 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     float* dOpl = c.take<float>(4ull * kStaticMaxSplats);
     float* dDc = c.take<float>(12ull * kStaticMaxSplats);
     float* dSh = c.take<float>(180ull * kStaticMaxSplats);
-    DlView* dView = c.take<DlView>(sizeof(DlView));
-    uint64_t* dSegStart = c.take<uint64_t>(8);
-    uint32_t* dSegLen = c.take<uint32_t>(4);
-    uint32_t* dSegTileBase = c.take<uint32_t>(4);
-    uint32_t* scr = c.take<uint32_t>(4ull * kScratchWords);
-    uint32_t* keys0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
-    uint32_t* keys1 = c.take<uint32_t>(4ull * kStaticMaxSplats);
-    uint32_t* vals0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
-    uint32_t* vals1 = c.take<uint32_t>(4ull * kStaticMaxSplats);
-    float4* recA = c.take<float4>(16ull * kStaticMaxSplats);
-    float4* recBC = c.take<float4>(32ull * kStaticMaxSplats);
-    uint2* bbox = c.take<uint2>(8ull * kStaticMaxSplats);
-    uint32_t* nvis = c.take<uint32_t>(4);
-    uint32_t* depthHist = c.take<uint32_t>(4ull * 4 * 256);
+    FramePtrs f;
+    std::memset(&f, 0, sizeof(f));
+    f.views = c.take<DlView>(sizeof(DlView));
+    f.segStart = c.take<uint64_t>(8);
+    f.segLen = c.take<uint32_t>(4);
+    f.segTileBase = c.take<uint32_t>(4);
+    f.scr = c.take<uint32_t>(4ull * kScratchWords);
+    f.keys0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    f.keys1 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    f.vals0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    f.vals1 = c.take<uint32_t>(4ull * kStaticMaxSplats);
+    f.recA = c.take<float4>(16ull * kStaticMaxSplats);
+    f.recBC = c.take<float4>(32ull * kStaticMaxSplats);
+    f.bbox = c.take<uint2>(8ull * kStaticMaxSplats);
+    f.nvis = c.take<uint32_t>(4);
+    f.depthHist = c.take<uint32_t>(4ull * 4 * 256);
     const uint32_t maxSortTiles = (uint32_t)((kStaticMaxPairs + dlsort::kTile - 1) / dlsort::kTile);
-    uint32_t* sortStatus = c.take<uint32_t>(4ull * 256 * maxSortTiles);
-    uint32_t** dOuts = c.take<uint32_t*>(sizeof(void*));
-    uint32_t* tileCount = c.take<uint32_t>(4ull * (kStaticMaxTiles + 1));
-    uint32_t* tileOff = c.take<uint32_t>(4ull * (kStaticMaxTiles + 1));
-    uint64_t* pairBase = c.take<uint64_t>(8);
-    uint64_t* pairCap = c.take<uint64_t>(8);
-    unsigned long long* npairs = c.take<unsigned long long>(8);
-    uint32_t* pairSegLen = c.take<uint32_t>(4);
-    uint32_t* pairSegTileBase = c.take<uint32_t>(4);
-    uint32_t* pairGlob = c.take<uint32_t>(4ull * 4 * 256);
-    const uint32_t emitTiles = (uint32_t)((stride + dlr::kEmitRanks - 1) / dlr::kEmitRanks);
-    unsigned long long* emitStatus = c.take<unsigned long long>(8ull * ((kStaticMaxSplats + dlr::kEmitRanks - 1) / dlr::kEmitRanks));
-    uint32_t* pkeys0 = c.take<uint32_t>(4ull * kStaticMaxPairs);
-    uint32_t* pkeys1 = c.take<uint32_t>(4ull * kStaticMaxPairs);
-    uint32_t* pvals0 = c.take<uint32_t>(4ull * kStaticMaxPairs);
-    uint32_t* pvals1 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    f.sortStatus = c.take<uint32_t>(4ull * 256 * maxSortTiles);
+    f.outs = c.take<uint32_t*>(sizeof(void*));
+    f.tileOff = c.take<uint32_t>(4ull * (kStaticMaxTiles + 1));
+    f.pairBase = c.take<uint64_t>(8);
+    f.pairCap = c.take<uint64_t>(8);
+    f.npairs = c.take<unsigned long long>(8);
+    f.pairSegLen = c.take<uint32_t>(4);
+    f.pairSegTileBase = c.take<uint32_t>(4);
+    f.pairGlob = c.take<uint32_t>(4ull * 4 * 256);
+    f.pairHist = c.take<uint32_t>(4ull * 4 * 256);
+    f.emitStatus = c.take<unsigned long long>(8ull * ((kStaticMaxSplats + dlr::kEmitRanks - 1) / dlr::kEmitRanks));
+    f.pkeys0 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    f.pkeys1 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    f.pvals0 = c.take<uint32_t>(4ull * kStaticMaxPairs);
+    f.pvals1 = c.take<uint32_t>(4ull * kStaticMaxPairs);
     uint32_t* rgba = c.take<uint32_t>(4ull * kStaticMaxPixels);
     if (c.off > kStaticBytes) { dl_set_error("dl_render_static: scratch layout exceeds the array"); return DL_E_CAPACITY; }
 
@@ -591,99 +676,27 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     const uint32_t segLen = N;
     uint32_t* outPtr = rgba;
     const uint64_t pairBaseH = 0, pairCapH = kStaticMaxPairs;
-    DL_CK(cudaMemcpyAsync(dView, &v, sizeof(DlView), cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(dSegStart, &segStart, 8, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(dSegLen, &segLen, 4, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(dOuts, &outPtr, sizeof(void*), cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(pairBase, &pairBaseH, 8, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemcpyAsync(pairCap, &pairCapH, 8, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemsetAsync(scr, 0, 4ull * kScratchWords, st));
-    DL_CK(cudaMemsetAsync(nvis, 0, 4, st));
-    DL_CK(cudaMemsetAsync(tileCount, 0, 4ull * TS, st));
-    DL_CK(cudaMemsetAsync(emitStatus, 0, 8ull * emitTiles, st));
+    DL_CK(cudaMemcpyAsync(f.views, &v, sizeof(DlView), cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.segStart, &segStart, 8, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.segLen, &segLen, 4, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.outs, &outPtr, sizeof(void*), cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.pairBase, &pairBaseH, 8, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemcpyAsync(f.pairCap, &pairCapH, 8, cudaMemcpyHostToDevice, st));
+    DL_CK(cudaMemsetAsync(f.scr, 0, 4ull * kScratchWords, st));
+    DL_CK(cudaMemsetAsync(f.nvis, 0, 4, st));
 
     DlSceneDev sc{};
     sc.pos = dPos; sc.rot = dRot; sc.lsc = dLsc; sc.opl = dOpl; sc.dc = dDc;
     sc.sh = M ? dSh : nullptr; sc.sh16 = nullptr; sc.n = N; sc.bands = bands; sc.sh_kind = 0;
 
-    // ---- project
-    dlr::ProjectArgs pa;
-    pa.sc = sc; pa.views = dView; pa.num_views = 1; pa.view_stride = stride; pa.keys = keys0; pa.recA = recA;
-    pa.recBC = recBC; pa.recH = nullptr; pa.bbox = bbox; pa.nvis = nvis;
-    if (N) dlr::project_k<<<(N + 255) / 256, 256, 0, st>>>(pa);
-    DL_CK(cudaGetLastError());
-
-    // ---- depth sort (4 x 8-bit stable passes)
-    dlsort::Segs ds;
-    ds.start = dSegStart; ds.len = dSegLen; ds.tile_base = dSegTileBase; ds.total_tiles = scr + SC_DEPTH_TILES; ds.num = 1;
-    const uint32_t depthGrid = std::max<uint32_t>(1, (N + dlsort::kTile - 1) / dlsort::kTile);
-    if (N) {
-        dlsort::prepare_k<<<1, 32, 0, st>>>(ds);
-        DL_CK(cudaMemsetAsync(depthHist, 0, 4ull * 4 * 256, st));
-        dlsort::hist_k<8><<<depthGrid, dlsort::kThreads, 0, st>>>(keys0, ds, 4, 0, depthHist);
-        dlsort::scan_hist_k<8><<<4, 256, 0, st>>>(depthHist, 4);
-        uint32_t *kin = keys0, *kout = keys1, *vin = nullptr, *vout = vals1;
-        for (int p = 0; p < 4; p++) {
-            DL_CK(cudaMemsetAsync(sortStatus, 0, 4ull * 256 * depthGrid, st));
-            dlsort::Pass sp;
-            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
-            sp.segs = ds; sp.glob_off = depthHist; sp.status = sortStatus; sp.counter = scr + SC_DEPTH_CTR + p;
-            sp.err = scr + SC_ERR; sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
-            launch_pass_bits(8, sp, depthGrid, st);
-            std::swap(kin, kout);
-            vin = vout;
-            vout = (vout == vals1) ? vals0 : vals1;
-        }
-        DL_CK(cudaGetLastError());
-    }
-
-    // ---- emit, tile offsets, pair sort (pair capacity is fixed: overflow is an error)
-    int keyBits = 0;
-    while ((1u << keyBits) < std::max<uint32_t>(v.numTiles, 1)) keyBits++;
-    const int pbits = 8, ppasses = (keyBits + pbits - 1) / pbits;
-    dlr::EmitArgs ea;
-    ea.sorted_vals = vals0; ea.bbox = bbox; ea.nvis = nvis; ea.views = dView; ea.view_stride = stride;
-    ea.tiles_per_view = emitTiles; ea.pair_base = pairBase; ea.pair_cap = pairCap; ea.pair_keys = pkeys0;
-    ea.pair_vals = pvals0; ea.npairs = npairs; ea.tile_count = tileCount; ea.tile_stride = TS;
-    ea.status = emitStatus; ea.counter = scr + SC_EMIT_CTR; ea.err = scr + SC_ERR; ea.ovf = scr + SC_OVF;
-    dlr::emit_k<<<emitTiles, dlr::kEmitThreads, 0, st>>>(ea);
-    dlr::TileOffArgs ta;
-    ta.views = dView; ta.tile_count = tileCount; ta.tile_off = tileOff; ta.tile_stride = TS; ta.npairs = npairs;
-    ta.pair_cap = pairCap; ta.seg_len = pairSegLen; ta.glob_off = pairGlob; ta.bits = pbits; ta.passes = ppasses;
-    dlr::tile_offsets_k<<<1, 1024, 0, st>>>(ta);
-    DL_CK(cudaGetLastError());
-    uint32_t* finalVals = pvals0;
-    if (ppasses > 0) {
-        dlsort::Segs ps;
-        ps.start = pairBase; ps.len = pairSegLen; ps.tile_base = pairSegTileBase; ps.total_tiles = scr + SC_PAIR_TILES;
-        ps.num = 1;
-        dlsort::prepare_k<<<1, 32, 0, st>>>(ps);
-        uint32_t *kin = pkeys0, *kout = pkeys1, *vin = pvals0, *vout = pvals1;
-        for (int p = 0; p < ppasses; p++) {
-            DL_CK(cudaMemsetAsync(sortStatus, 0, 4ull * 256 * maxSortTiles, st));
-            dlsort::Pass sp;
-            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = (p + 1 < ppasses) ? kout : nullptr; sp.vals_out = vout;
-            sp.segs = ps; sp.glob_off = pairGlob; sp.status = sortStatus; sp.counter = scr + SC_PAIR_CTR + p;
-            sp.err = scr + SC_ERR; sp.shift = pbits * p; sp.pass = p; sp.passes = ppasses;
-            launch_pass_bits(pbits, sp, maxSortTiles, st);
-            std::swap(kin, kout);
-            std::swap(vin, vout);
-        }
-        finalVals = vin;
-        DL_CK(cudaGetLastError());
-    }
-
-    // ---- rasterize + finalize (exact exp, f32 records: same pixels as dl_render)
-    dlr::RasterArgs ra;
-    std::memset(&ra, 0, sizeof(ra));
-    ra.views = dView; ra.tile_off = tileOff; ra.tile_stride = TS; ra.pair_vals = finalVals; ra.pair_base = pairBase;
-    ra.recA = recA; ra.recBC = recBC; ra.recH = nullptr; ra.view_stride = stride; ra.outs = dOuts;
-    dlr::rasterize_k<true><<<dim3(v.numTiles, 1), dlr::kRasterThreads, 0, st>>>(ra);
-    DL_CK(cudaGetLastError());
+    uint64_t launches = 0;
+    uint32_t* finalVals = nullptr;
+    DL_TRY(launch_front(f, d, sc, st, nullptr, &launches));
+    DL_TRY(launch_back(f, d, st, nullptr, &launches, &finalVals));
 
     uint32_t flagsH[2] = {0, 0};
-    DL_CK(cudaMemcpyAsync(&flagsH[0], scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));
-    DL_CK(cudaMemcpyAsync(&flagsH[1], scr + SC_OVF, 4, cudaMemcpyDeviceToHost, st));
+    DL_CK(cudaMemcpyAsync(&flagsH[0], f.scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));
+    DL_CK(cudaMemcpyAsync(&flagsH[1], f.scr + SC_OVF, 4, cudaMemcpyDeviceToHost, st));
     DL_CK(cudaMemcpyAsync(out_rgba, rgba, pixels * 4, cudaMemcpyDeviceToHost, st));
     DL_CK(cudaStreamSynchronize(st));
     if (flagsH[0] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return DL_E_TIMEOUT; }

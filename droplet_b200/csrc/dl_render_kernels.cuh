@@ -5,9 +5,10 @@
 //   project.ts:59-234 project                    -> project_k (same f32 op order)
 //   radix-sort.ts:65-117 CPU depth sort          -> dlsort passes (dl_sort.cuh)
 //   prefix-sum.ts + pipeline.ts:277-304 scan     -> emit_k (decoupled look-back)
+//   (pair-sort digit offsets)                    -> pair_digits_k
 //   emit-pairs.ts:164-193 emit                    -> emit_k (load-balanced emission)
 //   pipeline.ts:544-578 stable pair sort          -> dlsort passes on tile ids
-//   find-boundaries.ts:17-99 tile offsets         -> tile_offsets_k (scan of per-tile counts)
+//   find-boundaries.ts:17-99 tile offsets         -> boundaries_k (direct writes, no atomics)
 //   rasterize.ts:135-181 + finalize.ts:211-224    -> rasterize_k (fused)
 //
 // All f32 arithmetic that feeds an integer decision or an output byte is
@@ -302,8 +303,8 @@ struct EmitArgs {
     uint32_t* pair_keys;
     uint32_t* pair_vals;
     unsigned long long* npairs;    // [V] out
-    uint32_t* tile_count;          // [V][tile_stride] (zeroed)
-    uint32_t tile_stride;
+    uint32_t* digit_hist;          // [V][4][256] (zeroed): tile-id digit counts for the pair sort
+    int bits, passes;              // digit width and count of the pair sort
     unsigned long long* status;    // [V][tiles_per_view] (zeroed)
     uint32_t* counter;
     uint32_t* err;                 // DL_DEVERR_TIMEOUT
@@ -326,9 +327,11 @@ __global__ void __launch_bounds__(kEmitThreads) emit_k(EmitArgs a) {
     __shared__ uint32_t s_tile;
     __shared__ unsigned long long s_prefix;
     __shared__ uint32_t s_skip;
+    __shared__ uint32_t s_dh[4 * 256];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
+    for (int i = tid; i < 4 * 256; i += kEmitThreads) s_dh[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint32_t v = tile / a.tiles_per_view;
@@ -417,7 +420,7 @@ __global__ void __launch_bounds__(kEmitThreads) emit_k(EmitArgs a) {
     __syncthreads();
     if (s_skip) return;
     const uint64_t outBase = a.pair_base[v] + s_prefix;
-    uint32_t* tc = a.tile_count + (uint64_t)v * a.tile_stride;
+    const uint32_t dmask = (1u << a.bits) - 1u;
     for (uint32_t o = tid; o < total; o += kEmitThreads) {
         // last rank slot whose exclusive offset is <= o
         uint32_t lo = 0, hi = kEmitRanks;
@@ -433,84 +436,79 @@ __global__ void __launch_bounds__(kEmitThreads) emit_k(EmitArgs a) {
         const uint32_t tileId = ty * u.tilesX + tx;
         a.pair_keys[outBase + o] = tileId;
         a.pair_vals[outBase + o] = s_g[lo];
-        atomicAdd(&tc[tileId], 1u);
+        for (int p = 0; p < a.passes; p++) atomicAdd(&s_dh[p * 256 + ((tileId >> (p * a.bits)) & dmask)], 1u);
     }
+    __syncthreads();
+    uint32_t* gh = a.digit_hist + (uint64_t)v * 4 * 256;
+    for (int i = tid; i < a.passes * 256; i += kEmitThreads)
+        if (s_dh[i]) atomicAdd(&gh[i], s_dh[i]);
 }
 
-// ------------------------------------------------------------------ tile offsets
-// tileOffsets[t] = number of pairs with tile < t (find-boundaries.ts semantics,
-// including start == end for empty tiles and tileOffsets[T] = numPairs), plus
-// the pair sort's per-view digit offsets and segment lengths.  One CTA per view.
-struct TileOffArgs {
-    const DlView* views;
-    const uint32_t* tile_count;    // [V][tile_stride]
-    uint32_t* tile_off;            // [V][tile_stride] (T+1 used)
-    uint32_t tile_stride;
+// ------------------------------------------------------------------ pair digits
+// Per view: exclusive scan of the emit kernel's tile-id digit histograms (the
+// pair sort's global digit offsets) and the pair-sort segment length (0 when
+// the view overflowed its pair buffer).  One CTA per view.
+struct PairDigitArgs {
+    const uint32_t* digit_hist;    // [V][4][256]
+    uint32_t* glob_off;            // [V][passes][radix]
     const unsigned long long* npairs;
     const uint64_t* pair_cap;
-    uint32_t* seg_len;             // [V] pair-sort segment lengths (0 on overflow)
-    uint32_t* glob_off;            // [V][passes][radix]
+    uint32_t* seg_len;
     int bits, passes;
 };
 
-__global__ void __launch_bounds__(1024) tile_offsets_k(TileOffArgs a) {
-    __shared__ uint32_t s_hist[4 * 256];
-    __shared__ uint32_t s_wsum[32];
-    __shared__ uint32_t s_carry;
+__global__ void pair_digits_k(PairDigitArgs a) {
     const uint32_t v = blockIdx.x;
-    const uint32_t T = a.views[v].numTiles;
-    const uint32_t* tc = a.tile_count + (uint64_t)v * a.tile_stride;
-    uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
     const int radix = 1 << a.bits;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < 4 * 256; i += blockDim.x) s_hist[i] = 0;
-    if (tid == 0) s_carry = 0;
-    __syncthreads();
-    for (uint32_t base = 0; base < T; base += blockDim.x) {
-        const uint32_t t = base + tid;
-        const uint32_t c = t < T ? tc[t] : 0u;
-        if (c) {
-            for (int p = 0; p < a.passes; p++) atomicAdd(&s_hist[p * 256 + ((t >> (p * a.bits)) & (radix - 1))], c);
-        }
-        uint32_t inc = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += x;
-        }
-        if (lane == 31) s_wsum[warp] = inc;
-        __syncthreads();
-        uint32_t wpre = 0, tot = 0;
-        for (int w = 0; w < (int)(blockDim.x / 32); w++) { if (w < warp) wpre += s_wsum[w]; tot += s_wsum[w]; }
-        if (t < T) to[t] = s_carry + wpre + inc - c;
-        __syncthreads();
-        if (tid == 0) s_carry += tot;
-        __syncthreads();
+    if (threadIdx.x < (unsigned)a.passes) {
+        const int p = threadIdx.x;
+        const uint32_t* h = a.digit_hist + ((uint64_t)v * 4 + p) * 256;
+        uint32_t* o = a.glob_off + ((uint64_t)v * a.passes + p) * radix;
+        uint32_t acc = 0;
+        for (int d = 0; d < radix; d++) { o[d] = acc; acc += h[d]; }
     }
-    if (tid == 0) {
-        to[T] = s_carry;
+    if (threadIdx.x == 0) {
         const bool ok = a.npairs[v] <= a.pair_cap[v];
         a.seg_len[v] = ok ? (uint32_t)a.npairs[v] : 0u;
     }
-    for (int p = 0; p < a.passes; p++) {
-        if (tid == 0) {
-            uint32_t acc = 0;
-            for (int d = 0; d < radix; d++) {
-                const uint32_t x = s_hist[p * 256 + d];
-                a.glob_off[((uint64_t)v * a.passes + p) * radix + d] = acc;
-                acc += x;
-            }
-        }
+}
+
+// ------------------------------------------------------------------ boundaries
+// find-boundaries.ts:31-99 on the sorted tile ids, with direct writes: the
+// thread at pair i writes tileOffsets[t] = i for every tile t in
+// (key[i-1], key[i]]; the thread at i = n writes n for the tiles after the
+// last key and the sentinel tileOffsets[T].  Each entry has exactly one writer.
+struct BoundArgs {
+    const DlView* views;
+    const uint32_t* keys;          // sorted tile ids, view v at pair_base[v]
+    const uint64_t* pair_base;
+    const uint32_t* seg_len;       // [V] pairs per view (0 on overflow)
+    uint32_t* tile_off;            // [V][tile_stride]
+    uint32_t tile_stride;
+};
+
+__global__ void boundaries_k(BoundArgs a) {
+    const uint32_t v = blockIdx.y;
+    const uint32_t n = a.seg_len[v];
+    const uint32_t T = a.views[v].numTiles;
+    const uint32_t* k = a.keys + a.pair_base[v];
+    uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+        const int64_t prev = i == 0 ? -1 : (int64_t)k[i - 1];
+        const int64_t cur = i == n ? (int64_t)T : (int64_t)k[i];
+        for (int64_t t = prev + 1; t <= cur; t++) to[t] = i;
     }
 }
 
 // ------------------------------------------------------------------ rasterize
-// One CTA per (view, 16x16 tile), one thread per pixel.  The tile's slice is
-// walked in batches of 256 pairs staged in shared memory; a staging thread
-// drops pairs whose screen box cannot reach any pixel centre of the tile
-// (conservative by one pixel, so no pixel's per-pixel box test could pass),
-// keeping order.  Each pixel then runs rasterize.ts:161-178 verbatim, and the
-// finalize shader (finalize.ts:211-224) is fused as the epilogue.
+// One CTA per (view, 16x16 tile), one thread per pixel; warp w owns the 8x4
+// sub-tile (w & 1, w >> 1).  The tile's slice is walked in batches of 256
+// pairs staged in shared memory.  A staging thread computes, from the splat's
+// screen box widened by one pixel, which of the 8 sub-tiles holds a pixel
+// centre whose per-pixel box test could pass, and drops the pair if none
+// (order kept).  Each warp then visits only the staged splats whose mask has
+// its bit, in slice order, and runs rasterize.ts:161-178 per pixel.
+// finalize.ts:211-224 is fused as the epilogue.
 struct RasterArgs {
     const DlView* views;
     const uint32_t* tile_off;      // [V][tile_stride]
@@ -531,6 +529,10 @@ struct RasterArgs {
 };
 
 constexpr int kRasterThreads = 256;
+// dl_expf(p) <= DL_GAUSS_FLOOR exactly when p <= -4.5f (dl_expf is monotone
+// there), so alpha = opacity * max(0, exp(p) - floor) is 0 and the splat is
+// skipped by the MIN_ALPHA test; skipping before the exp is result-identical.
+#define DL_POWER_CUT (-4.5f)
 
 template <bool kExactExp>
 __device__ __forceinline__ float raster_exp(float p) {
@@ -541,36 +543,54 @@ __device__ __forceinline__ float raster_exp(float p) {
 }
 
 template <bool kExactExp>
-__device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uint32_t tile,
-                                            float4* s_a, float4* s_b, float2* s_c, uint32_t* s_wc) {
+__device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uint32_t tile, float4* s_a, float4* s_b,
+                                            float2* s_c, uint8_t* s_m, uint32_t* s_wc) {
     const DlView& u = a.views[v];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
-    const uint32_t x = tx * DL_TILE + (tid & 15), y = ty * DL_TILE + (tid >> 4);
+    const uint32_t x = tx * DL_TILE + (warp & 1) * 8 + (lane & 7);
+    const uint32_t y = ty * DL_TILE + (warp >> 1) * 4 + (lane >> 3);
     const bool inImage = x < u.W && y < u.H;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
-    const float tx0 = (float)(tx * DL_TILE) + 0.5f - 1.0f, tx1 = (float)(tx * DL_TILE + DL_TILE - 1) + 0.5f + 1.0f;
-    const float ty0 = (float)(ty * DL_TILE) + 0.5f - 1.0f, ty1 = (float)(ty * DL_TILE + DL_TILE - 1) + 0.5f + 1.0f;
+    const float bx = (float)(tx * DL_TILE) + 0.5f, by = (float)(ty * DL_TILE) + 0.5f;
     const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
     const uint32_t start = to[tile], end = to[tile + 1];
     const uint32_t* vals = a.pair_vals + a.pair_base[v];
     const uint64_t vo = (uint64_t)v * a.view_stride;
+    const uint32_t myBit = 1u << warp;
 
     float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
     bool done = !inImage;
     uint32_t evals = 0;
     for (uint32_t b = start; b < end; b += kRasterThreads) {
-        // ---- stage: load, conservative tile-box filter, ordered compaction
+        // ---- stage: load, sub-tile mask (1 px margin), ordered compaction
         const uint32_t e = b + tid;
-        bool keep = false;
+        uint32_t mask = 0;
         float4 ra = make_float4(0, 0, 0, 0);
         uint32_t g = 0;
         if (e < end) {
             g = vals[e];
             ra = __ldg(a.recA + vo + g);
             const float r = ra.z;
-            keep = r > 0.0f && !(ra.x - r > tx1) && !(ra.x + r < tx0) && !(ra.y - r > ty1) && !(ra.y + r < ty0);
+            if (r > 0.0f) {
+                const float lo_x = ra.x - r, hi_x = ra.x + r, lo_y = ra.y - r, hi_y = ra.y + r;
+                uint32_t cm = 0, rm = 0;
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    const float x0 = bx + 8.0f * c - 1.0f, x1 = bx + 8.0f * c + 7.0f + 1.0f;
+                    if (!(lo_x > x1) && !(hi_x < x0)) cm |= 1u << c;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float y0 = by + 4.0f * q - 1.0f, y1 = by + 4.0f * q + 3.0f + 1.0f;
+                    if (!(lo_y > y1) && !(hi_y < y0)) rm |= 1u << q;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (rm & (1u << q)) mask |= cm << (2 * q);
+            }
         }
+        const bool keep = mask != 0;
         const uint32_t bal = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) s_wc[warp] = __popc(bal);
         __syncthreads();
@@ -595,28 +615,38 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uin
             s_a[slot] = make_float4(ra.x, ra.y, ra.z, A);
             s_b[slot] = make_float4(2.0f * B, C, al, cr);
             s_c[slot] = make_float2(cg, cb);
+            s_m[slot] = (uint8_t)mask;
         }
         __syncthreads();
-        // ---- per-pixel front-to-back compositing (rasterize.ts:161-178)
-        if (!done) {
-            for (uint32_t j = 0; j < nsurv; j++) {
-                const float4 sa = s_a[j];
-                const float dx = px - sa.x;
-                const float dy = py - sa.y;
-                if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
-                const float4 sb = s_b[j];
-                evals++;
-                const float power = -0.5f * ((((sa.w * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
-                if (power > 0.0f) continue;
-                const float alpha = fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
-                if (alpha < DL_MIN_ALPHA) continue;
-                const float w = T * alpha;
-                const float2 sc = s_c[j];
-                c0 = c0 + w * sb.w;
-                c1 = c1 + w * sc.x;
-                c2 = c2 + w * sc.y;
-                T = T * (1.0f - alpha);
-                if (T < DL_MIN_T) { done = true; break; }
+        // ---- this warp's splats, in slice order; per-pixel compositing
+        if (!__all_sync(0xffffffffu, done)) {
+            for (uint32_t c = 0; c < nsurv; c += 32) {
+                const uint32_t k = c + lane;
+                uint32_t m = __ballot_sync(0xffffffffu, k < nsurv && (s_m[k] & myBit));
+                while (m) {
+                    const uint32_t j = c + __ffs(m) - 1;
+                    m &= m - 1;
+                    if (done) continue;
+                    const float4 sa = s_a[j];
+                    const float dx = px - sa.x;
+                    const float dy = py - sa.y;
+                    if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
+                    const float4 sb = s_b[j];
+                    evals++;
+                    const float power = -0.5f * ((((sa.w * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
+                    if (power > 0.0f || power <= DL_POWER_CUT) continue;
+                    const float alpha =
+                        fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
+                    if (alpha < DL_MIN_ALPHA) continue;
+                    const float w = T * alpha;
+                    const float2 sc = s_c[j];
+                    c0 = c0 + w * sb.w;
+                    c1 = c1 + w * sc.x;
+                    c2 = c2 + w * sc.y;
+                    T = T * (1.0f - alpha);
+                    if (T < DL_MIN_T) done = true;
+                }
+                if (__all_sync(0xffffffffu, done)) break;
             }
         }
         if (__syncthreads_count(!done) == 0) break;
@@ -648,12 +678,13 @@ __global__ void __launch_bounds__(kRasterThreads) rasterize_k(RasterArgs a) {
     __shared__ float4 s_a[kRasterThreads];
     __shared__ float4 s_b[kRasterThreads];
     __shared__ float2 s_c[kRasterThreads];
+    __shared__ uint8_t s_m[kRasterThreads];
     __shared__ uint32_t s_wc[kRasterThreads / 32];
     __shared__ uint32_t s_item;
     if (a.work == nullptr) {
         const uint32_t v = blockIdx.y;
         if (blockIdx.x >= a.views[v].numTiles) return;
-        raster_tile<kExactExp>(a, v, blockIdx.x, s_a, s_b, s_c, s_wc);
+        raster_tile<kExactExp>(a, v, blockIdx.x, s_a, s_b, s_c, s_m, s_wc);
         return;
     }
     // persistent: pull (view, tile) items in the order of the work list
@@ -664,7 +695,7 @@ __global__ void __launch_bounds__(kRasterThreads) rasterize_k(RasterArgs a) {
         __syncthreads();
         if (i >= a.num_work) return;
         const uint32_t w = a.work[i];
-        raster_tile<kExactExp>(a, w >> 20, w & 0xfffffu, s_a, s_b, s_c, s_wc);
+        raster_tile<kExactExp>(a, w >> 20, w & 0xfffffu, s_a, s_b, s_c, s_m, s_wc);
         __syncthreads();
     }
 }
