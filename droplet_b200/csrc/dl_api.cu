@@ -70,7 +70,7 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
     if (!r) return DL_OK;
     cudaSetDevice(r->dev->ordinal);
     cudaStreamSynchronize(r->stream);
-    DevBuf* bufs[] = {&r->views, &r->segStart, &r->segLen, &r->segTileBase, &r->scratch, &r->keys0, &r->keys1,
+    DevBuf* bufs[] = {&r->views, &r->tileBase, &r->segStart, &r->segLen, &r->segTileBase, &r->scratch, &r->keys0, &r->keys1,
                       &r->vals0, &r->vals1, &r->recA, &r->recBC, &r->recH, &r->bbox, &r->nvis, &r->depthHist,
                       &r->sortStatus, &r->pairBase, &r->pairCap, &r->pkeys0, &r->pkeys1, &r->pvals0, &r->pvals1,
                       &r->npairs, &r->emitStatus, &r->tileCount, &r->tileOff, &r->pairSegLen, &r->pairSegTileBase,

@@ -70,7 +70,7 @@ struct dl_renderer {
     cudaStream_t own_stream = nullptr;
 
     // frame buffers (grow-only)
-    DevBuf views, segStart, segLen, segTileBase, scratch;     // scratch: counters + error word
+    DevBuf views, tileBase, segStart, segLen, segTileBase, scratch;     // scratch: counters + error word
     DevBuf keys0, keys1, vals0, vals1, recA, recBC, recH, bbox, nvis;
     DevBuf depthHist, sortStatus;
     DevBuf pairBase, pairCap, pkeys0, pkeys1, pvals0, pvals1, npairs, emitStatus;

@@ -89,8 +89,8 @@ int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlVie
     v->H = cam->height;
     v->tilesX = (cam->width + DL_TILE - 1) / DL_TILE;
     v->tilesY = (cam->height + DL_TILE - 1) / DL_TILE;
-    if (v->tilesX > 0xffffu || v->tilesY > 0xffffu || (uint64_t)v->tilesX * v->tilesY >= (1u << 20)) {
-        dl_set_error("image too large: at most 2^20 16x16 tiles and 65535 tiles per axis");
+    if (v->tilesX > 0x7fffu || v->tilesY > 0x7fffu || (uint64_t)v->tilesX * v->tilesY >= (1u << 20)) {
+        dl_set_error("image too large: at most 2^20 16x16 tiles and 32767 tiles per axis");
         return DL_E_CAPACITY;
     }
     v->numTiles = v->tilesX * v->tilesY;
@@ -160,6 +160,7 @@ namespace {
 // Device pointers of one frame's working set (renderer buffers or the static array).
 struct FramePtrs {
     DlView* views;
+    uint32_t* tileBase;            // [V+1] first global tile of each view
     uint64_t* segStart;
     uint32_t* segLen;
     uint32_t* segTileBase;
@@ -181,22 +182,44 @@ struct FramePtrs {
     uint32_t *pkeys0, *pkeys1, *pvals0, *pvals1;
     float4* accum;
     unsigned long long* evalCount;
+    const uint32_t* work;          // optional tile order for the rasterizer
+    uint32_t* tileEvals;           // optional per-tile counters (cost logging)
+    uint32_t* tileCycles;
 };
 
 struct FrameDims {
-    uint32_t V = 1, N = 0, maxT = 1, TS = 2;
+    uint32_t V = 1, N = 0, maxT = 1, TS = 2, totalTiles = 0, rasterGrid = 148;
     uint64_t stride = 64, cap = 0;
     uint32_t depthGrid = 1, emitTilesPerView = 1, pairGrid = 1;
     int pbits = 8, ppasses = 0;
     bool f16rec = false, fastExp = false;
 };
 
+// Persistent rasterizer grid: every SM filled to its occupancy limit.
+uint32_t raster_grid(bool fastExp) {
+    static int cached[64][2] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int* c = (dev >= 0 && dev < 64) ? &cached[dev][fastExp ? 1 : 0] : nullptr;
+    if (c && *c) return (uint32_t)*c;
+    int sms = 148, per = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (fastExp) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_k<false>, dlr::kRasterThreads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_k<true>, dlr::kRasterThreads, 0);
+    const int g = std::max(sms, 1) * std::max(per, 1);
+    if (c) *c = g;
+    return (uint32_t)g;
+}
+
 FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uint32_t flags) {
     FrameDims d;
     d.V = V;
     d.N = N;
     d.stride = round_up(std::max<uint32_t>(N, 1), 64);
-    for (uint32_t v = 0; v < V; v++) d.maxT = std::max(d.maxT, hv[v].numTiles);
+    for (uint32_t v = 0; v < V; v++) {
+        d.maxT = std::max(d.maxT, hv[v].numTiles);
+        d.totalTiles += hv[v].numTiles;
+    }
     d.TS = d.maxT + 1;
     d.depthGrid = std::max<uint32_t>(1, V * (uint32_t)((N + dlsort::kTile - 1) / dlsort::kTile));
     d.emitTilesPerView = (uint32_t)((d.stride + dlr::kEmitRanks - 1) / dlr::kEmitRanks);
@@ -207,6 +230,7 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     d.pairGrid = std::max<uint32_t>(1, (uint32_t)(V * ((cap + dlsort::kTile - 1) / dlsort::kTile)));
     d.f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
     d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
+    d.rasterGrid = raster_grid(d.fastExp);
     return d;
 }
 
@@ -356,6 +380,8 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     dlr::RasterArgs ra;
     std::memset(&ra, 0, sizeof(ra));
     ra.views = f.views;
+    ra.num_views = d.V;
+    ra.tile_base = f.tileBase;
     ra.tile_off = f.tileOff;
     ra.tile_stride = d.TS;
     ra.pair_vals = vals;
@@ -366,10 +392,14 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.view_stride = d.stride;
     ra.outs = f.outs;
     ra.accum = f.accum;
+    ra.work = f.work;
+    ra.num_items = 8u * d.totalTiles;
+    ra.work_counter = f.scr + SC_WORK_CTR;
     ra.eval_count = f.evalCount;
-    const dim3 rg(d.maxT, d.V);
-    if (d.fastExp) dlr::rasterize_k<false><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
-    else dlr::rasterize_k<true><<<rg, dlr::kRasterThreads, 0, st>>>(ra);
+    ra.tile_evals = f.tileEvals;
+    ra.tile_cycles = f.tileCycles;
+    if (d.fastExp) dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+    else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
     (*launches)++;
     DL_CK(cudaGetLastError());
     rec_event(ev, 7, st);
@@ -389,7 +419,9 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     r->launches = 0;
 
     // ---- buffers
+    if (d.totalTiles >= (1u << 29)) { dl_set_error("more than 2^29 tiles in one batch"); return DL_E_CAPACITY; }
     DL_TRY(r->views.ensure(sizeof(DlView) * V));
+    DL_TRY(r->tileBase.ensure(4ull * (V + 1)));
     DL_TRY(r->segStart.ensure(8ull * V));
     DL_TRY(r->segLen.ensure(4ull * V));
     DL_TRY(r->segTileBase.ensure(4ull * V));
@@ -421,6 +453,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     FramePtrs f;
     std::memset(&f, 0, sizeof(f));
     f.views = r->views.as<DlView>();
+    f.tileBase = r->tileBase.as<uint32_t>();
     f.segStart = r->segStart.as<uint64_t>();
     f.segLen = r->segLen.as<uint32_t>();
     f.segTileBase = r->segTileBase.as<uint32_t>();
@@ -447,7 +480,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     f.evalCount = countEvals ? r->evalCount.as<unsigned long long>() : nullptr;
 
     // ---- host-side tables (pinned staging), one upload
-    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + sizeof(void*) * V + 64;
+    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + sizeof(void*) * V + 4ull * (V + 1) + 64;
     DL_TRY(ensure_pinned((void**)&r->h_views, &r->h_views_cap, hbytes));
     char* hb = (char*)r->h_views;
     std::memcpy(hb, hv, sizeof(DlView) * V);
@@ -456,6 +489,10 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     for (uint32_t v = 0; v < V; v++) { hSegStart[v] = (uint64_t)v * d.stride; hSegLen[v] = N; }
     void** hOuts = (void**)(hSegLen + V + (V & 1));
     for (uint32_t v = 0; v < V; v++) hOuts[v] = d_outs[v];
+    uint32_t* hTileBase = (uint32_t*)(hOuts + V);
+    hTileBase[0] = 0;
+    for (uint32_t v = 0; v < V; v++) hTileBase[v + 1] = hTileBase[v] + hv[v].numTiles;
+    DL_CK(cudaMemcpyAsync(f.tileBase, hTileBase, 4ull * (V + 1), cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.views, hb, sizeof(DlView) * V, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.segStart, hSegStart, 8ull * V, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.segLen, hSegLen, 4ull * V, cudaMemcpyHostToDevice, st));
@@ -631,6 +668,7 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     FramePtrs f;
     std::memset(&f, 0, sizeof(f));
     f.views = c.take<DlView>(sizeof(DlView));
+    f.tileBase = c.take<uint32_t>(8);
     f.segStart = c.take<uint64_t>(8);
     f.segLen = c.take<uint32_t>(4);
     f.segTileBase = c.take<uint32_t>(4);
@@ -677,6 +715,8 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     uint32_t* outPtr = rgba;
     const uint64_t pairBaseH = 0, pairCapH = kStaticMaxPairs;
     DL_CK(cudaMemcpyAsync(f.views, &v, sizeof(DlView), cudaMemcpyHostToDevice, st));
+    const uint32_t tileBaseH[2] = {0u, v.numTiles};
+    DL_CK(cudaMemcpyAsync(f.tileBase, tileBaseH, 8, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.segStart, &segStart, 8, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.segLen, &segLen, 4, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.outs, &outPtr, sizeof(void*), cudaMemcpyHostToDevice, st));

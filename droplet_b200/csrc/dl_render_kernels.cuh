@@ -31,7 +31,8 @@ struct ProjectArgs {
     float4* recA;             // [V][stride] (screenX, screenY, radius, depth)
     float4* recBC;            // [V][stride][2] (A, B, C, alpha), (r, g, b, 0)   (f32 records)
     uint4* recH;              // [V][stride] half records: (A,B) (C,alpha) (r,g) (b,0)  (f16 records)
-    uint2* bbox;              // [V][stride] (minX | minY<<16, maxX | maxY<<16); empty if minX > maxX
+    uint2* bbox;              // [V][stride] (minX | minY<<16, maxX | maxY<<16), bit 15 of each max
+                              // field = box entirely left of / above the image; empty if minX > maxX
     uint32_t* nvis;           // [V] visible count
 };
 
@@ -270,10 +271,15 @@ __global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
         // project.ts:224-233 tile AABB (u32() saturates: off-screen left/top splats land in row/col 0)
         const uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
         const uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
-        const uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, floorf((screenX + radius) / 16.0f)));
-        const uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, floorf((screenY + radius) / 16.0f)));
+        const float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
+        const uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
+        const uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        // A box right edge left of x = 0 (or bottom edge above y = 0) still counts
+        // column (row) 0 after the saturation, but no pixel centre can pass its
+        // box test there: flag it so the rasterizer skips these pairs unread.
+        const uint32_t phantom = ((fx1 < 0.0f) ? 0x8000u : 0u) | ((fy1 < 0.0f) ? 0x80000000u : 0u);
         if (maxTX >= minTX && maxTY >= minTY)
-            a.bbox[o] = make_uint2(minTX | (minTY << 16), maxTX | (maxTY << 16));
+            a.bbox[o] = make_uint2(minTX | (minTY << 16), (maxTX | (maxTY << 16)) | phantom);
         else
             a.bbox[o] = make_uint2(0xffffu, 0u);
     }
@@ -311,8 +317,12 @@ struct EmitArgs {
     uint32_t* ovf;                 // DL_DEVERR_OVERFLOW
 };
 
+// Pair values carry this bit for splats whose box lies entirely left of or
+// above the image (see project_k); the splat index is in the low 30 bits.
+constexpr uint32_t kPhantomBit = 0x80000000u;
+
 __device__ __forceinline__ uint32_t bbox_count(uint2 bb, uint32_t maxCov) {
-    const uint32_t minX = bb.x & 0xffffu, minY = bb.x >> 16, maxX = bb.y & 0xffffu, maxY = bb.y >> 16;
+    const uint32_t minX = bb.x & 0xffffu, minY = bb.x >> 16, maxX = bb.y & 0x7fffu, maxY = (bb.y >> 16) & 0x7fffu;
     if (maxX < minX || maxY < minY) return 0u;
     const uint32_t c = (maxX - minX + 1u) * (maxY - minY + 1u);
     return c > maxCov ? maxCov : c;
@@ -354,10 +364,10 @@ __global__ void __launch_bounds__(kEmitThreads) emit_k(EmitArgs a) {
         if (r < n) {
             const uint32_t g = a.sorted_vals[vo + r];
             const uint2 bb = a.bbox[vo + g];
-            gs[j] = g;
+            gs[j] = g | ((bb.y & 0x80008000u) ? kPhantomBit : 0u);
             cnt[j] = bbox_count(bb, u.maxCoverage);
             mins[j] = bb.x;
-            spans[j] = (bb.y & 0xffffu) - (bb.x & 0xffffu) + 1u;
+            spans[j] = (bb.y & 0x7fffu) - (bb.x & 0xffffu) + 1u;
         }
         local += cnt[j];
     }
@@ -501,16 +511,23 @@ __global__ void boundaries_k(BoundArgs a) {
 }
 
 // ------------------------------------------------------------------ rasterize
-// One CTA per (view, 16x16 tile), one thread per pixel; warp w owns the 8x4
-// sub-tile (w & 1, w >> 1).  The tile's slice is walked in batches of 256
-// pairs staged in shared memory.  A staging thread computes, from the splat's
-// screen box widened by one pixel, which of the 8 sub-tiles holds a pixel
-// centre whose per-pixel box test could pass, and drops the pair if none
-// (order kept).  Each warp then visits only the staged splats whose mask has
-// its bit, in slice order, and runs rasterize.ts:161-178 per pixel.
-// finalize.ts:211-224 is fused as the epilogue.
+// Persistent, warp-granular rasterizer.  A work item is one 8x4-pixel
+// sub-tile (a quarter-row block) of one 16x16 tile of one view; each warp pulls
+// items from a queue (natural order, or the cost order of a work list) and
+// owns the item's 32 pixels, one per lane.  It walks its tile's slice 32 pairs
+// at a time: every lane loads one pair's screen record, keeps it if the
+// splat's box widened by one pixel reaches a pixel centre of the sub-tile (no
+// pixel whose per-pixel box test could pass is dropped), and the kept splats,
+// in slice order, are staged in warp-private shared memory and composited by
+// all 32 lanes with rasterize.ts:161-178 verbatim.  Pairs whose value has
+// kPhantomBit (a splat box wholly left of / above the image) are skipped
+// without reading their record: no pixel's box test can pass for them.  No CTA barrier: a warp
+// leaves as soon as its own pixels saturate.  finalize.ts:211-224 is fused as
+// the epilogue.
 struct RasterArgs {
     const DlView* views;
+    uint32_t num_views;
+    const uint32_t* tile_base;     // [V+1] first global tile of each view
     const uint32_t* tile_off;      // [V][tile_stride]
     uint32_t tile_stride;
     const uint32_t* pair_vals;     // sorted by tile, rank order within a tile
@@ -521,14 +538,16 @@ struct RasterArgs {
     uint64_t view_stride;
     uint32_t* const* outs;         // [V] packed RGBA8 per pixel
     float4* accum;                 // optional [W*H] (single view debug)
-    const uint32_t* work;          // optional persistent work list: (v << 20) | tile
-    uint32_t num_work;
+    const uint32_t* work;          // optional tile order (global tile ids); NULL: natural order
+    uint32_t num_items;            // 8 x total tiles
     uint32_t* work_counter;
     unsigned long long* eval_count;   // optional: total evaluated (pixel, splat) pairs
-    uint32_t* tile_evals;          // optional [V][tile_stride] per-tile evaluated-pair counts
+    uint32_t* tile_evals;          // optional [total tiles] evaluated pairs per tile
+    uint32_t* tile_cycles;         // optional [total tiles] SM cycles / 16 spent per tile
 };
 
 constexpr int kRasterThreads = 256;
+constexpr int kRasterWarps = kRasterThreads / 32;
 // dl_expf(p) <= DL_GAUSS_FLOOR exactly when p <= -4.5f (dl_expf is monotone
 // there), so alpha = opacity * max(0, exp(p) - floor) is 0 and the splat is
 // skipped by the MIN_ALPHA test; skipping before the exp is result-identical.
@@ -542,121 +561,115 @@ __device__ __forceinline__ float raster_exp(float p) {
     return y;
 }
 
+__device__ __forceinline__ uint32_t view_of_tile(const RasterArgs& a, uint32_t gt) {
+    uint32_t lo = 0, hi = a.num_views;        // last view with tile_base <= gt
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.tile_base[mid] <= gt) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 template <bool kExactExp>
-__device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uint32_t tile, float4* s_a, float4* s_b,
-                                            float2* s_c, uint8_t* s_m, uint32_t* s_wc) {
+__device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, uint32_t tile, uint32_t sub,
+                                               uint32_t gt, float4* s_a, float4* s_b, float2* s_c) {
     const DlView& u = a.views[v];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lane = threadIdx.x & 31;
     const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
-    const uint32_t x = tx * DL_TILE + (warp & 1) * 8 + (lane & 7);
-    const uint32_t y = ty * DL_TILE + (warp >> 1) * 4 + (lane >> 3);
+    const uint32_t sx0 = tx * DL_TILE + (sub & 1) * 8, sy0 = ty * DL_TILE + (sub >> 1) * 4;
+    const uint32_t x = sx0 + (lane & 7), y = sy0 + (lane >> 3);
     const bool inImage = x < u.W && y < u.H;
+    if (__all_sync(0xffffffffu, !inImage)) return;       // sub-tile entirely outside the image
+    const long long t0 = a.tile_cycles ? clock64() : 0;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
-    const float bx = (float)(tx * DL_TILE) + 0.5f, by = (float)(ty * DL_TILE) + 0.5f;
+    const float rx0 = (float)sx0 + 0.5f - 1.0f, rx1 = (float)sx0 + 7.5f + 1.0f;
+    const float ry0 = (float)sy0 + 0.5f - 1.0f, ry1 = (float)sy0 + 3.5f + 1.0f;
     const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
     const uint32_t start = to[tile], end = to[tile + 1];
     const uint32_t* vals = a.pair_vals + a.pair_base[v];
     const uint64_t vo = (uint64_t)v * a.view_stride;
-    const uint32_t myBit = 1u << warp;
+    const uint32_t lmask = dl_lanemask_lt();
 
     float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
     bool done = !inImage;
     uint32_t evals = 0;
-    for (uint32_t b = start; b < end; b += kRasterThreads) {
-        // ---- stage: load, sub-tile mask (1 px margin), ordered compaction
-        const uint32_t e = b + tid;
-        uint32_t mask = 0;
-        float4 ra = make_float4(0, 0, 0, 0);
-        uint32_t g = 0;
-        if (e < end) {
-            g = vals[e];
-            ra = __ldg(a.recA + vo + g);
-            const float r = ra.z;
-            if (r > 0.0f) {
-                const float lo_x = ra.x - r, hi_x = ra.x + r, lo_y = ra.y - r, hi_y = ra.y + r;
-                uint32_t cm = 0, rm = 0;
-#pragma unroll
-                for (int c = 0; c < 2; c++) {
-                    const float x0 = bx + 8.0f * c - 1.0f, x1 = bx + 8.0f * c + 7.0f + 1.0f;
-                    if (!(lo_x > x1) && !(hi_x < x0)) cm |= 1u << c;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const float y0 = by + 4.0f * q - 1.0f, y1 = by + 4.0f * q + 3.0f + 1.0f;
-                    if (!(lo_y > y1) && !(hi_y < y0)) rm |= 1u << q;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (rm & (1u << q)) mask |= cm << (2 * q);
-            }
+    for (uint32_t b = start; b < end; b += 64) {
+        // two chunks of 32 pairs per step: independent load chains in flight
+        const uint32_t e0 = b + lane, e1 = b + 32 + lane;
+        const uint32_t g0 = e0 < end ? __ldg(vals + e0) : kPhantomBit;
+        const uint32_t g1 = e1 < end ? __ldg(vals + e1) : kPhantomBit;
+        bool hit0 = false, hit1 = false;
+        float4 ra0 = make_float4(0, 0, 0, 0), ra1 = make_float4(0, 0, 0, 0);
+        if (!(g0 & kPhantomBit)) {
+            ra0 = __ldg(a.recA + vo + g0);
+            const float r = ra0.z;
+            hit0 = r > 0.0f && !(ra0.x - r > rx1) && !(ra0.x + r < rx0) && !(ra0.y - r > ry1) && !(ra0.y + r < ry0);
         }
-        const bool keep = mask != 0;
-        const uint32_t bal = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) s_wc[warp] = __popc(bal);
-        __syncthreads();
-        uint32_t before = 0, nsurv = 0;
+        if (!(g1 & kPhantomBit)) {
+            ra1 = __ldg(a.recA + vo + g1);
+            const float r = ra1.z;
+            hit1 = r > 0.0f && !(ra1.x - r > rx1) && !(ra1.x + r < rx0) && !(ra1.y - r > ry1) && !(ra1.y + r < ry0);
+        }
+        const uint32_t m0 = __ballot_sync(0xffffffffu, hit0);
+        const uint32_t m1 = __ballot_sync(0xffffffffu, hit1);
+        if ((m0 | m1) == 0u) continue;
 #pragma unroll
-        for (int w = 0; w < kRasterThreads / 32; w++) { if (w < warp) before += s_wc[w]; nsurv += s_wc[w]; }
-        if (keep) {
-            const uint32_t slot = before + __popc(bal & dl_lanemask_lt());
+        for (int h = 0; h < 2; h++) {
+            const bool hit = h ? hit1 : hit0;
+            if (!hit) continue;
+            const uint32_t g = h ? g1 : g0;
+            const float4 ra = h ? ra1 : ra0;
+            const uint32_t slot = h ? __popc(m0) + __popc(m1 & lmask) : __popc(m0 & lmask);
             float A, B, C, al, cr, cg, cb;
             if (a.recBC) {
                 const float4 p = __ldg(a.recBC + 2 * (vo + g));
                 const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
                 A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
             } else {
-                const uint4 h = __ldg(a.recH + vo + g);
-                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&h.x));
-                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&h.y));
-                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&h.z));
-                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&h.w));
+                const uint4 hv = __ldg(a.recH + vo + g);
+                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
+                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
+                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
+                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
                 A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
             }
             s_a[slot] = make_float4(ra.x, ra.y, ra.z, A);
             s_b[slot] = make_float4(2.0f * B, C, al, cr);
             s_c[slot] = make_float2(cg, cb);
-            s_m[slot] = (uint8_t)mask;
         }
-        __syncthreads();
-        // ---- this warp's splats, in slice order; per-pixel compositing
-        if (!__all_sync(0xffffffffu, done)) {
-            for (uint32_t c = 0; c < nsurv; c += 32) {
-                const uint32_t k = c + lane;
-                uint32_t m = __ballot_sync(0xffffffffu, k < nsurv && (s_m[k] & myBit));
-                while (m) {
-                    const uint32_t j = c + __ffs(m) - 1;
-                    m &= m - 1;
-                    if (done) continue;
-                    const float4 sa = s_a[j];
-                    const float dx = px - sa.x;
-                    const float dy = py - sa.y;
-                    if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
-                    const float4 sb = s_b[j];
-                    evals++;
-                    const float power = -0.5f * ((((sa.w * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
-                    if (power > 0.0f || power <= DL_POWER_CUT) continue;
-                    const float alpha =
-                        fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
-                    if (alpha < DL_MIN_ALPHA) continue;
-                    const float w = T * alpha;
-                    const float2 sc = s_c[j];
-                    c0 = c0 + w * sb.w;
-                    c1 = c1 + w * sc.x;
-                    c2 = c2 + w * sc.y;
-                    T = T * (1.0f - alpha);
-                    if (T < DL_MIN_T) done = true;
-                }
-                if (__all_sync(0xffffffffu, done)) break;
+        __syncwarp();
+        const uint32_t n = __popc(m0) + __popc(m1);
+        if (!done) {
+            for (uint32_t j = 0; j < n; j++) {
+                const float4 sa = s_a[j];
+                const float dx = px - sa.x;
+                const float dy = py - sa.y;
+                if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
+                const float4 sb = s_b[j];
+                evals++;
+                const float power = -0.5f * ((((sa.w * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
+                if (power > 0.0f || power <= DL_POWER_CUT) continue;
+                const float alpha =
+                    fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
+                if (alpha < DL_MIN_ALPHA) continue;
+                const float w = T * alpha;
+                const float2 sc = s_c[j];
+                c0 = c0 + w * sb.w;
+                c1 = c1 + w * sc.x;
+                c2 = c2 + w * sc.y;
+                T = T * (1.0f - alpha);
+                if (T < DL_MIN_T) { done = true; break; }
             }
         }
-        if (__syncthreads_count(!done) == 0) break;
+        if (__all_sync(0xffffffffu, done)) break;
+        __syncwarp();                                   // staging area is reused by the next step
     }
     if (a.tile_evals || a.eval_count) {
         uint32_t s = evals;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0 && s) {
-            if (a.tile_evals) atomicAdd(&a.tile_evals[(uint64_t)v * a.tile_stride + tile], s);
+            if (a.tile_evals) atomicAdd(&a.tile_evals[gt], s);
             if (a.eval_count) atomicAdd(a.eval_count, (unsigned long long)s);
         }
     }
@@ -671,32 +684,24 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, uint32_t v, uin
         a.outs[v][(uint64_t)y * u.W + x] = out;
         if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c0, c1, c2, T);
     }
+    if (a.tile_cycles && lane == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
 }
 
 template <bool kExactExp>
-__global__ void __launch_bounds__(kRasterThreads) rasterize_k(RasterArgs a) {
-    __shared__ float4 s_a[kRasterThreads];
-    __shared__ float4 s_b[kRasterThreads];
-    __shared__ float2 s_c[kRasterThreads];
-    __shared__ uint8_t s_m[kRasterThreads];
-    __shared__ uint32_t s_wc[kRasterThreads / 32];
-    __shared__ uint32_t s_item;
-    if (a.work == nullptr) {
-        const uint32_t v = blockIdx.y;
-        if (blockIdx.x >= a.views[v].numTiles) return;
-        raster_tile<kExactExp>(a, v, blockIdx.x, s_a, s_b, s_c, s_m, s_wc);
-        return;
-    }
-    // persistent: pull (view, tile) items in the order of the work list
+__global__ void __launch_bounds__(kRasterThreads, 5) rasterize_k(RasterArgs a) {
+    __shared__ float4 s_a[kRasterWarps][64];
+    __shared__ float4 s_b[kRasterWarps][64];
+    __shared__ float2 s_c[kRasterWarps][64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     while (true) {
-        if (threadIdx.x == 0) s_item = atomicAdd(a.work_counter, 1u);
-        __syncthreads();
-        const uint32_t i = s_item;
-        __syncthreads();
-        if (i >= a.num_work) return;
-        const uint32_t w = a.work[i];
-        raster_tile<kExactExp>(a, w >> 20, w & 0xfffffu, s_a, s_b, s_c, s_m, s_wc);
-        __syncthreads();
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.num_items) return;
+        const uint32_t gt = a.work ? a.work[item >> 3] : (item >> 3);
+        const uint32_t v = view_of_tile(a, gt);
+        raster_subtile<kExactExp>(a, v, gt - a.tile_base[v], item & 7u, gt, s_a[warp], s_b[warp], s_c[warp]);
+        __syncwarp();
     }
 }
 

@@ -9,7 +9,7 @@ ORACLE_FIELDS = ("rgba", "accum", "sorted_idx", "depth_keys", "records", "counts
 
 def bbox_count(bb, max_cov=16384):
     mnx, mny = bb[:, 0] & 0xFFFF, bb[:, 0] >> 16
-    mxx, mxy = bb[:, 1] & 0xFFFF, bb[:, 1] >> 16
+    mxx, mxy = bb[:, 1] & 0x7FFF, (bb[:, 1] >> 16) & 0x7FFF
     ok = (mxx >= mnx) & (mxy >= mny)
     c = (mxx.astype(np.int64) - mnx + 1) * (mxy.astype(np.int64) - mny + 1)
     return np.where(ok, np.minimum(c, max_cov), 0)
@@ -51,7 +51,13 @@ def assert_render_parity(g, o, max_cov=16384):
     assert np.array_equal(g["tile_off"], o["chunk_tile_offsets"] if o["n_pairs"] else np.zeros_like(g["tile_off"]))
     rank = np.empty(max(int(idx.max()) + 1 if nv else 1, 1), np.int64)
     rank[idx] = np.arange(nv)
-    assert np.array_equal(rank[g["pair_vals"].astype(np.int64)], o["tile_list_val"].astype(np.int64)), \
-        "tile pair lists differ"
+    pv = g["pair_vals"].astype(np.int64)
+    phantom = ((pv >> 31) & 1).astype(bool)
+    splat = pv & 0x3FFFFFFF
+    assert np.array_equal(rank[splat], o["tile_list_val"].astype(np.int64)), "tile pair lists differ"
+    # the flag marks exactly the splats whose box lies wholly left of / above the image
+    rA = g["recA"][splat]
+    wholly_out = (np.floor((rA[:, 0] + rA[:, 2]) / 16) < 0) | (np.floor((rA[:, 1] + rA[:, 2]) / 16) < 0)
+    assert np.array_equal(phantom, wholly_out), "phantom flags differ"
     assert np.array_equal(g["rgba"], o["rgba"]), "RGBA8 differs"
     assert np.array_equal(g["accum"].view(np.uint32), o["accum"].view(np.uint32)), "f32 accumulator differs"
