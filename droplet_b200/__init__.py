@@ -3,10 +3,10 @@ droplet scenes, behind droplet's public API (src/index.ts:16-38)."""
 from .types import (BackgroundRGBA, Bounds, RenderCamera, SplatData, mat4Identity, mat4LookAt,
                     numSHCoeffsPerChannel, quatRotate, splatInputStride, vec3)
 from ._lib import DropletError
-from .api import (BlockMaskBuffer, Device, Renderer, Scene, VoxelBlock, VoxelizeResult, createDevice,
+from .api import (BlockMaskBuffer, Device, Mlp, Renderer, Scene, VoxelBlock, VoxelizeResult, createDevice,
                   voxelize)
 
 __all__ = ["BackgroundRGBA", "Bounds", "RenderCamera", "SplatData", "mat4Identity", "mat4LookAt",
            "numSHCoeffsPerChannel", "quatRotate", "splatInputStride", "vec3", "DropletError",
-           "BlockMaskBuffer", "Device", "Renderer", "Scene", "VoxelBlock", "VoxelizeResult", "createDevice",
+           "BlockMaskBuffer", "Device", "Mlp", "Renderer", "Scene", "VoxelBlock", "VoxelizeResult", "createDevice",
            "voxelize"]

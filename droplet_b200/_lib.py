@@ -22,6 +22,9 @@ DL_BATCH_NO_GRAPH = 8
 DL_BATCH_STATIC = 16
 DL_BATCH_FAST_EXP = 32
 DL_BATCH_COUNT_EVALS = 64
+DL_BATCH_LOG_TILES = 128
+DL_MLP_IN, DL_MLP_HIDDEN = 12, 64
+DL_MLP_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = [
@@ -30,7 +33,8 @@ EXPORTS = [
     "dl_voxelize", "dl_vox_result_info", "dl_vox_result_copy", "dl_vox_result_free",
     "dl_renderer_debug_get", "dl_renderer_set_profiling", "dl_renderer_stage_times",
     "dl_renderer_launch_count", "dl_renderer_set_debug", "dl_render_many",
-    "dl_render_static",
+    "dl_render_static", "dl_mlp_create", "dl_mlp_destroy", "dl_mlp_get_params", "dl_mlp_set_params",
+    "dl_mlp_predict", "dl_mlp_grad", "dl_mlp_train", "dl_renderer_set_scheduler", "dl_renderer_tile_log",
 ]
 
 
@@ -88,6 +92,15 @@ def load():
         "dl_render_batch": [vp, vp, P(DlCamera), i, P(ctypes.c_float), P(vp), ctypes.c_uint32],
         "dl_render_many": [vp, P(DlSplats), P(DlCamera), i, P(ctypes.c_float), P(vp), ctypes.c_uint32],
         "dl_render_static": [P(DlSplats), P(DlCamera), P(ctypes.c_float), ctypes.c_uint32, vp, ctypes.c_size_t],
+        "dl_mlp_create": [vp, ctypes.c_uint64, P(vp)],
+        "dl_mlp_destroy": [vp],
+        "dl_mlp_get_params": [vp, vp, ctypes.c_size_t],
+        "dl_mlp_set_params": [vp, vp, ctypes.c_size_t],
+        "dl_mlp_predict": [vp, vp, ctypes.c_uint64, vp],
+        "dl_mlp_grad": [vp, vp, vp, ctypes.c_uint64, vp, P(ctypes.c_float)],
+        "dl_mlp_train": [vp, vp, vp, ctypes.c_uint64, i, i, ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)],
+        "dl_renderer_set_scheduler": [vp, vp],
+        "dl_renderer_tile_log": [vp, vp, vp, ctypes.c_uint64, P(ctypes.c_uint64)],
         "dl_voxelize": [vp, P(DlSplats), P(DlVoxOpts), P(vp)],
         "dl_vox_result_info": [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_uint64)],
         "dl_vox_result_copy": [vp, vp, vp, vp],

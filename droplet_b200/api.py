@@ -184,6 +184,25 @@ class Renderer:
         check(_lib.load().dl_render_batch(self.handle, scene._h, cams, n, _bg(background), ptrs, flags))
         return host
 
+    def set_scheduler(self, mlp: Optional["Mlp"]):
+        """Attach the learned tile-cost model (batched frames then rasterize
+        tiles longest-predicted first); None restores launch order."""
+        self._sched = mlp
+        check(_lib.load().dl_renderer_set_scheduler(self.handle, mlp.handle if mlp else None))
+
+    def tile_log(self):
+        """(features [T, 12], measured cost [T]) of the last frame rendered with
+        DL_BATCH_LOG_TILES."""
+        L = _lib.load()
+        n = ctypes.c_uint64()
+        check(L.dl_renderer_tile_log(self.handle, None, None, 0, ctypes.byref(n)))
+        T = int(n.value)
+        feats = np.empty((T, _lib.DL_MLP_IN), np.float32)
+        cost = np.empty(T, np.float32)
+        if T:
+            check(L.dl_renderer_tile_log(self.handle, feats.ctypes.data, cost.ctypes.data, T, ctypes.byref(n)))
+        return feats, cost
+
     # ---- instrumentation
     def set_stream(self, stream_ptr: Optional[int]):
         check(_lib.load().dl_renderer_set_stream(self.handle, stream_ptr))
@@ -337,3 +356,64 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
         L.dl_vox_result_free(h)
     return VoxelizeResult(BlockMaskBuffer(idx, lo, hi), Bounds(tuple(bmin), tuple(bmax)),
                           o.voxel_resolution, dims[0], dims[1], dims[2])
+
+
+# ---------------------------------------------------------------- learned tile-cost model
+class Mlp:
+    """The renderer's tile-cost model (12 -> 64 -> 64 -> 1, BF16 weights), trained
+    and evaluated by the library's own kernels."""
+
+    def __init__(self, device: Device, seed: int = 0):
+        h = ctypes.c_void_p()
+        check(_lib.load().dl_mlp_create(device.handle, seed, ctypes.byref(h)))
+        self._h = h.value
+        self.device = device
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise DropletError(_lib.DL_E_INVALID_ARG, "model is destroyed")
+        return self._h
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(_lib.DL_MLP_PARAMS, np.float32)
+        check(_lib.load().dl_mlp_get_params(self.handle, p.ctypes.data, p.size))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        check(_lib.load().dl_mlp_set_params(self.handle, p.ctypes.data, p.size))
+
+    def predict(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, _lib.DL_MLP_IN)
+        out = np.empty(len(X), np.float32)
+        check(_lib.load().dl_mlp_predict(self.handle, X.ctypes.data, len(X), out.ctypes.data))
+        return out
+
+    def grad(self, X, y):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, _lib.DL_MLP_IN)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.empty(_lib.DL_MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        check(_lib.load().dl_mlp_grad(self.handle, X.ctypes.data, y.ctypes.data, len(X), g.ctypes.data,
+                                      ctypes.byref(loss)))
+        return g, float(loss.value)
+
+    def train(self, X, y, epochs=10, batch=4096, lr=1e-3, seed=0) -> float:
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, _lib.DL_MLP_IN)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = ctypes.c_float()
+        check(_lib.load().dl_mlp_train(self.handle, X.ctypes.data, y.ctypes.data, len(X), epochs, batch, lr, seed,
+                                       ctypes.byref(loss)))
+        return float(loss.value)
+
+    def destroy(self):
+        if self._h:
+            _lib.load().dl_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -74,11 +74,13 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
                       &r->vals0, &r->vals1, &r->recA, &r->recBC, &r->recH, &r->bbox, &r->nvis, &r->depthHist,
                       &r->sortStatus, &r->pairBase, &r->pairCap, &r->pkeys0, &r->pkeys1, &r->pvals0, &r->pvals1,
                       &r->npairs, &r->emitStatus, &r->tileCount, &r->tileOff, &r->pairSegLen, &r->pairSegTileBase,
-                      &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->evalCount, &r->own_scene.mem};
+                      &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->evalCount, &r->own_scene.mem, &r->feat, &r->pred,
+                      &r->skeys0, &r->skeys1, &r->svals0, &r->svals1, &r->sseg, &r->sstatus, &r->shist, &r->tileCycles};
     for (DevBuf* b : bufs) b->release();
     if (r->h_views) cudaFreeHost(r->h_views);
     if (r->h_u64) cudaFreeHost(r->h_u64);
     for (auto& e : r->ev) if (e) cudaEventDestroy(e);
+    if (r->graph_exec) cudaGraphExecDestroy(r->graph_exec);
     delete r;
     return DL_OK;
 }
@@ -214,6 +216,28 @@ extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cam
             DL_CK(cudaMemcpyAsync(outs[i], dOuts[i], (uint64_t)views[i].W * views[i].H * 4, cudaMemcpyDeviceToHost, r->stream));
     }
     DL_CK(cudaStreamSynchronize(r->stream));
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_set_scheduler(dl_renderer* r, dl_mlp* mlp) {
+    if (!r) { dl_set_error("renderer is NULL"); return DL_E_INVALID_ARG; }
+    r->sched = mlp;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_tile_log(dl_renderer* r, float* features, float* cost, uint64_t cap, uint64_t* n) {
+    if (!r) { dl_set_error("renderer is NULL"); return DL_E_INVALID_ARG; }
+    const uint64_t T = r->log_tiles;
+    if (n) *n = T;
+    if (T == 0 || (!features && !cost)) return DL_OK;
+    if (cap < T) { dl_set_error("dl_renderer_tile_log: capacity smaller than the tile count"); return DL_E_INVALID_ARG; }
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    if (features) DL_CK(cudaMemcpy(features, r->feat.p, 48ull * T, cudaMemcpyDeviceToHost));
+    if (cost) {
+        std::vector<uint32_t> c(T);
+        DL_CK(cudaMemcpy(c.data(), r->tileCycles.p, 4ull * T, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < T; i++) cost[i] = (float)c[i];
+    }
     return DL_OK;
 }
 

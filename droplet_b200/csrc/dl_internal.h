@@ -99,7 +99,22 @@ struct dl_renderer {
     cudaEvent_t ev[8] = {};
     double stage_ms[6] = {0, 0, 0, 0, 0, 0};
     uint64_t launches = 0;
+
+    // CUDA graph of the last batched frame, replayed while its key matches
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<uint64_t> graph_key;
+    uint64_t graph_launches = 0;
+    uint64_t graph_replays = 0;
+    uint32_t* graph_final_vals = nullptr;
+
+    // learned schedule and tile-cost logging
+    dl_mlp* sched = nullptr;
+    DevBuf feat, pred, skeys0, skeys1, svals0, svals1, sseg, sstatus, shist, tileCycles;
+    uint32_t log_tiles = 0;
 };
+
+struct dl_mlp;
+int dl_mlp_infer_launch(const dl_mlp* mlp, const float* X, uint32_t n, float* out, cudaStream_t st);
 
 // dl_render.cu
 int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hviews, uint32_t V,

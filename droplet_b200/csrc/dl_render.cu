@@ -26,7 +26,9 @@ enum {
     SC_ERR = 10,
     SC_DEPTH_TILES = 11,
     SC_PAIR_TILES = 12,
-    SC_OVF = 13
+    SC_OVF = 13,
+    SC_SCHED_CTR = 14,     // 4 counters
+    SC_SCHED_TILES = 18
 };
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
@@ -185,6 +187,13 @@ struct FramePtrs {
     const uint32_t* work;          // optional tile order for the rasterizer
     uint32_t* tileEvals;           // optional per-tile counters (cost logging)
     uint32_t* tileCycles;
+    // learned schedule: features -> MLP -> longest-first tile order
+    float* feat;                   // [total tiles][12], or NULL
+    float* pred;
+    const dl_mlp* sched;           // NULL: no learned order
+    uint32_t *skeys0, *skeys1, *svals0, *svals1, *sstatus, *shist;
+    uint64_t* ssegStart;
+    uint32_t *ssegLen, *ssegTileBase;
 };
 
 struct FrameDims {
@@ -375,6 +384,45 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     dlr::boundaries_k<<<dim3(bgrid, d.V), 256, 0, st>>>(ba);
     (*launches)++;
     DL_CK(cudaGetLastError());
+
+    // learned schedule: per-tile features, predicted cost, tiles in decreasing order
+    const uint32_t* work = f.work;
+    if (f.feat && d.totalTiles) {
+        dlr::tile_features_k<<<(d.totalTiles + 255) / 256, 256, 0, st>>>(f.views, d.V, f.tileBase, f.tileOff, d.TS,
+                                                                         d.totalTiles, f.feat);
+        (*launches)++;
+        DL_CK(cudaGetLastError());
+    }
+    if (f.sched && f.feat && d.totalTiles) {
+        DL_TRY(dl_mlp_infer_launch(f.sched, f.feat, d.totalTiles, f.pred, st));
+        dlr::sched_keys_k<<<(d.totalTiles + 255) / 256, 256, 0, st>>>(f.pred, d.totalTiles, f.skeys0);
+        *launches += 2;
+        dlsort::Segs ss;
+        ss.start = f.ssegStart; ss.len = f.ssegLen; ss.tile_base = f.ssegTileBase;
+        ss.total_tiles = f.scr + SC_SCHED_TILES; ss.num = 1;
+        const uint32_t sgrid = (d.totalTiles + dlsort::kTile - 1) / dlsort::kTile;
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ss);
+        DL_CK(cudaMemsetAsync(f.shist, 0, 4ull * 4 * 256, st));
+        dlsort::hist_k<8><<<sgrid, dlsort::kThreads, 0, st>>>(f.skeys0, ss, 4, 0, f.shist);
+        dlsort::scan_hist_k<8><<<4, 256, 0, st>>>(f.shist, 4);
+        *launches += 3;
+        uint32_t *kin = f.skeys0, *kout = f.skeys1, *vin = nullptr, *vout = f.svals1;
+        for (int p = 0; p < 4; p++) {
+            DL_CK(cudaMemsetAsync(f.sstatus, 0, 4ull * 256 * sgrid, st));
+            dlsort::Pass sp;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = (p < 3) ? kout : nullptr; sp.vals_out = vout;
+            sp.segs = ss; sp.glob_off = f.shist; sp.status = f.sstatus;
+            sp.counter = f.scr + SC_SCHED_CTR + p;
+            sp.err = f.scr + SC_ERR; sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
+            launch_pass_bits(8, sp, sgrid, st);
+            (*launches)++;
+            std::swap(kin, kout);
+            vin = vout;
+            vout = (vout == f.svals1) ? f.svals0 : f.svals1;
+        }
+        work = vin;
+        DL_CK(cudaGetLastError());
+    }
     rec_event(ev, 6, st);
 
     dlr::RasterArgs ra;
@@ -392,7 +440,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.view_stride = d.stride;
     ra.outs = f.outs;
     ra.accum = f.accum;
-    ra.work = f.work;
+    ra.work = work;
     ra.num_items = 8u * d.totalTiles;
     ra.work_counter = f.scr + SC_WORK_CTR;
     ra.eval_count = f.evalCount;
@@ -450,8 +498,38 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     if (r->keep_accum && V == 1) DL_TRY(r->accum.ensure(16ull * hv[0].W * hv[0].H));
     if (countEvals) DL_TRY(r->evalCount.ensure(8));
 
+    // learned schedule (batched frames only) and tile-cost logging
+    const bool useSched = r->sched && !(flags & (DL_BATCH_PLAIN | DL_BATCH_STATIC));
+    const bool logTiles = (flags & DL_BATCH_LOG_TILES) != 0;
+    if (useSched || logTiles) {
+        DL_TRY(r->feat.ensure(48ull * d.totalTiles));
+        DL_TRY(r->pred.ensure(4ull * d.totalTiles));
+    }
+    if (useSched) {
+        const uint64_t sg = (d.totalTiles + dlsort::kTile - 1) / dlsort::kTile;
+        DL_TRY(r->skeys0.ensure(4ull * d.totalTiles));
+        DL_TRY(r->skeys1.ensure(4ull * d.totalTiles));
+        DL_TRY(r->svals0.ensure(4ull * d.totalTiles));
+        DL_TRY(r->svals1.ensure(4ull * d.totalTiles));
+        DL_TRY(r->sstatus.ensure(4ull * 256 * std::max<uint64_t>(sg, 1)));
+        DL_TRY(r->shist.ensure(4ull * 4 * 256));
+        DL_TRY(r->sseg.ensure(64));
+    }
+    if (logTiles) DL_TRY(r->tileCycles.ensure(4ull * d.totalTiles));
+
     FramePtrs f;
     std::memset(&f, 0, sizeof(f));
+    if (useSched || logTiles) { f.feat = r->feat.as<float>(); f.pred = r->pred.as<float>(); }
+    if (useSched) {
+        f.sched = r->sched;
+        f.skeys0 = r->skeys0.as<uint32_t>(); f.skeys1 = r->skeys1.as<uint32_t>();
+        f.svals0 = r->svals0.as<uint32_t>(); f.svals1 = r->svals1.as<uint32_t>();
+        f.sstatus = r->sstatus.as<uint32_t>(); f.shist = r->shist.as<uint32_t>();
+        f.ssegStart = r->sseg.as<uint64_t>();
+        f.ssegLen = (uint32_t*)(f.ssegStart + 1);
+        f.ssegTileBase = f.ssegLen + 1;
+    }
+    if (logTiles) f.tileCycles = r->tileCycles.as<uint32_t>();
     f.views = r->views.as<DlView>();
     f.tileBase = r->tileBase.as<uint32_t>();
     f.segStart = r->segStart.as<uint64_t>();
@@ -480,7 +558,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     f.evalCount = countEvals ? r->evalCount.as<unsigned long long>() : nullptr;
 
     // ---- host-side tables (pinned staging), one upload
-    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + sizeof(void*) * V + 4ull * (V + 1) + 64;
+    const size_t hbytes = sizeof(DlView) * V + 8ull * V + 4ull * V + sizeof(void*) * V + 4ull * (V + 1) + 128;
     DL_TRY(ensure_pinned((void**)&r->h_views, &r->h_views_cap, hbytes));
     char* hb = (char*)r->h_views;
     std::memcpy(hb, hv, sizeof(DlView) * V);
@@ -493,17 +571,21 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     hTileBase[0] = 0;
     for (uint32_t v = 0; v < V; v++) hTileBase[v + 1] = hTileBase[v] + hv[v].numTiles;
     DL_CK(cudaMemcpyAsync(f.tileBase, hTileBase, 4ull * (V + 1), cudaMemcpyHostToDevice, st));
+    if (useSched) {
+        uint64_t* hs = (uint64_t*)(hTileBase + V + 1 + ((V + 1) & 1));
+        hs[0] = 0;
+        reinterpret_cast<uint32_t*>(hs + 1)[0] = d.totalTiles;
+        reinterpret_cast<uint32_t*>(hs + 1)[1] = 0;
+        DL_CK(cudaMemcpyAsync(f.ssegStart, hs, 16, cudaMemcpyHostToDevice, st));
+    }
     DL_CK(cudaMemcpyAsync(f.views, hb, sizeof(DlView) * V, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.segStart, hSegStart, 8ull * V, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.segLen, hSegLen, 4ull * V, cudaMemcpyHostToDevice, st));
     DL_CK(cudaMemcpyAsync(f.outs, hOuts, sizeof(void*) * V, cudaMemcpyHostToDevice, st));
-    DL_CK(cudaMemsetAsync(f.scr, 0, 4ull * kScratchWords, st));
-    DL_CK(cudaMemsetAsync(f.nvis, 0, 4ull * V, st));
-    if (f.evalCount) DL_CK(cudaMemsetAsync(f.evalCount, 0, 8, st));
     cudaEvent_t* ev = r->profiling ? r->ev : nullptr;
-
     f.sortStatus = r->sortStatus.as<uint32_t>();
-    DL_TRY(launch_front(f, d, sc, st, ev, &r->launches));
+    const bool useGraph = !(flags & DL_BATCH_NO_GRAPH) && !(flags & DL_BATCH_PLAIN) && V > 1 && !r->profiling &&
+                          st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
 
     for (int attempt = 0; attempt < 3; attempt++) {
         const uint64_t cap = r->pair_cap_per_view;
@@ -522,7 +604,49 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         DL_CK(cudaMemcpyAsync(f.pairBase, r->h_u64, 8ull * V, cudaMemcpyHostToDevice, st));
         DL_CK(cudaMemcpyAsync(f.pairCap, r->h_u64 + V, 8ull * V, cudaMemcpyHostToDevice, st));
         uint32_t* finalVals = nullptr;
-        DL_TRY(launch_back(f, d, st, ev, &r->launches, &finalVals));
+        // the device sequence of the frame: clears, project, depth sort, pair stages
+        auto sequence = [&]() -> int {
+            DL_CK(cudaMemsetAsync(f.scr, 0, 4ull * kScratchWords, st));
+            DL_CK(cudaMemsetAsync(f.nvis, 0, 4ull * V, st));
+            if (f.evalCount) DL_CK(cudaMemsetAsync(f.evalCount, 0, 8, st));
+            if (f.tileCycles) DL_CK(cudaMemsetAsync(f.tileCycles, 0, 4ull * d.totalTiles, st));
+            uint64_t n = 0;
+            DL_TRY(launch_front(f, d, sc, st, ev, &n));
+            DL_TRY(launch_back(f, d, st, ev, &n, &finalVals));
+            r->launches = n;
+            return DL_OK;
+        };
+        if (!useGraph) {
+            DL_TRY(sequence());
+        } else {
+            // key: every pointer and size baked into the captured launches
+            std::vector<uint64_t> key;
+            const uint64_t* fp = reinterpret_cast<const uint64_t*>(&f);
+            key.assign(fp, fp + sizeof(FramePtrs) / 8);
+            const uint64_t* sp = reinterpret_cast<const uint64_t*>(&sc);
+            key.insert(key.end(), sp, sp + sizeof(DlSceneDev) / 8);
+            key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid});
+            if (!r->graph_exec || key != r->graph_key) {
+                if (r->graph_exec) { cudaGraphExecDestroy(r->graph_exec); r->graph_exec = nullptr; }
+                cudaGraph_t g = nullptr;
+                DL_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                const int cs = sequence();
+                const cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (cs != DL_OK) { if (g) cudaGraphDestroy(g); return cs; }
+                if (ce != cudaSuccess) { dl_set_error(std::string("stream capture: ") + cudaGetErrorString(ce)); return DL_E_CUDA; }
+                const cudaError_t ie = cudaGraphInstantiate(&r->graph_exec, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) { r->graph_exec = nullptr; dl_set_error(std::string("graph instantiate: ") + cudaGetErrorString(ie)); return DL_E_CUDA; }
+                r->graph_key = key;
+                r->graph_launches = r->launches;
+                r->graph_final_vals = finalVals;
+            } else {
+                finalVals = r->graph_final_vals;
+                r->launches = r->graph_launches;
+            }
+            DL_CK(cudaGraphLaunch(r->graph_exec, st));
+            r->graph_replays++;
+        }
 
         // one sync per frame: error word and pair totals
         DL_CK(cudaMemcpyAsync(r->h_u64, f.npairs, 8ull * V, cudaMemcpyDeviceToHost, st));
@@ -555,6 +679,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         r->last_rec_kind = d.f16rec ? 1 : 0;
         r->last_final_vals = finalVals;
         r->last_V = V;
+        r->log_tiles = logTiles ? d.totalTiles : 0;
         return DL_OK;
     }
     dl_set_error("pair buffers overflowed repeatedly");

@@ -510,6 +510,51 @@ __global__ void boundaries_k(BoundArgs a) {
     }
 }
 
+// ------------------------------------------------------------------ tile features
+// The 12 inputs of the learned cost model, per global tile, from the tile
+// offsets alone (computed after boundaries_k, before the rasterizer).
+__global__ void tile_features_k(const DlView* views, uint32_t V, const uint32_t* tile_base, const uint32_t* tile_off,
+                                uint32_t tile_stride, uint32_t total, float* __restrict__ X) {
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gt >= total) return;
+    uint32_t lo = 0, hi = V;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tile_base[mid] <= gt) lo = mid; else hi = mid;
+    }
+    const uint32_t v = lo;
+    const DlView& u = views[v];
+    const uint32_t t = gt - tile_base[v];
+    const int tx = (int)(t % u.tilesX), ty = (int)(t / u.tilesX);
+    const uint32_t* to = tile_off + (uint64_t)v * tile_stride;
+    auto cnt = [&](int x, int y) {
+        x = min(max(x, 0), (int)u.tilesX - 1);
+        y = min(max(y, 0), (int)u.tilesY - 1);
+        const uint32_t k = (uint32_t)y * u.tilesX + (uint32_t)x;
+        return (float)(to[k + 1] - to[k]);
+    };
+    float* x = X + (uint64_t)gt * 12;
+    x[0] = log1pf(cnt(tx, ty)) * 0.1f;
+    x[1] = log1pf(cnt(tx - 1, ty)) * 0.1f;
+    x[2] = log1pf(cnt(tx + 1, ty)) * 0.1f;
+    x[3] = log1pf(cnt(tx, ty - 1)) * 0.1f;
+    x[4] = log1pf(cnt(tx, ty + 1)) * 0.1f;
+    x[5] = ((float)tx + 0.5f) / (float)u.tilesX;
+    x[6] = ((float)ty + 0.5f) / (float)u.tilesY;
+    x[7] = ty == 0 ? 1.0f : 0.0f;
+    x[8] = tx == 0 ? 1.0f : 0.0f;
+    x[9] = logf((float)u.W * (float)u.H) * (1.0f / 16.0f);
+    x[10] = log1pf((float)to[u.numTiles] / (float)u.numTiles) * 0.1f;
+    const float wx = fminf(16.0f, (float)u.W - 16.0f * tx), wy = fminf(16.0f, (float)u.H - 16.0f * ty);
+    x[11] = wx * wy * (1.0f / 256.0f);
+}
+
+// Sort key for longest-predicted-first: ascending order of -prediction.
+__global__ void sched_keys_k(const float* __restrict__ pred, uint32_t n, uint32_t* __restrict__ keys) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = dl_sortable_key(-pred[i]);
+}
+
 // ------------------------------------------------------------------ rasterize
 // Persistent, warp-granular rasterizer.  A work item is one 8x4-pixel
 // sub-tile (a quarter-row block) of one 16x16 tile of one view; each warp pulls

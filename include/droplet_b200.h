@@ -117,7 +117,8 @@ enum {
     DL_BATCH_NO_GRAPH = 8,        /* launch directly instead of replaying a CUDA graph */
     DL_BATCH_STATIC = 16,         /* rasterize tiles in launch order, not cost order */
     DL_BATCH_FAST_EXP = 32,       /* hardware ex2 in the rasterizer (+-1 LSB) */
-    DL_BATCH_COUNT_EVALS = 64     /* count evaluated (pixel, splat) pairs ("evals") */
+    DL_BATCH_COUNT_EVALS = 64,    /* count evaluated (pixel, splat) pairs ("evals") */
+    DL_BATCH_LOG_TILES = 128      /* keep per-tile features and measured cost (dl_renderer_tile_log) */
 };
 /* Render n views of one resident scene; outs[i] receives cams[i].width *
  * cams[i].height RGBA8 pixels (host or device memory, per flags). */
@@ -144,6 +145,36 @@ int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams,
  * max_coverage 0 selects the default 16384. */
 int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg[4], uint32_t max_coverage,
                      uint8_t* out_rgba, size_t out_len);
+
+/* ---- learned schedule (no reference counterpart: the reference rasterizes
+ * tiles in dispatch order, src/render/pipeline.ts:402-422).  A small MLP
+ * (DL_MLP_IN features -> 64 -> 64 -> 1, ReLU, BF16 weights, FP32 accumulation)
+ * predicts each tile's rasterizer cost; with a scheduler attached, batched
+ * frames (not DL_BATCH_PLAIN / DL_BATCH_STATIC) rasterize tiles in decreasing
+ * predicted cost.  The order changes timing only, never a pixel. */
+#define DL_MLP_IN 12
+#define DL_MLP_HIDDEN 64
+#define DL_MLP_PARAMS (DL_MLP_IN * DL_MLP_HIDDEN + DL_MLP_HIDDEN + DL_MLP_HIDDEN * DL_MLP_HIDDEN + DL_MLP_HIDDEN + \
+                       DL_MLP_HIDDEN + 1)
+typedef struct dl_mlp dl_mlp;
+int dl_mlp_create(dl_device* dev, uint64_t seed, dl_mlp** out);
+int dl_mlp_destroy(dl_mlp* mlp);
+/* FP32 master parameters, layout W1[IN][H], b1[H], W2[H][H], b2[H], W3[H], b3. */
+int dl_mlp_get_params(dl_mlp* mlp, float* out, size_t n);
+int dl_mlp_set_params(dl_mlp* mlp, const float* in, size_t n);
+/* X: n x DL_MLP_IN row-major host array; out: n predictions. */
+int dl_mlp_predict(dl_mlp* mlp, const float* X, uint64_t n, float* out);
+/* Gradient of the mean squared error over the n samples w.r.t. the parameters. */
+int dl_mlp_grad(dl_mlp* mlp, const float* X, const float* y, uint64_t n, float* grad_out, float* loss_out);
+/* Adam on mini-batches of `batch` samples, reshuffled each epoch from `seed`. */
+int dl_mlp_train(dl_mlp* mlp, const float* X, const float* y, uint64_t n, int epochs, int batch, float lr,
+                 uint64_t seed, float* loss_out);
+/* Attach (or with NULL detach) the cost model that orders batched frames. */
+int dl_renderer_set_scheduler(dl_renderer* r, dl_mlp* mlp);
+/* After a frame rendered with DL_BATCH_LOG_TILES: per tile (views in order,
+ * tiles row-major) its DL_MLP_IN features and measured cost (SM cycles / 16
+ * summed over the tile's warps).  *n receives the tile count. */
+int dl_renderer_tile_log(dl_renderer* r, float* features, float* cost, uint64_t cap, uint64_t* n);
 
 /* ---- voxelizer: src/voxel/voxelize.ts:59-248 voxelize(device, data, opts) */
 int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_opts* opts, dl_vox_result** out);

@@ -1,0 +1,102 @@
+"""The learned tile-cost model: its hand-written GPU kernels against a float64
+NumPy restatement, and the guarantee that the schedule it produces changes no
+pixel.  The gain it brings is measured in bench.py (value vs static_value)."""
+import numpy as np
+import pytest
+
+import droplet_b200 as dl
+from droplet_b200 import _lib, learned, synth
+
+pytestmark = pytest.mark.gpu
+IN, H = _lib.DL_MLP_IN, _lib.DL_MLP_HIDDEN
+
+
+def bf16(a):
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def unpack(p):
+    o = 0
+    W1 = p[o:o + IN * H].reshape(IN, H); o += IN * H
+    b1 = p[o:o + H]; o += H
+    W2 = p[o:o + H * H].reshape(H, H); o += H * H
+    b2 = p[o:o + H]; o += H
+    W3 = p[o:o + H]; o += H
+    return W1, b1, W2, b2, W3, p[o]
+
+
+def numpy_grad(p, X, t):
+    """float64 forward/backward of the BF16-weight MLP (straight-through rounding)."""
+    W1, b1, W2, b2, W3, b3 = [np.asarray(a, np.float64) for a in unpack(bf16(p).astype(np.float64))]
+    X = X.astype(np.float64)
+    a1 = X @ W1 + b1; h1 = np.maximum(a1, 0)
+    a2 = h1 @ W2 + b2; h2 = np.maximum(a2, 0)
+    y = h2 @ W3 + b3
+    e = y - t
+    loss = (e ** 2).mean()
+    gy = 2 * e / len(t)
+    gW3 = h2.T @ gy; gb3 = gy.sum()
+    g2 = np.outer(gy, W3) * (a2 > 0)
+    gW2 = h1.T @ g2; gb2 = g2.sum(0)
+    g1 = (g2 @ W2.T) * (a1 > 0)
+    gW1 = X.T @ g1; gb1 = g1.sum(0)
+    return np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3, [gb3]]), loss, y
+
+
+def test_gradients_match_float64(device):
+    rng = np.random.default_rng(0)
+    m = dl.Mlp(device, seed=3)
+    X = rng.normal(0, 1, (3000, IN)).astype(np.float32)
+    t = rng.normal(0, 1, 3000).astype(np.float32)
+    g, loss = m.grad(X, t)
+    ref, ref_loss, y = numpy_grad(m.get_params(), X, t)
+    assert loss == pytest.approx(ref_loss, rel=1e-4)
+    assert np.linalg.norm(g - ref) / np.linalg.norm(ref) < 1e-4
+    assert np.allclose(m.predict(X[:100]), y[:100], rtol=1e-4, atol=1e-4)
+
+
+def test_training_fits_a_tile_cost_like_target(device):
+    rng = np.random.default_rng(1)
+    X = rng.uniform(0, 1, (60000, IN)).astype(np.float32)
+    t = (2 * X[:, 0] + np.sin(3 * X[:, 5]) - X[:, 7] * X[:, 1]).astype(np.float32)
+    m = dl.Mlp(device, seed=1)
+    before = float(((m.predict(X) - t) ** 2).mean())
+    m.train(X, t, epochs=20, batch=1024, lr=3e-3, seed=0)
+    after = float(((m.predict(X) - t) ** 2).mean())
+    assert after < 0.05 * before and after < 0.01
+
+
+def test_schedule_changes_no_pixel(device):
+    d = synth.cluster_scene(300_000, seed=17, clusters=64, extent=10.0, bands=3)
+    cams = synth.ring_cameras(8, resolutions=[(640, 360), (1280, 720)])
+    r = dl.Renderer(device)
+    sc = r.upload(d, "f16")
+    flags = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
+    base = r.render_batch(sc, cams, flags=flags)
+    models = [dl.Mlp(device, seed=5)]
+    trained = learned.load_default(device)
+    if trained is not None:
+        models.append(trained)
+    for m in models:
+        r.set_scheduler(m)
+        got = r.render_batch(sc, cams, flags=flags)
+        again = r.render_batch(sc, cams, flags=flags | _lib.DL_BATCH_NO_GRAPH)
+        for a, b, c in zip(base, got, again):
+            assert np.array_equal(a, b) and np.array_equal(a, c)
+    r.set_scheduler(None)
+
+
+def test_tile_log_covers_every_tile(device):
+    d = synth.cluster_scene(50_000, seed=18, clusters=16, extent=10.0)
+    r = dl.Renderer(device)
+    sc = r.upload(d)
+    cam = synth.pinhole(640, 360, (0.0, 2.0, 12.0))
+    r.render_batch(sc, [cam], flags=_lib.DL_BATCH_PLAIN | _lib.DL_BATCH_LOG_TILES)
+    f, c = r.tile_log()
+    assert f.shape == (40 * 23, IN) and len(c) == 40 * 23
+    assert np.all(np.isfinite(f)) and np.all(c > 0)
+    # feature 0 is log1p(pairs in the tile) / 10: recover the per-tile counts
+    off = r.debug_get("tile_off", np.uint32)
+    assert np.allclose(np.expm1(f[:, 0] * 10), np.diff(off.astype(np.int64)), rtol=1e-3, atol=1e-2)
