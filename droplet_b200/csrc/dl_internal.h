@@ -115,6 +115,7 @@ struct dl_renderer {
 
 struct dl_mlp;
 int dl_mlp_infer_launch(const dl_mlp* mlp, const float* X, uint32_t n, float* out, cudaStream_t st);
+const void* dl_mlp_weights(const dl_mlp* mlp);   // device BF16 parameters
 
 // dl_render.cu
 int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hviews, uint32_t V,

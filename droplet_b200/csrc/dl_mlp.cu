@@ -24,48 +24,11 @@
 #include <vector>
 
 #include "dl_internal.h"
+#include "dl_mlp.cuh"
 
 namespace {
 
-constexpr int kIn = DL_MLP_IN, kH = DL_MLP_HIDDEN;
-// parameter layout (f32 count): W1 [kIn][kH], b1 [kH], W2 [kH][kH], b2 [kH], W3 [kH], b3
-constexpr int oW1 = 0, oB1 = oW1 + kIn * kH, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH,
-              oB3 = oW3 + kH, kParams = oB3 + 1;
-static_assert(kParams == DL_MLP_PARAMS, "parameter count");
-
-__device__ __forceinline__ void load_params(const __nv_bfloat16* w, float* s) {
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) s[i] = __bfloat162float(w[i]);
-    __syncthreads();
-}
-
-// forward for one sample; writes hidden activations when h1/h2 are given
-__device__ __forceinline__ float mlp_forward(const float* P, const float* x, float* h1, float* h2) {
-    float a1[kH];
-#pragma unroll
-    for (int j = 0; j < kH; j++) a1[j] = P[oB1 + j];
-#pragma unroll
-    for (int i = 0; i < kIn; i++) {
-        const float xi = x[i];
-#pragma unroll
-        for (int j = 0; j < kH; j++) a1[j] += xi * P[oW1 + i * kH + j];
-    }
-#pragma unroll
-    for (int j = 0; j < kH; j++) a1[j] = fmaxf(a1[j], 0.0f);
-    if (h1) {
-#pragma unroll
-        for (int j = 0; j < kH; j++) h1[j] = a1[j];
-    }
-    float y = P[oB3];
-    for (int j = 0; j < kH; j++) {
-        float a = P[oB2 + j];
-#pragma unroll
-        for (int k = 0; k < kH; k++) a += a1[k] * P[oW2 + k * kH + j];
-        a = fmaxf(a, 0.0f);
-        if (h2) h2[j] = a;
-        y += a * P[oW3 + j];
-    }
-    return y;
-}
+using namespace dlmlp;
 
 __global__ void __launch_bounds__(128) mlp_infer_k(const __nv_bfloat16* w, const float* __restrict__ X, uint32_t n,
                                                    float* __restrict__ out) {
@@ -75,7 +38,7 @@ __global__ void __launch_bounds__(128) mlp_infer_k(const __nv_bfloat16* w, const
         float x[kIn];
 #pragma unroll
         for (int i = 0; i < kIn; i++) x[i] = X[(uint64_t)s * kIn + i];
-        out[s] = mlp_forward(P, x, nullptr, nullptr);
+        out[s] = forward(P, x, nullptr, nullptr);
     }
 }
 
@@ -96,7 +59,7 @@ __global__ void __launch_bounds__(128) mlp_fwd_bwd_k(const __nv_bfloat16* w, con
     for (int i = 0; i < kIn; i++) { x[i] = X[(uint64_t)s * kIn + i]; xs[(uint64_t)b * kIn + i] = x[i]; }
     float* h1 = h1s + (uint64_t)b * kH;
     float* h2 = h2s + (uint64_t)b * kH;
-    const float y = mlp_forward(P, x, h1, h2);
+    const float y = forward(P, x, h1, h2);
     const float e = y - Y[s];
     atomicAdd(loss, e * e / (float)B);
     const float dy = 2.0f * e / (float)B;
@@ -167,6 +130,8 @@ struct dl_mlp {
     DevBuf X, Y, idx, xs, h1s, h2s, g1s, g2s, gy;
     uint64_t steps = 0;
 };
+
+const void* dl_mlp_weights(const dl_mlp* mlp) { return mlp->w.p; }
 
 int dl_mlp_infer_launch(const dl_mlp* mlp, const float* X, uint32_t n, float* out, cudaStream_t st) {
     if (n == 0) return DL_OK;

@@ -387,41 +387,24 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
 
     // learned schedule: per-tile features, predicted cost, tiles in decreasing order
     const uint32_t* work = f.work;
-    if (f.feat && d.totalTiles) {
+    if (f.feat && !f.sched && d.totalTiles) {
         dlr::tile_features_k<<<(d.totalTiles + 255) / 256, 256, 0, st>>>(f.views, d.V, f.tileBase, f.tileOff, d.TS,
                                                                          d.totalTiles, f.feat);
         (*launches)++;
         DL_CK(cudaGetLastError());
     }
-    if (f.sched && f.feat && d.totalTiles) {
-        DL_TRY(dl_mlp_infer_launch(f.sched, f.feat, d.totalTiles, f.pred, st));
-        dlr::sched_keys_k<<<(d.totalTiles + 255) / 256, 256, 0, st>>>(f.pred, d.totalTiles, f.skeys0);
-        *launches += 2;
-        dlsort::Segs ss;
-        ss.start = f.ssegStart; ss.len = f.ssegLen; ss.tile_base = f.ssegTileBase;
-        ss.total_tiles = f.scr + SC_SCHED_TILES; ss.num = 1;
-        const uint32_t sgrid = (d.totalTiles + dlsort::kTile - 1) / dlsort::kTile;
-        dlsort::prepare_k<<<1, 32, 0, st>>>(ss);
-        DL_CK(cudaMemsetAsync(f.shist, 0, 4ull * 4 * 256, st));
-        dlsort::hist_k<8><<<sgrid, dlsort::kThreads, 0, st>>>(f.skeys0, ss, 4, 0, f.shist);
-        dlsort::scan_hist_k<8><<<4, 256, 0, st>>>(f.shist, 4);
+    if (f.sched && d.totalTiles) {
+        const uint32_t g = std::min<uint32_t>((d.totalTiles + dlr::kSchedThreads - 1) / dlr::kSchedThreads, 2048);
+        DL_CK(cudaMemsetAsync(f.shist, 0, 4ull * 256 * d.V, st));
+        dlr::sched_pred_k<<<g, dlr::kSchedThreads, 0, st>>>(f.views, d.V, f.tileBase, f.tileOff, d.TS, d.totalTiles,
+                                                            (const __nv_bfloat16*)dl_mlp_weights(f.sched), f.svals1,
+                                                            f.shist);
+        dlr::sched_scan_k<<<d.V, 32, 0, st>>>(f.tileBase, f.shist);
+        dlr::sched_scatter_k<<<std::min<uint32_t>((d.totalTiles + 255) / 256, 2048), 256, 0, st>>>(
+            f.svals1, d.totalTiles, f.shist, f.svals0);
         *launches += 3;
-        uint32_t *kin = f.skeys0, *kout = f.skeys1, *vin = nullptr, *vout = f.svals1;
-        for (int p = 0; p < 4; p++) {
-            DL_CK(cudaMemsetAsync(f.sstatus, 0, 4ull * 256 * sgrid, st));
-            dlsort::Pass sp;
-            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = (p < 3) ? kout : nullptr; sp.vals_out = vout;
-            sp.segs = ss; sp.glob_off = f.shist; sp.status = f.sstatus;
-            sp.counter = f.scr + SC_SCHED_CTR + p;
-            sp.err = f.scr + SC_ERR; sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
-            launch_pass_bits(8, sp, sgrid, st);
-            (*launches)++;
-            std::swap(kin, kout);
-            vin = vout;
-            vout = (vout == f.svals1) ? f.svals0 : f.svals1;
-        }
-        work = vin;
         DL_CK(cudaGetLastError());
+        work = f.svals0;
     }
     rec_event(ev, 6, st);
 
@@ -512,7 +495,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         DL_TRY(r->svals0.ensure(4ull * d.totalTiles));
         DL_TRY(r->svals1.ensure(4ull * d.totalTiles));
         DL_TRY(r->sstatus.ensure(4ull * 256 * std::max<uint64_t>(sg, 1)));
-        DL_TRY(r->shist.ensure(4ull * 4 * 256));
+        DL_TRY(r->shist.ensure(4ull * 256 * std::max<uint32_t>(V, 4)));
         DL_TRY(r->sseg.ensure(64));
     }
     if (logTiles) DL_TRY(r->tileCycles.ensure(4ull * d.totalTiles));

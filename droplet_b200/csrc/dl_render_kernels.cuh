@@ -19,6 +19,8 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 
+#include "dl_mlp.cuh"
+
 namespace dlr {
 
 // ------------------------------------------------------------------ project
@@ -511,29 +513,16 @@ __global__ void boundaries_k(BoundArgs a) {
 }
 
 // ------------------------------------------------------------------ tile features
-// The 12 inputs of the learned cost model, per global tile, from the tile
-// offsets alone (computed after boundaries_k, before the rasterizer).
-__global__ void tile_features_k(const DlView* views, uint32_t V, const uint32_t* tile_base, const uint32_t* tile_off,
-                                uint32_t tile_stride, uint32_t total, float* __restrict__ X) {
-    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gt >= total) return;
-    uint32_t lo = 0, hi = V;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (tile_base[mid] <= gt) lo = mid; else hi = mid;
-    }
-    const uint32_t v = lo;
-    const DlView& u = views[v];
-    const uint32_t t = gt - tile_base[v];
+// The 12 inputs of the learned cost model for tile t of view u, from the tile
+// offsets alone (available after boundaries_k, before the rasterizer).
+__device__ __forceinline__ void tile_features(const DlView& u, const uint32_t* to, uint32_t t, float* x) {
     const int tx = (int)(t % u.tilesX), ty = (int)(t / u.tilesX);
-    const uint32_t* to = tile_off + (uint64_t)v * tile_stride;
-    auto cnt = [&](int x, int y) {
-        x = min(max(x, 0), (int)u.tilesX - 1);
-        y = min(max(y, 0), (int)u.tilesY - 1);
-        const uint32_t k = (uint32_t)y * u.tilesX + (uint32_t)x;
+    auto cnt = [&](int cx, int cy) {
+        cx = min(max(cx, 0), (int)u.tilesX - 1);
+        cy = min(max(cy, 0), (int)u.tilesY - 1);
+        const uint32_t k = (uint32_t)cy * u.tilesX + (uint32_t)cx;
         return (float)(to[k + 1] - to[k]);
     };
-    float* x = X + (uint64_t)gt * 12;
     x[0] = log1pf(cnt(tx, ty)) * 0.1f;
     x[1] = log1pf(cnt(tx - 1, ty)) * 0.1f;
     x[2] = log1pf(cnt(tx + 1, ty)) * 0.1f;
@@ -549,10 +538,63 @@ __global__ void tile_features_k(const DlView* views, uint32_t V, const uint32_t*
     x[11] = wx * wy * (1.0f / 256.0f);
 }
 
-// Sort key for longest-predicted-first: ascending order of -prediction.
-__global__ void sched_keys_k(const float* __restrict__ pred, uint32_t n, uint32_t* __restrict__ keys) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) keys[i] = dl_sortable_key(-pred[i]);
+// Per global tile features (cost logging).
+__global__ void tile_features_k(const DlView* views, uint32_t V, const uint32_t* tile_base, const uint32_t* tile_off,
+                                uint32_t tile_stride, uint32_t total, float* __restrict__ X) {
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gt >= total) return;
+    uint32_t lo = 0, hi = V;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tile_base[mid] <= gt) lo = mid; else hi = mid;
+    }
+    tile_features(views[lo], tile_off + (uint64_t)lo * tile_stride, gt - tile_base[lo], X + (uint64_t)gt * 12);
+}
+
+// The learned order.  sched_pred_k: per tile (all views in parallel) the
+// features, the MLP's prediction and an 8-bit bucket that decreases with the
+// predicted cost, counted per view; sched_scan_k: per view, bucket offsets
+// after the view's first tile; sched_scatter_k: tiles into the work list by
+// bucket.  Views keep their launch order (their tiles share splat records in
+// L2); inside a view tiles go most expensive bucket first, and inside a bucket
+// in whatever order the atomics give — any order yields the same pixels.
+constexpr int kSchedThreads = 128;
+__global__ void __launch_bounds__(kSchedThreads) sched_pred_k(const DlView* views, uint32_t V, const uint32_t* tile_base,
+                                                              const uint32_t* tile_off, uint32_t tile_stride,
+                                                              uint32_t total, const __nv_bfloat16* w,
+                                                              uint32_t* __restrict__ bucket, uint32_t* __restrict__ vhist) {
+    __shared__ float P[dlmlp::kParams];
+    dlmlp::load_params(w, P);
+    for (uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x; gt < total; gt += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = V;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (tile_base[mid] <= gt) lo = mid; else hi = mid;
+        }
+        float x[12];
+        tile_features(views[lo], tile_off + (uint64_t)lo * tile_stride, gt - tile_base[lo], x);
+        const float y = dlmlp::forward(P, x, nullptr, nullptr);
+        const float q = (y == y) ? fminf(fmaxf((y + 4.0f) * 32.0f, 0.0f), 255.0f) : 0.0f;  // standardised log cost
+        const uint32_t b = 255u - (uint32_t)q;                                               // 0 = most expensive
+        bucket[gt] = (lo << 8) | b;
+        atomicAdd(&vhist[lo * 256 + b], 1u);
+    }
+}
+
+__global__ void sched_scan_k(const uint32_t* tile_base, uint32_t* vhist) {
+    const uint32_t v = blockIdx.x;
+    if (threadIdx.x == 0) {
+        uint32_t acc = tile_base[v];
+        for (int b = 0; b < 256; b++) { const uint32_t c = vhist[v * 256 + b]; vhist[v * 256 + b] = acc; acc += c; }
+    }
+}
+
+__global__ void sched_scatter_k(const uint32_t* __restrict__ bucket, uint32_t total, uint32_t* vhist,
+                                uint32_t* __restrict__ work) {
+    for (uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x; gt < total; gt += gridDim.x * blockDim.x) {
+        const uint32_t vb = bucket[gt];
+        work[atomicAdd(&vhist[(vb >> 8) * 256 + (vb & 255u)], 1u)] = gt;
+    }
 }
 
 // ------------------------------------------------------------------ rasterize
@@ -678,13 +720,19 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
                 A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
             }
-            s_a[slot] = make_float4(ra.x, ra.y, ra.z, A);
-            s_b[slot] = make_float4(2.0f * B, C, al, cr);
+            if (kExactExp) {
+                s_a[slot] = make_float4(ra.x, ra.y, ra.z, A);
+                s_b[slot] = make_float4(2.0f * B, C, al, cr);
+            } else {
+                // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
+                s_a[slot] = make_float4(ra.x, ra.y, ra.z, -0.72134752044448170f * A);
+                s_b[slot] = make_float4(-1.4426950408889634f * B, -0.72134752044448170f * C, al, cr);
+            }
             s_c[slot] = make_float2(cg, cb);
         }
         __syncwarp();
         const uint32_t n = __popc(m0) + __popc(m1);
-        if (!done) {
+        if (!done && kExactExp) {
             for (uint32_t j = 0; j < n; j++) {
                 const float4 sa = s_a[j];
                 const float dx = px - sa.x;
@@ -703,6 +751,30 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 c1 = c1 + w * sc.x;
                 c2 = c2 + w * sc.y;
                 T = T * (1.0f - alpha);
+                if (T < DL_MIN_T) { done = true; break; }
+            }
+        } else if (!done) {
+            // +-1 LSB variant: fused multiply-adds and the hardware ex2 on the
+            // pre-scaled quadratic form (same skips, same order of splats)
+            for (uint32_t j = 0; j < n; j++) {
+                const float4 sa = s_a[j];
+                const float dx = px - sa.x;
+                const float dy = py - sa.y;
+                if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
+                const float4 sb = s_b[j];
+                evals++;
+                const float p2 = __fmaf_rn(dx, __fmaf_rn(sa.w, dx, sb.x * dy), sb.y * dy * dy);
+                if (p2 > 0.0f || p2 <= -6.4921275f) continue;          // -4.5 * log2(e)
+                float e;
+                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
+                const float alpha = fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, e - DL_GAUSS_FLOOR));
+                if (alpha < DL_MIN_ALPHA) continue;
+                const float w = T * alpha;
+                const float2 sc = s_c[j];
+                c0 = __fmaf_rn(w, sb.w, c0);
+                c1 = __fmaf_rn(w, sc.x, c1);
+                c2 = __fmaf_rn(w, sc.y, c2);
+                T = __fmaf_rn(-T, alpha, T);
                 if (T < DL_MIN_T) { done = true; break; }
             }
         }
