@@ -30,6 +30,7 @@
 // for voxels whose opacity lies within float rounding of the cutoff.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -97,6 +98,7 @@ struct VoxParams {
     const double* qmn[3];           // per-axis batch box (f64)
     const double* qmx[3];
     const float* bmin32[3];         // per-axis f32 batch min (BatchInfo.blockMin*)
+    int64_t zlo, zhi;               // block z range of the slab being processed
 };
 
 __global__ void vox_prep_k(VoxParams p, float* __restrict__ ext, VoxRec* __restrict__ rec, double* __restrict__ part) {
@@ -190,6 +192,24 @@ __device__ void axis_range(const VoxParams& p, int a, float c, float e, float eh
     v1 = min(v1 + 1, NB - 1);
     lo = max(v0, blo * 16);
     hi = min(v1, min(bhi * 16 + 15, NB - 1));
+    if (a == 2) { lo = max(lo, p.zlo); hi = min(hi, p.zhi); }
+}
+
+// Gaussian-block pairs per 16-block z row of batches (sizes the slabs).
+__global__ void vox_zcount_k(VoxParams p, const float* __restrict__ ext, unsigned long long* __restrict__ zcount) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= p.n) return;
+    int64_t lo[3], hi[3];
+    for (int k = 0; k < 3; k++) {
+        const float e = ext[3ull * g + k];
+        axis_range(p, k, p.pos[3ull * g + k], e, e + p.half, lo[k], hi[k]);
+    }
+    if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2]) return;
+    const unsigned long long xy = (unsigned long long)(hi[0] - lo[0] + 1) * (unsigned long long)(hi[1] - lo[1] + 1);
+    for (int64_t bz = lo[2] >> 4; bz <= (hi[2] >> 4); bz++) {
+        const int64_t z0 = max(lo[2], bz * 16), z1 = min(hi[2], bz * 16 + 15);
+        atomicAdd(&zcount[bz], xy * (unsigned long long)(z1 - z0 + 1));
+    }
 }
 
 constexpr int kVT = 256, kVI = 4, kVR = kVT * kVI;
@@ -648,12 +668,54 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     if ((s = B.scratch.ensure(4 * VS_WORDS)) != DL_OK) return fail(s);
     uint32_t* scr = B.scratch.as<uint32_t>();
 
-    // ---- binning with retry on overflow
-    unsigned long long cap = std::max<unsigned long long>(1ull << 22, 16ull * n);
-    unsigned long long npairs = 0;
+    // ---- slabs of 16-block z rows of batches, each within the pair capacity.
+    // Blocks are appended in batch order (z rows outermost), so processing the
+    // rows in order and concatenating reproduces the reference's block order.
+    // (DL_VOX_SLAB_PAIRS lowers the capacity, to exercise the slab loop on small inputs.)
+    unsigned long long kSlabCap = 1ull << 29;
+    if (const char* env = std::getenv("DL_VOX_SLAB_PAIRS")) {
+        const unsigned long long e = std::strtoull(env, nullptr, 10);
+        if (e > 0 && e < kSlabCap) kSlabCap = e;
+    }
+    std::vector<unsigned long long> zc((size_t)p.NBB[2], 0ull);
+    {
+        DevBuf zcount;
+        if ((s = zcount.ensure(8ull * p.NBB[2])) != DL_OK) return fail(s);
+        cudaMemsetAsync(zcount.p, 0, 8ull * p.NBB[2], st);
+        p.zlo = 0;
+        p.zhi = p.NB[2] - 1;
+        vox_zcount_k<<<prepGrid, 256, 0, st>>>(p, B.ext.as<float>(), zcount.as<unsigned long long>());
+        if (cudaMemcpyAsync(zc.data(), zcount.p, 8ull * p.NBB[2], cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            dl_set_error(std::string("voxelize count: ") + cudaGetErrorString(cudaGetLastError()));
+            return fail(DL_E_CUDA);
+        }
+    }
+    std::vector<std::pair<int64_t, int64_t>> slabs;     // [bz0, bz1) in batch rows
+    {
+        int64_t b0 = 0;
+        unsigned long long acc = 0;
+        for (int64_t bz = 0; bz < p.NBB[2]; bz++) {
+            if (zc[bz] > kSlabCap && kSlabCap == (1ull << 29)) {
+                dl_set_error("one 16-block z row needs more than 2^29 Gaussian-block pairs");
+                return fail(DL_E_CAPACITY);
+            }
+            if (acc + zc[bz] > kSlabCap && bz > b0) { slabs.push_back({b0, bz}); b0 = bz; acc = 0; }
+            acc += zc[bz];
+        }
+        slabs.push_back({b0, p.NBB[2]});
+    }
     const uint32_t emitTiles = (uint32_t)((n + kVR - 1) / kVR);
-    for (int attempt = 0; attempt < 3; attempt++) {
-        if (cap >= (1ull << 30)) { dl_set_error("more than 2^30 Gaussian-block pairs"); return fail(DL_E_CAPACITY); }
+    int keyBits = 12;
+    while ((1ull << (keyBits - 12)) < numBatches) keyBits++;
+    const int passes = (keyBits + 7) / 8;
+    for (const auto& slab : slabs) {
+        unsigned long long cap = 0;
+        for (int64_t bz = slab.first; bz < slab.second; bz++) cap += zc[bz];
+        if (cap == 0) continue;
+        p.zlo = slab.first * 16;
+        p.zhi = std::min<int64_t>(slab.second * 16, p.NB[2]) - 1;
+        // ---- binning (exactly `cap` pairs)
         if ((s = B.keys0.ensure(4 * cap)) != DL_OK || (s = B.vals0.ensure(4 * cap)) != DL_OK ||
             (s = B.status.ensure(8ull * std::max<uint64_t>(emitTiles, 1))) != DL_OK)
             return fail(s);
@@ -664,135 +726,134 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         ea.cap = cap; ea.npairs = (unsigned long long*)(scr + 14); ea.status = B.status.as<unsigned long long>();
         ea.counter = scr + VS_EMIT; ea.err = scr + VS_ERR; ea.ovf = scr + VS_OVF;
         vox_emit_k<<<emitTiles, kVT, 0, st>>>(ea);
-        uint32_t h[16];
-        if (cudaMemcpyAsync(h, scr, 64, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
-            dl_set_error(std::string("voxelize binning: ") + cudaGetErrorString(cudaGetLastError()));
-            return fail(DL_E_CUDA);
-        }
-        if (h[VS_ERR] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return fail(DL_E_TIMEOUT); }
-        if (h[VS_OVF] & 4u) { dl_set_error("a Gaussian overlaps more than 2^31 blocks"); return fail(DL_E_CAPACITY); }
-        std::memcpy(&npairs, &h[14], 8);
-        if (h[VS_OVF] & DL_DEVERR_OVERFLOW) { cap = npairs + npairs / 8 + 1024; continue; }
-        break;
-    }
-    if (npairs > cap) { dl_set_error("binning overflowed repeatedly"); return fail(DL_E_CAPACITY); }
-
-    // ---- cutoff <= 0: every voxel of every batch with a non-empty list is solid
-    if (!(p.cutoff > 0.0f) && p.cutoff <= 0.0f) {
-        std::vector<uint32_t> hk(npairs);
-        if (npairs && cudaMemcpy(hk.data(), B.keys0.p, 4 * npairs, cudaMemcpyDeviceToHost) != cudaSuccess) {
-            dl_set_error("voxelize: copy failed");
-            return fail(DL_E_CUDA);
-        }
-        std::vector<char> used(numBatches, 0);
-        for (uint32_t k : hk) used[k >> 12] = 1;
-        for (uint64_t b = 0; b < numBatches; b++) {
-            if (!used[b]) continue;
-            const int64_t bxI = b % p.NBB[0], byI = (b / p.NBB[0]) % p.NBB[1], bzI = b / (p.NBB[0] * p.NBB[1]);
-            const int64_t cx = std::min<int64_t>(16, p.NB[0] - bxI * 16), cy = std::min<int64_t>(16, p.NB[1] - byI * 16);
-            const int64_t cz = std::min<int64_t>(16, p.NB[2] - bzI * 16);
-            for (int64_t bi = 0; bi < cx * cy * cz; bi++) {
-                const int64_t ax = bxI * 16 + bi % cx, ay = byI * 16 + (bi / cx) % cy, az = bzI * 16 + bi / (cx * cy);
-                R->idx.push_back((uint32_t)(ax + ay * p.NB[0] + az * p.NB[0] * p.NB[1]));
-                R->lo.push_back(0xffffffffu);
-                R->hi.push_back(0xffffffffu);
+        unsigned long long npairs = 0;
+        {
+            uint32_t h[16];
+            if (cudaMemcpyAsync(h, scr, 64, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                dl_set_error(std::string("voxelize binning: ") + cudaGetErrorString(cudaGetLastError()));
+                return fail(DL_E_CUDA);
             }
+            if (h[VS_ERR] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return fail(DL_E_TIMEOUT); }
+            if (h[VS_OVF] & 4u) { dl_set_error("a Gaussian overlaps more than 2^31 blocks"); return fail(DL_E_CAPACITY); }
+            if (h[VS_OVF] & DL_DEVERR_OVERFLOW) { dl_set_error("voxelize: binning disagrees with its count"); return fail(DL_E_CAPACITY); }
+            std::memcpy(&npairs, &h[14], 8);
         }
-        *out = R;
-        return DL_OK;
-    }
 
-    // ---- stable sort by block key
-    int keyBits = 12;
-    while ((1ull << (keyBits - 12)) < numBatches) keyBits++;
-    const int passes = (keyBits + 7) / 8;
-    const uint32_t sortTiles = (uint32_t)std::max<unsigned long long>(1, (npairs + dlsort::kTile - 1) / dlsort::kTile);
-    if ((s = B.keys1.ensure(4 * std::max<unsigned long long>(npairs, 1))) != DL_OK ||
-        (s = B.vals1.ensure(4 * std::max<unsigned long long>(npairs, 1))) != DL_OK ||
-        (s = B.status.ensure(std::max<uint64_t>(4ull * 256 * sortTiles, 8ull * ((npairs + kVR - 1) / kVR + 1)))) != DL_OK ||
-        (s = B.hist.ensure(4ull * 4 * 256)) != DL_OK || (s = B.segs.ensure(64)) != DL_OK)
-        return fail(s);
-    uint32_t* keysF = B.keys0.as<uint32_t>();
-    uint32_t* valsF = B.vals0.as<uint32_t>();
-    if (npairs > 0) {
-        uint64_t* segStart = B.segs.as<uint64_t>();
-        uint32_t* segLen = (uint32_t*)(segStart + 1);
-        uint32_t* segTileBase = segLen + 1;
-        cudaMemsetAsync(segStart, 0, 8, st);
-        const uint32_t len32 = (uint32_t)npairs;
-        cudaMemcpyAsync(segLen, &len32, 4, cudaMemcpyHostToDevice, st);
-        dlsort::Segs sg;
-        sg.start = segStart; sg.len = segLen; sg.tile_base = segTileBase; sg.total_tiles = scr + VS_TILES; sg.num = 1;
-        dlsort::prepare_k<<<1, 32, 0, st>>>(sg);
-        cudaMemsetAsync(B.hist.p, 0, 4ull * 4 * 256, st);
-        dlsort::hist_k<8><<<std::min<uint32_t>(sortTiles, 4096), dlsort::kThreads, 0, st>>>(keysF, sg, passes, 0, B.hist.as<uint32_t>());
-        dlsort::scan_hist_k<8><<<passes, 256, 0, st>>>(B.hist.as<uint32_t>(), passes);
-        uint32_t *kin = keysF, *kout = B.keys1.as<uint32_t>(), *vin = valsF, *vout = B.vals1.as<uint32_t>();
-        for (int ps = 0; ps < passes; ps++) {
-            cudaMemsetAsync(B.status.p, 0, 4ull * 256 * sortTiles, st);
-            dlsort::Pass sp;
-            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout; sp.segs = sg;
-            sp.glob_off = B.hist.as<uint32_t>(); sp.status = B.status.as<uint32_t>(); sp.counter = scr + VS_SORT + ps;
-            sp.err = scr + VS_ERR; sp.shift = 8 * ps; sp.pass = ps; sp.passes = passes;
-            dlsort::pass_k<8><<<sortTiles, dlsort::kThreads, 0, st>>>(sp);
-            std::swap(kin, kout);
-            std::swap(vin, vout);
+        // ---- cutoff <= 0: every voxel of every batch with a non-empty list is solid
+        if (!(p.cutoff > 0.0f) && p.cutoff <= 0.0f) {
+            std::vector<uint32_t> hk(npairs);
+            if (npairs && cudaMemcpy(hk.data(), B.keys0.p, 4 * npairs, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                dl_set_error("voxelize: copy failed");
+                return fail(DL_E_CUDA);
+            }
+            std::vector<char> used(numBatches, 0);
+            for (uint32_t k : hk) used[k >> 12] = 1;
+            for (uint64_t b = 0; b < numBatches; b++) {
+                if (!used[b]) continue;
+                const int64_t bxI = b % p.NBB[0], byI = (b / p.NBB[0]) % p.NBB[1], bzI = b / (p.NBB[0] * p.NBB[1]);
+                const int64_t cx = std::min<int64_t>(16, p.NB[0] - bxI * 16), cy = std::min<int64_t>(16, p.NB[1] - byI * 16);
+                const int64_t cz = std::min<int64_t>(16, p.NB[2] - bzI * 16);
+                for (int64_t bi = 0; bi < cx * cy * cz; bi++) {
+                    const int64_t ax = bxI * 16 + bi % cx, ay = byI * 16 + (bi / cx) % cy, az = bzI * 16 + bi / (cx * cy);
+                    R->idx.push_back((uint32_t)(ax + ay * p.NB[0] + az * p.NB[0] * p.NB[1]));
+                    R->lo.push_back(0xffffffffu);
+                    R->hi.push_back(0xffffffffu);
+                }
+            }
+            continue;
         }
-        keysF = kin;
-        valsF = vin;
-    }
-    // ---- blocks, evaluation, compaction
-    const uint64_t maxBlocks = std::max<unsigned long long>(npairs, 1);
-    if ((s = B.bkey.ensure(4 * maxBlocks)) != DL_OK || (s = B.bstart.ensure(4 * (maxBlocks + 1))) != DL_OK ||
-        (s = B.masks.ensure(8 * maxBlocks)) != DL_OK)
-        return fail(s);
-    const uint32_t headTiles = (uint32_t)std::max<unsigned long long>(1, (npairs + kVR - 1) / kVR);
-    cudaMemsetAsync(B.status.p, 0, 8ull * headTiles, st);
-    HeadsArgs ha;
-    ha.keys = keysF; ha.npairs = (const unsigned long long*)(scr + 14); ha.bkey = B.bkey.as<uint32_t>();
-    ha.bstart = B.bstart.as<uint32_t>(); ha.nblocks = scr + VS_NBLK; ha.status = B.status.as<unsigned long long>();
-    ha.counter = scr + VS_HEADS; ha.err = scr + VS_ERR;
-    vox_heads_k<<<headTiles, kVT, 0, st>>>(ha);
 
-    EvalArgs va;
-    va.p = p; va.rec = B.rec.as<VoxRec>(); va.vals = valsF; va.bkey = B.bkey.as<uint32_t>();
-    va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
-    va.counter = scr + VS_EVAL; va.evals = nullptr;
-    vox_eval_k<<<dev->sm_count * 24, 64, 0, st>>>(va);
+        // ---- stable sort by block key
+        const uint32_t sortTiles = (uint32_t)std::max<unsigned long long>(1, (npairs + dlsort::kTile - 1) / dlsort::kTile);
+        if ((s = B.keys1.ensure(4 * std::max<unsigned long long>(npairs, 1))) != DL_OK ||
+            (s = B.vals1.ensure(4 * std::max<unsigned long long>(npairs, 1))) != DL_OK ||
+            (s = B.status.ensure(std::max<uint64_t>(4ull * 256 * sortTiles, 8ull * ((npairs + kVR - 1) / kVR + 1)))) != DL_OK ||
+            (s = B.hist.ensure(4ull * 4 * 256)) != DL_OK || (s = B.segs.ensure(64)) != DL_OK)
+            return fail(s);
+        uint32_t* keysF = B.keys0.as<uint32_t>();
+        uint32_t* valsF = B.vals0.as<uint32_t>();
+        if (npairs > 0) {
+            uint64_t* segStart = B.segs.as<uint64_t>();
+            uint32_t* segLen = (uint32_t*)(segStart + 1);
+            uint32_t* segTileBase = segLen + 1;
+            cudaMemsetAsync(segStart, 0, 8, st);
+            const uint32_t len32 = (uint32_t)npairs;
+            cudaMemcpyAsync(segLen, &len32, 4, cudaMemcpyHostToDevice, st);
+            dlsort::Segs sg;
+            sg.start = segStart; sg.len = segLen; sg.tile_base = segTileBase; sg.total_tiles = scr + VS_TILES; sg.num = 1;
+            dlsort::prepare_k<<<1, 32, 0, st>>>(sg);
+            cudaMemsetAsync(B.hist.p, 0, 4ull * 4 * 256, st);
+            dlsort::hist_k<8><<<std::min<uint32_t>(sortTiles, 4096), dlsort::kThreads, 0, st>>>(keysF, sg, passes, 0, B.hist.as<uint32_t>());
+            dlsort::scan_hist_k<8><<<passes, 256, 0, st>>>(B.hist.as<uint32_t>(), passes);
+            uint32_t *kin = keysF, *kout = B.keys1.as<uint32_t>(), *vin = valsF, *vout = B.vals1.as<uint32_t>();
+            for (int ps = 0; ps < passes; ps++) {
+                cudaMemsetAsync(B.status.p, 0, 4ull * 256 * sortTiles, st);
+                dlsort::Pass sp;
+                sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout; sp.segs = sg;
+                sp.glob_off = B.hist.as<uint32_t>(); sp.status = B.status.as<uint32_t>(); sp.counter = scr + VS_SORT + ps;
+                sp.err = scr + VS_ERR; sp.shift = 8 * ps; sp.pass = ps; sp.passes = passes;
+                dlsort::pass_k<8><<<sortTiles, dlsort::kThreads, 0, st>>>(sp);
+                std::swap(kin, kout);
+                std::swap(vin, vout);
+            }
+            keysF = kin;
+            valsF = vin;
+        }
+        // ---- blocks, evaluation, compaction
+        const uint64_t maxBlocks = std::max<unsigned long long>(npairs, 1);
+        if ((s = B.bkey.ensure(4 * maxBlocks)) != DL_OK || (s = B.bstart.ensure(4 * (maxBlocks + 1))) != DL_OK ||
+            (s = B.masks.ensure(8 * maxBlocks)) != DL_OK)
+            return fail(s);
+        const uint32_t headTiles = (uint32_t)std::max<unsigned long long>(1, (npairs + kVR - 1) / kVR);
+        cudaMemsetAsync(B.status.p, 0, 8ull * headTiles, st);
+        HeadsArgs ha;
+        ha.keys = keysF; ha.npairs = (const unsigned long long*)(scr + 14); ha.bkey = B.bkey.as<uint32_t>();
+        ha.bstart = B.bstart.as<uint32_t>(); ha.nblocks = scr + VS_NBLK; ha.status = B.status.as<unsigned long long>();
+        ha.counter = scr + VS_HEADS; ha.err = scr + VS_ERR;
+        vox_heads_k<<<headTiles, kVT, 0, st>>>(ha);
 
-    uint32_t hn[2] = {0, 0};
-    if (cudaMemcpyAsync(hn, scr + VS_NBLK, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-        dl_set_error(std::string("voxelize eval: ") + cudaGetErrorString(cudaGetLastError()));
-        return fail(DL_E_CUDA);
-    }
-    const uint32_t nblk = hn[0];
-    if ((s = B.oidx.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK ||
-        (s = B.olo.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK ||
-        (s = B.ohi.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK)
-        return fail(s);
-    const uint32_t compTiles = std::max<uint32_t>(1, (nblk + kVR - 1) / kVR);
-    cudaMemsetAsync(B.status.p, 0, 8ull * compTiles, st);
-    CompactArgs ca;
-    ca.p = p; ca.bkey = B.bkey.as<uint32_t>(); ca.masks = B.masks.as<uint2>(); ca.nblocks = scr + VS_NBLK;
-    ca.out_idx = B.oidx.as<uint32_t>(); ca.out_lo = B.olo.as<uint32_t>(); ca.out_hi = B.ohi.as<uint32_t>();
-    ca.nout = scr + VS_NOUT; ca.status = B.status.as<unsigned long long>(); ca.counter = scr + VS_COMPACT;
-    ca.err = scr + VS_ERR;
-    vox_compact_k<<<compTiles, kVT, 0, st>>>(ca);
-    uint32_t h2[16];
-    if (cudaMemcpyAsync(h2, scr, 64, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
-        dl_set_error(std::string("voxelize compact: ") + cudaGetErrorString(cudaGetLastError()));
-        return fail(DL_E_CUDA);
-    }
-    if (h2[VS_ERR] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return fail(DL_E_TIMEOUT); }
-    const uint32_t nout = h2[VS_NOUT];
-    R->idx.resize(nout); R->lo.resize(nout); R->hi.resize(nout);
-    if (nout) {
-        if (cudaMemcpy(R->idx.data(), B.oidx.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(R->lo.data(), B.olo.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(R->hi.data(), B.ohi.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess) {
-            dl_set_error("voxelize: result copy failed");
+        EvalArgs va;
+        va.p = p; va.rec = B.rec.as<VoxRec>(); va.vals = valsF; va.bkey = B.bkey.as<uint32_t>();
+        va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
+        va.counter = scr + VS_EVAL; va.evals = nullptr;
+        vox_eval_k<<<dev->sm_count * 24, 64, 0, st>>>(va);
+
+        uint32_t hn[2] = {0, 0};
+        if (cudaMemcpyAsync(hn, scr + VS_NBLK, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            dl_set_error(std::string("voxelize eval: ") + cudaGetErrorString(cudaGetLastError()));
             return fail(DL_E_CUDA);
+        }
+        const uint32_t nblk = hn[0];
+        if ((s = B.oidx.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK ||
+            (s = B.olo.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK ||
+            (s = B.ohi.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK)
+            return fail(s);
+        const uint32_t compTiles = std::max<uint32_t>(1, (nblk + kVR - 1) / kVR);
+        cudaMemsetAsync(B.status.p, 0, 8ull * compTiles, st);
+        CompactArgs ca;
+        ca.p = p; ca.bkey = B.bkey.as<uint32_t>(); ca.masks = B.masks.as<uint2>(); ca.nblocks = scr + VS_NBLK;
+        ca.out_idx = B.oidx.as<uint32_t>(); ca.out_lo = B.olo.as<uint32_t>(); ca.out_hi = B.ohi.as<uint32_t>();
+        ca.nout = scr + VS_NOUT; ca.status = B.status.as<unsigned long long>(); ca.counter = scr + VS_COMPACT;
+        ca.err = scr + VS_ERR;
+        vox_compact_k<<<compTiles, kVT, 0, st>>>(ca);
+        uint32_t h2[16];
+        if (cudaMemcpyAsync(h2, scr, 64, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+            dl_set_error(std::string("voxelize compact: ") + cudaGetErrorString(cudaGetLastError()));
+            return fail(DL_E_CUDA);
+        }
+        if (h2[VS_ERR] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return fail(DL_E_TIMEOUT); }
+        const uint32_t nout = h2[VS_NOUT];
+        const size_t o0 = R->idx.size();
+        R->idx.resize(o0 + nout); R->lo.resize(o0 + nout); R->hi.resize(o0 + nout);
+        if (nout) {
+            if (cudaMemcpy(R->idx.data() + o0, B.oidx.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                cudaMemcpy(R->lo.data() + o0, B.olo.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                cudaMemcpy(R->hi.data() + o0, B.ohi.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                dl_set_error("voxelize: result copy failed");
+                return fail(DL_E_CUDA);
+            }
         }
     }
     *out = R;

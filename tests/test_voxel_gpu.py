@@ -52,6 +52,20 @@ def test_clustered_100k_exact(device):
     assert_same(g, o)
 
 
+def test_slabbed_grid_matches_one_pass(device, monkeypatch):
+    # the grid is processed in z rows of 16^3-block batches bounded by a pair
+    # capacity; a tiny capacity forces many slabs and must not change anything
+    d = synth.voxel_1m(40_000)
+    g1 = dl.voxelize(device, d, {"voxelResolution": 0.04, "opacityCutoff": 0.1})
+    monkeypatch.setenv("DL_VOX_SLAB_PAIRS", "20000")
+    g2 = dl.voxelize(device, d, {"voxelResolution": 0.04, "opacityCutoff": 0.1})
+    assert np.array_equal(g1.buffer.blockIdx, g2.buffer.blockIdx)
+    assert np.array_equal(g1.buffer.maskLo, g2.buffer.maskLo) and np.array_equal(g1.buffer.maskHi, g2.buffer.maskHi)
+    assert g1.buffer.count > 100
+    o = O.voxelize(d, 0.04, 0.1)
+    assert np.array_equal(g2.buffer.blockIdx, o["block_idx"]) and np.array_equal(g2.buffer.maskLo, o["mask_lo"])
+
+
 def test_user_bounds_and_partial_batches(device):
     d = synth.voxel_1m(30_000)
     g, o = run_both(device, d, res=0.07, cut=0.3, bounds=((-3.1, -2.0, -4.4), (2.3, 5.0, 1.7)))
