@@ -99,6 +99,8 @@ struct VoxParams {
     const double* qmx[3];
     const float* bmin32[3];         // per-axis f32 batch min (BatchInfo.blockMin*)
     int64_t zlo, zhi;               // block z range of the slab being processed
+    int64_t ylo, yhi;               // block y range of the slab being processed
+    int64_t xlo, xhi;               // block x range of the slab being processed
 };
 
 __global__ void vox_prep_k(VoxParams p, float* __restrict__ ext, VoxRec* __restrict__ rec, double* __restrict__ part) {
@@ -164,39 +166,73 @@ __global__ void vox_bounds_k(const double* part, uint32_t nparts, double* out) {
     out[k] = v;
 }
 
-// Block range [lo, hi] along one axis for Gaussian centre c, extent e (hi < lo: none).
-__device__ void axis_range(const VoxParams& p, int a, float c, float e, float eh, int64_t& lo, int64_t& hi) {
-    lo = 0; hi = -1;
-    const int64_t NB = p.NB[a], NBB = p.NBB[a];
-    // batches passing the f64 box test (bvh.ts:310-316)
+// Batches along axis a whose f64 box the Gaussian's f64 AABB overlaps
+// (bvh.ts:310-316); bhi < blo: none.
+__device__ void batch_range(const VoxParams& p, int a, float c, float e, int64_t& blo, int64_t& bhi) {
+    blo = INT64_MAX; bhi = -1;
+    const int64_t NBB = p.NBB[a];
     const double gmn = (double)c - (double)e, gmx = (double)c + (double)e;
     const double span = 16.0 * p.blockSize;
     const double f0 = floor((gmn - p.boundsMin[a]) / span) - 1.0, f1 = floor((gmx - p.boundsMin[a]) / span) + 1.0;
     if (!(f1 >= 0.0) || !(f0 <= (double)(NBB - 1))) return;
     const int64_t b0 = f0 < 0.0 ? 0 : (int64_t)f0, b1 = f1 > (double)(NBB - 1) ? NBB - 1 : (int64_t)f1;
-    int64_t blo = INT64_MAX, bhi = -1;
     for (int64_t b = b0; b <= b1; b++) {
         if (gmx < p.qmn[a][b] || gmn > p.qmx[a][b]) continue;
         blo = min(blo, b); bhi = max(bhi, b);
     }
+}
+
+// Block range [lo, hi] along one axis for Gaussian centre c, extent e (hi < lo: none).
+__device__ void axis_range(const VoxParams& p, int a, float c, float e, float eh, int64_t& lo, int64_t& hi) {
+    lo = 0; hi = -1;
+    const int64_t NB = p.NB[a];
+    int64_t blo, bhi;
+    batch_range(p, a, c, e, blo, bhi);
     if (bhi < 0) return;
-    // blocks whose voxel centres (f32, from the batch min) can be within eh of c
-    const double tol = 0.01 * (double)p.res + 1e-5 * (fabs((double)c) + fabs(p.boundsMin[a]) + 1.0);
+    // blocks with a voxel centre coordinate (the f32 expression of vox_eval_k)
+    // within eh of c on this axis: the shader's per-axis test, evaluated exactly
     const double step = 4.0 * (double)p.res;
-    const double u0 = ((double)c - (double)eh - tol - p.boundsMin[a] - 3.5 * (double)p.res) / step;
-    const double u1 = ((double)c + (double)eh + tol - p.boundsMin[a] - 0.5 * (double)p.res) / step;
+    const double u0 = ((double)c - (double)eh - p.boundsMin[a]) / step - 1.0;
+    const double u1 = ((double)c + (double)eh - p.boundsMin[a]) / step + 1.0;
     if (!(u1 >= 0.0) || !(u0 <= (double)(NB - 1))) return;
-    int64_t v0 = u0 < 0.0 ? 0 : (int64_t)ceil(u0 - 1e-9);
-    int64_t v1 = u1 > (double)(NB - 1) ? NB - 1 : (int64_t)floor(u1 + 1e-9);
-    v0 = max(v0 - 1, (int64_t)0);            // one extra block each side: generous superset
-    v1 = min(v1 + 1, NB - 1);
+    const int64_t c0 = u0 < 0.0 ? 0 : (int64_t)u0;
+    const int64_t c1 = u1 > (double)(NB - 1) ? NB - 1 : (int64_t)u1;
+    int64_t v0 = INT64_MAX, v1 = -1;
+    for (int64_t l = c0; l <= c1; l++) {
+        const float bmin = p.bmin32[a][l >> 4];
+        const float boff = ((float)(l & 15) * 4.0f) * p.res;
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float vc = (bmin + boff) + (((float)k + 0.5f) * p.res);
+            if (!(fabsf(vc - c) > eh)) any = true;
+        }
+        if (any) { v0 = min(v0, l); v1 = max(v1, l); }
+    }
+    if (v1 < 0) return;
     lo = max(v0, blo * 16);
     hi = min(v1, min(bhi * 16 + 15, NB - 1));
     if (a == 2) { lo = max(lo, p.zlo); hi = min(hi, p.zhi); }
+    if (a == 1) { lo = max(lo, p.ylo); hi = min(hi, p.yhi); }
+    if (a == 0) { lo = max(lo, p.xlo); hi = min(hi, p.xhi); }
 }
 
-// Gaussian-block pairs per 16-block z row of batches (sizes the slabs).
-__global__ void vox_zcount_k(VoxParams p, const float* __restrict__ ext, unsigned long long* __restrict__ zcount) {
+// Batches with a non-empty batch list (the reference dispatches exactly these).
+__global__ void vox_batchused_k(VoxParams p, const float* __restrict__ ext, uint32_t* __restrict__ used) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= p.n) return;
+    int64_t lo[3], hi[3];
+    for (int k = 0; k < 3; k++) {
+        batch_range(p, k, p.pos[3ull * g + k], ext[3ull * g + k], lo[k], hi[k]);
+        if (hi[k] < 0) return;
+    }
+    for (int64_t bz = lo[2]; bz <= hi[2]; bz++)
+        for (int64_t by = lo[1]; by <= hi[1]; by++)
+            for (int64_t bx = lo[0]; bx <= hi[0]; bx++) used[(bz * p.NBB[1] + by) * p.NBB[0] + bx] = 1u;
+}
+
+// Gaussian-block pairs per 16^3-block batch (sizes the slabs).
+__global__ void vox_batchcount_k(VoxParams p, const float* __restrict__ ext, unsigned long long* __restrict__ cnt) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= p.n) return;
     int64_t lo[3], hi[3];
@@ -205,10 +241,15 @@ __global__ void vox_zcount_k(VoxParams p, const float* __restrict__ ext, unsigne
         axis_range(p, k, p.pos[3ull * g + k], e, e + p.half, lo[k], hi[k]);
     }
     if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2]) return;
-    const unsigned long long xy = (unsigned long long)(hi[0] - lo[0] + 1) * (unsigned long long)(hi[1] - lo[1] + 1);
     for (int64_t bz = lo[2] >> 4; bz <= (hi[2] >> 4); bz++) {
-        const int64_t z0 = max(lo[2], bz * 16), z1 = min(hi[2], bz * 16 + 15);
-        atomicAdd(&zcount[bz], xy * (unsigned long long)(z1 - z0 + 1));
+        const int64_t nz = min(hi[2], bz * 16 + 15) - max(lo[2], bz * 16) + 1;
+        for (int64_t by = lo[1] >> 4; by <= (hi[1] >> 4); by++) {
+            const int64_t ny = min(hi[1], by * 16 + 15) - max(lo[1], by * 16) + 1;
+            for (int64_t bx = lo[0] >> 4; bx <= (hi[0] >> 4); bx++) {
+                const int64_t nx = min(hi[0], bx * 16 + 15) - max(lo[0], bx * 16) + 1;
+                atomicAdd(&cnt[(bz * p.NBB[1] + by) * p.NBB[0] + bx], (unsigned long long)(nx * ny * nz));
+            }
+        }
     }
 }
 
@@ -672,49 +713,120 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     // Blocks are appended in batch order (z rows outermost), so processing the
     // rows in order and concatenating reproduces the reference's block order.
     // (DL_VOX_SLAB_PAIRS lowers the capacity, to exercise the slab loop on small inputs.)
-    unsigned long long kSlabCap = 1ull << 29;
+    unsigned long long kSlabCap = (1ull << 30) - 1;
     if (const char* env = std::getenv("DL_VOX_SLAB_PAIRS")) {
         const unsigned long long e = std::strtoull(env, nullptr, 10);
         if (e > 0 && e < kSlabCap) kSlabCap = e;
     }
-    std::vector<unsigned long long> zc((size_t)p.NBB[2], 0ull);
+    // ---- cutoff <= 0: 1 - exp(-sigma) >= cutoff holds for every voxel, so every
+    // voxel of every batch with a non-empty batch list is solid
+    if (!(p.cutoff > 0.0f) && p.cutoff <= 0.0f) {
+        DevBuf usedD;
+        if ((s = usedD.ensure(4ull * numBatches)) != DL_OK) return fail(s);
+        cudaMemsetAsync(usedD.p, 0, 4ull * numBatches, st);
+        vox_batchused_k<<<prepGrid, 256, 0, st>>>(p, B.ext.as<float>(), usedD.as<uint32_t>());
+        std::vector<uint32_t> used(numBatches, 0);
+        if (cudaMemcpyAsync(used.data(), usedD.p, 4ull * numBatches, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            dl_set_error(std::string("voxelize: ") + cudaGetErrorString(cudaGetLastError()));
+            return fail(DL_E_CUDA);
+        }
+        for (uint64_t b = 0; b < numBatches; b++) {
+            if (!used[b]) continue;
+            const int64_t bxI = b % p.NBB[0], byI = (b / p.NBB[0]) % p.NBB[1], bzI = b / (p.NBB[0] * p.NBB[1]);
+            const int64_t cx = std::min<int64_t>(16, p.NB[0] - bxI * 16), cy = std::min<int64_t>(16, p.NB[1] - byI * 16);
+            const int64_t cz = std::min<int64_t>(16, p.NB[2] - bzI * 16);
+            for (int64_t bi = 0; bi < cx * cy * cz; bi++) {
+                const int64_t ax = bxI * 16 + bi % cx, ay = byI * 16 + (bi / cx) % cy, az = bzI * 16 + bi / (cx * cy);
+                R->idx.push_back((uint32_t)(ax + ay * p.NB[0] + az * p.NB[0] * p.NB[1]));
+                R->lo.push_back(0xffffffffu);
+                R->hi.push_back(0xffffffffu);
+            }
+        }
+        *out = R;
+        return DL_OK;
+    }
+    const int64_t NBX_ = p.NBB[0], NBY_ = p.NBB[1], NBZ_ = p.NBB[2];
+    std::vector<unsigned long long> bc((size_t)(NBX_ * NBY_ * NBZ_), 0ull);     // pairs per batch
     {
-        DevBuf zcount;
-        if ((s = zcount.ensure(8ull * p.NBB[2])) != DL_OK) return fail(s);
-        cudaMemsetAsync(zcount.p, 0, 8ull * p.NBB[2], st);
-        p.zlo = 0;
-        p.zhi = p.NB[2] - 1;
-        vox_zcount_k<<<prepGrid, 256, 0, st>>>(p, B.ext.as<float>(), zcount.as<unsigned long long>());
-        if (cudaMemcpyAsync(zc.data(), zcount.p, 8ull * p.NBB[2], cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        DevBuf cnt;
+        if ((s = cnt.ensure(8ull * bc.size())) != DL_OK) return fail(s);
+        cudaMemsetAsync(cnt.p, 0, 8ull * bc.size(), st);
+        p.zlo = 0; p.zhi = p.NB[2] - 1;
+        p.ylo = 0; p.yhi = p.NB[1] - 1;
+        p.xlo = 0; p.xhi = p.NB[0] - 1;
+        vox_batchcount_k<<<prepGrid, 256, 0, st>>>(p, B.ext.as<float>(), cnt.as<unsigned long long>());
+        if (cudaMemcpyAsync(bc.data(), cnt.p, 8ull * bc.size(), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
             dl_set_error(std::string("voxelize count: ") + cudaGetErrorString(cudaGetLastError()));
             return fail(DL_E_CUDA);
         }
     }
-    std::vector<std::pair<int64_t, int64_t>> slabs;     // [bz0, bz1) in batch rows
+    // A slab is a box of batches contiguous in batch order: whole z rows, or
+    // whole y rows of one z row, or a range of batches of one (z, y) row.
+    struct Slab { int64_t z0, z1, y0, y1, x0, x1; unsigned long long pairs; };
+    std::vector<Slab> slabs;
     {
-        int64_t b0 = 0;
-        unsigned long long acc = 0;
-        for (int64_t bz = 0; bz < p.NBB[2]; bz++) {
-            if (zc[bz] > kSlabCap && kSlabCap == (1ull << 29)) {
-                dl_set_error("one 16-block z row needs more than 2^29 Gaussian-block pairs");
-                return fail(DL_E_CAPACITY);
+        auto rowSum = [&](int64_t z, int64_t y) {
+            unsigned long long a = 0;
+            for (int64_t x = 0; x < NBX_; x++) a += bc[(z * NBY_ + y) * NBX_ + x];
+            return a;
+        };
+        Slab cur{0, 0, 0, NBY_, 0, NBX_, 0};                     // whole z rows being merged
+        for (int64_t z = 0; z < NBZ_; z++) {
+            unsigned long long zs = 0;
+            for (int64_t y = 0; y < NBY_; y++) zs += rowSum(z, y);
+            if (zs <= kSlabCap) {
+                if (cur.z1 > cur.z0 && cur.pairs + zs > kSlabCap) { slabs.push_back(cur); cur = {z, z, 0, NBY_, 0, NBX_, 0}; }
+                if (cur.z1 == cur.z0) cur.z0 = z;
+                cur.z1 = z + 1;
+                cur.pairs += zs;
+                continue;
             }
-            if (acc + zc[bz] > kSlabCap && bz > b0) { slabs.push_back({b0, bz}); b0 = bz; acc = 0; }
-            acc += zc[bz];
+            if (cur.z1 > cur.z0) slabs.push_back(cur);
+            Slab yr{z, z + 1, 0, 0, 0, NBX_, 0};                  // whole y rows of this z row
+            for (int64_t y = 0; y < NBY_; y++) {
+                const unsigned long long ys = rowSum(z, y);
+                if (ys <= kSlabCap) {
+                    if (yr.y1 > yr.y0 && yr.pairs + ys > kSlabCap) { slabs.push_back(yr); yr = {z, z + 1, y, y, 0, NBX_, 0}; }
+                    if (yr.y1 == yr.y0) yr.y0 = y;
+                    yr.y1 = y + 1;
+                    yr.pairs += ys;
+                    continue;
+                }
+                if (yr.y1 > yr.y0) slabs.push_back(yr);
+                Slab xr{z, z + 1, y, y + 1, 0, 0, 0};             // batches of this (z, y) row
+                for (int64_t x = 0; x < NBX_; x++) {
+                    const unsigned long long c = bc[(z * NBY_ + y) * NBX_ + x];
+                    if (c > (1ull << 30) - 1) {
+                        dl_set_error("one 16^3-block batch needs 2^30 or more Gaussian-block pairs");
+                        return fail(DL_E_CAPACITY);
+                    }
+                    if (xr.x1 > xr.x0 && xr.pairs + c > kSlabCap) { slabs.push_back(xr); xr = {z, z + 1, y, y + 1, x, x, 0}; }
+                    xr.x1 = x + 1;
+                    xr.pairs += c;
+                }
+                slabs.push_back(xr);
+                yr = {z, z + 1, y + 1, y + 1, 0, NBX_, 0};
+            }
+            if (yr.y1 > yr.y0) slabs.push_back(yr);
+            cur = {z + 1, z + 1, 0, NBY_, 0, NBX_, 0};
         }
-        slabs.push_back({b0, p.NBB[2]});
+        if (cur.z1 > cur.z0) slabs.push_back(cur);
     }
     const uint32_t emitTiles = (uint32_t)((n + kVR - 1) / kVR);
     int keyBits = 12;
     while ((1ull << (keyBits - 12)) < numBatches) keyBits++;
     const int passes = (keyBits + 7) / 8;
-    for (const auto& slab : slabs) {
-        unsigned long long cap = 0;
-        for (int64_t bz = slab.first; bz < slab.second; bz++) cap += zc[bz];
+    for (const Slab& slab : slabs) {
+        const unsigned long long cap = slab.pairs;
         if (cap == 0) continue;
-        p.zlo = slab.first * 16;
-        p.zhi = std::min<int64_t>(slab.second * 16, p.NB[2]) - 1;
+        p.zlo = slab.z0 * 16;
+        p.zhi = std::min<int64_t>(slab.z1 * 16, p.NB[2]) - 1;
+        p.ylo = slab.y0 * 16;
+        p.yhi = std::min<int64_t>(slab.y1 * 16, p.NB[1]) - 1;
+        p.xlo = slab.x0 * 16;
+        p.xhi = std::min<int64_t>(slab.x1 * 16, p.NB[0]) - 1;
         // ---- binning (exactly `cap` pairs)
         if ((s = B.keys0.ensure(4 * cap)) != DL_OK || (s = B.vals0.ensure(4 * cap)) != DL_OK ||
             (s = B.status.ensure(8ull * std::max<uint64_t>(emitTiles, 1))) != DL_OK)
@@ -738,30 +850,6 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             if (h[VS_OVF] & 4u) { dl_set_error("a Gaussian overlaps more than 2^31 blocks"); return fail(DL_E_CAPACITY); }
             if (h[VS_OVF] & DL_DEVERR_OVERFLOW) { dl_set_error("voxelize: binning disagrees with its count"); return fail(DL_E_CAPACITY); }
             std::memcpy(&npairs, &h[14], 8);
-        }
-
-        // ---- cutoff <= 0: every voxel of every batch with a non-empty list is solid
-        if (!(p.cutoff > 0.0f) && p.cutoff <= 0.0f) {
-            std::vector<uint32_t> hk(npairs);
-            if (npairs && cudaMemcpy(hk.data(), B.keys0.p, 4 * npairs, cudaMemcpyDeviceToHost) != cudaSuccess) {
-                dl_set_error("voxelize: copy failed");
-                return fail(DL_E_CUDA);
-            }
-            std::vector<char> used(numBatches, 0);
-            for (uint32_t k : hk) used[k >> 12] = 1;
-            for (uint64_t b = 0; b < numBatches; b++) {
-                if (!used[b]) continue;
-                const int64_t bxI = b % p.NBB[0], byI = (b / p.NBB[0]) % p.NBB[1], bzI = b / (p.NBB[0] * p.NBB[1]);
-                const int64_t cx = std::min<int64_t>(16, p.NB[0] - bxI * 16), cy = std::min<int64_t>(16, p.NB[1] - byI * 16);
-                const int64_t cz = std::min<int64_t>(16, p.NB[2] - bzI * 16);
-                for (int64_t bi = 0; bi < cx * cy * cz; bi++) {
-                    const int64_t ax = bxI * 16 + bi % cx, ay = byI * 16 + (bi / cx) % cy, az = bzI * 16 + bi / (cx * cy);
-                    R->idx.push_back((uint32_t)(ax + ay * p.NB[0] + az * p.NB[0] * p.NB[1]));
-                    R->lo.push_back(0xffffffffu);
-                    R->hi.push_back(0xffffffffu);
-                }
-            }
-            continue;
         }
 
         // ---- stable sort by block key
