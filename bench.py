@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--workload", default="ring64", choices=["ring64", "voxel1m", "zipf10m"],
+                   help="ring64: the headline render batch; voxel1m / zipf10m: voxelize lines")
     return p.parse_args()
 
 
@@ -180,6 +182,63 @@ def run_reference(args, rank, world):
                                        "WebGPU unavailable on this box), one view per step"},
             "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+VOXEL = {"voxel1m": ("1M Gaussians, 64 clusters in [-5,5]^3, voxelResolution 0.05, opacityCutoff 0.1", 0.05),
+         "zipf10m": ("10M Gaussians, 1024 Zipf(1.2) clusters in [-20,20]^3, voxelResolution 0.02, opacityCutoff 0.1",
+                     0.02)}
+
+
+def run_voxel(args, rank, world, local_rank):
+    """Mvox/s of voxelize (voxels of the block grid / time), through the public
+    call: host SplatData in, host block list out (so value and e2e coincide)."""
+    import numpy as np
+    import torch
+
+    import droplet_b200 as dl
+    from droplet_b200 import synth
+    torch.cuda.set_device(local_rank)
+    data = synth.voxel_1m() if args.workload == "voxel1m" else synth.zipf_10m()
+    desc, res = VOXEL[args.workload]
+    opts = {"voxelResolution": res, "opacityCutoff": 0.1}
+    dev = dl.createDevice({"ordinal": local_rank})
+    out = None
+    for _ in range(args.warmup):
+        out = dl.voxelize(dev, data, opts)
+    vox = out.numBlocksX * out.numBlocksY * out.numBlocksZ * 64
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            dl.voxelize(dev, data, opts)        # synchronous: returns with the block list on the host
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    value = world * vox / (ms / 1e3) / 1e6
+    line = {"metric": "Mvox/s (voxels of the block grid per second), voxelize", "value": value, "unit": "Mvox/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": f"{args.workload}: {desc}", "grid_blocks": [out.numBlocksX, out.numBlocksY,
+                                                                               out.numBlocksZ],
+                       "blocks_out": out.buffer.count, "solid_voxels": out.buffer.popcount()},
+            "clocks": clk.summary(),
+            "e2e": {"value": value, "unit": "Mvox/s", "h2d_bytes_per_step": int(data.count * 44),
+                    "d2h_bytes_per_step": int(out.buffer.count * 12)}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        sub = synth.voxel_1m(100_000) if args.workload == "voxel1m" else synth.cluster_scene(
+            200_000, seed=11, clusters=1024, extent=20.0, log_lo=0.005, log_hi=0.2, bands=1, zipf_s=1.2)
+        t = time.perf_counter()
+        o = O.voxelize(sub, res, 0.1)
+        dt = time.perf_counter() - t
+        v = float(np.prod(o["dims"])) * 64 / dt / 1e6
+        line["cpu_baseline"] = {"value": v, "unit": "Mvox/s", "cores": int(os.environ.get("OMP_NUM_THREADS",
+                                                                                               os.cpu_count() or 1)),
+                                "kind": "port", "sample": f"oracle voxelizes {sub.count} Gaussians of the same "
+                                                          f"distribution in {dt:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_ours(args, rank, world, local_rank):
@@ -327,6 +386,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload != "ring64":
+        run_voxel(args, rank, world, local_rank)
         return
     if world > 1:
         import datetime
