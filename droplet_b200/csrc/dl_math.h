@@ -21,8 +21,8 @@
 //
 // Reference semantics this stands in for: WGSL `exp`, `atan2`, `asin` in
 // src/render/shaders/project.ts:55,77,258-259 and
-// src/voxel/shaders/voxelize.ts:384-389,440, and JS `Math.exp` in
-// src/spatial/aabb.ts:119-121.  WGSL only bounds their error (exp: 3+2|x| ulp),
+// src/voxel/shaders/voxelize.ts:78-83,440, and JS `Math.exp` in
+// src/spatial/aabb.ts:33-35.  WGSL only bounds their error (exp: 3+2|x| ulp),
 // so any implementation within those bounds is a faithful restatement; the
 // tests check this one against glibc to <= 2 ulp (f32) and <= 1 ulp (f64).
 //

@@ -6,10 +6,10 @@
 //   radix-sort.ts:65-117 CPU depth sort          -> dlsort passes (dl_sort.cuh)
 //   prefix-sum.ts + pipeline.ts:277-304 scan     -> emit_k (decoupled look-back)
 //   (pair-sort digit offsets)                    -> pair_digits_k
-//   emit-pairs.ts:164-193 emit                    -> emit_k (load-balanced emission)
+//   emit-pairs.ts:28-57 emit                    -> emit_k (load-balanced emission)
 //   pipeline.ts:544-578 stable pair sort          -> dlsort passes on tile ids
 //   find-boundaries.ts:17-99 tile offsets         -> boundaries_k (direct writes, no atomics)
-//   rasterize.ts:135-181 + finalize.ts:211-224    -> rasterize_k (fused)
+//   rasterize.ts:36-82 + finalize.ts:30-43    -> rasterize_k (fused)
 //
 // All f32 arithmetic that feeds an integer decision or an output byte is
 // written in the shaders' evaluation order and compiled with --fmad=false,
@@ -606,10 +606,10 @@ __global__ void sched_scatter_k(const uint32_t* __restrict__ bucket, uint32_t to
 // splat's box widened by one pixel reaches a pixel centre of the sub-tile (no
 // pixel whose per-pixel box test could pass is dropped), and the kept splats,
 // in slice order, are staged in warp-private shared memory and composited by
-// all 32 lanes with rasterize.ts:161-178 verbatim.  Pairs whose value has
+// all 32 lanes with rasterize.ts:62-79 verbatim.  Pairs whose value has
 // kPhantomBit (a splat box wholly left of / above the image) are skipped
 // without reading their record: no pixel's box test can pass for them.  No CTA barrier: a warp
-// leaves as soon as its own pixels saturate.  finalize.ts:211-224 is fused as
+// leaves as soon as its own pixels saturate.  finalize.ts:30-43 is fused as
 // the epilogue.
 struct RasterArgs {
     const DlView* views;
@@ -791,7 +791,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
         }
     }
     if (inImage) {
-        // finalize.ts:211-224
+        // finalize.ts:30-43
         const float rr = fminf(fmaxf(c0 + T * u.bg[0], 0.0f), 1.0f);
         const float gg = fminf(fmaxf(c1 + T * u.bg[1], 0.0f), 1.0f);
         const float bb = fminf(fmaxf(c2 + T * u.bg[2], 0.0f), 1.0f);

@@ -6,13 +6,13 @@
 // decode of the masks into a BlockMaskBuffer.
 //
 // Here:
-//   vox_prep_k     per-Gaussian f64 extents (aabb.ts:108-148, same op order),
+//   vox_prep_k     per-Gaussian f64 extents (aabb.ts:22-62, same op order),
 //                  the 64-byte evaluation record, and partial bounds.
 //   vox_bounds_k   final min/max reduction (voxelize.ts:278-306 inputs).
 //   vox_emit_k     Gaussian -> block binning: for every block a Gaussian can
 //                  touch, one (block key, Gaussian) pair.  A Gaussian is binned
 //                  to a block only if it is in the block's 16^3 batch list under
-//                  the reference's f64 box test (bvh.ts:301-316), and only if
+//                  the reference's f64 box test (bvh.ts:153-168), and only if
 //                  its box can reach one of the block's voxel centres (a
 //                  superset of the shader's per-voxel test, which still runs).
 //                  The key orders blocks exactly as the reference appends them
@@ -22,7 +22,7 @@
 //   vox_eval_k     per block, 64 threads = 64 voxels; 64-Gaussian tiles staged
 //                  through shared memory; the density sum, the sigma >= 7 early
 //                  exit and the Beer-Lambert threshold of shaders/voxelize.ts:
-//                  368-453 in the same f32 order; warp ballots build the two
+//                  62-147 in the same f32 order; warp ballots build the two
 //                  32-bit masks directly (thread = linear bit index).
 //   vox_compact_k  drop all-zero masks (BlockMaskBuffer.addBlock skips them).
 // The density of a voxel is summed over its batch list in ascending Gaussian
@@ -107,7 +107,7 @@ __global__ void vox_prep_k(VoxParams p, float* __restrict__ ext, VoxRec* __restr
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     if (g < p.n) {
-        // aabb.ts:114-146 (f64)
+        // aabb.ts:28-60 (f64)
         const double qw = p.rot[4ull * g], qx = p.rot[4ull * g + 1], qy = p.rot[4ull * g + 2], qz = p.rot[4ull * g + 3];
         const float l0 = p.lsc[3ull * g], l1 = p.lsc[3ull * g + 1], l2 = p.lsc[3ull * g + 2];
         const double sx = dl_exp((double)l0), sy = dl_exp((double)l1), sz = dl_exp((double)l2);
@@ -167,7 +167,7 @@ __global__ void vox_bounds_k(const double* part, uint32_t nparts, double* out) {
 }
 
 // Batches along axis a whose f64 box the Gaussian's f64 AABB overlaps
-// (bvh.ts:310-316); bhi < blo: none.
+// (bvh.ts:162-168); bhi < blo: none.
 __device__ void batch_range(const VoxParams& p, int a, float c, float e, int64_t& blo, int64_t& bhi) {
     blo = INT64_MAX; bhi = -1;
     const int64_t NBB = p.NBB[a];
@@ -430,7 +430,7 @@ struct EvalArgs {
 };
 
 __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, const VoxRec& g) {
-    // shaders/voxelize.ts:368-390, same f32 operation order
+    // shaders/voxelize.ts:62-84, same f32 operation order
     const float d0 = vc[0] - g.px, d1 = vc[1] - g.py, d2 = vc[2] - g.pz;
     if (fabsf(d0) > g.ehx || fabsf(d1) > g.ehy || fabsf(d2) > g.ehz) return 0.0f;
     const float cd0 = fminf(fmaxf(g.px, vc[0] - half), vc[0] + half) - g.px;
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(64) vox_eval_k(EvalArgs a) {
     __shared__ uint32_t s_mask[2];
     const int tid = threadIdx.x;
     const uint32_t nb = *a.nblocks;
-    // linear bit index = z*16 + y*4 + x (shaders/voxelize.ts:443)
+    // linear bit index = z*16 + y*4 + x (shaders/voxelize.ts:137)
     const uint32_t lx = tid & 3, ly = (tid >> 2) & 3, lz = tid >> 4;
     const int64_t NX = a.p.NB[0], NY = a.p.NB[1], NBX = a.p.NBB[0], NBY = a.p.NBB[1];
     uint64_t evals = 0;
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(64) vox_eval_k(EvalArgs a) {
         const int64_t bxI = batch % NBX, byI = (batch / NBX) % NBY, bzI = batch / (NBX * NBY);
         const int64_t cx = min((int64_t)16, NX - bxI * 16), cy = min((int64_t)16, NY - byI * 16);
         const uint32_t blockX = bi % cx, blockY = (bi / cx) % cy, blockZ = bi / (cx * cy);
-        // voxel centre exactly as shaders/voxelize.ts:409-412
+        // voxel centre exactly as shaders/voxelize.ts:103-106
         const float res = a.p.res;
         const float bmin[3] = {a.p.bmin32[0][bxI], a.p.bmin32[1][byI], a.p.bmin32[2][bzI]};
         const float boff[3] = {((float)blockX * 4.0f) * res, ((float)blockY * 4.0f) * res, ((float)blockZ * 4.0f) * res};

@@ -2,9 +2,9 @@
  * behind droplet's TypeScript API.
  *
  * The TypeScript surface stays as it is (src/index.ts:16-38); a thin shim
- * calls these entry points through bun:ffi.  Each entry
- * point cites the reference interface it replaces.  Paths are relative to the
- * droplet repository.
+ * calls these entry points through bun:ffi.  Each entry point cites the
+ * reference interface it replaces.  Paths are relative to the droplet
+ * repository.
  *
  * Conventions
  *   - Every function returns an int status: DL_OK (0) or a DL_E_* code; the

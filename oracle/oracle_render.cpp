@@ -373,7 +373,7 @@ uint32_t projectOne(const ProjUniforms& u, const float* in, int M, float* proj) 
     return count;
 }
 
-// emit-pairs.ts:164-193
+// emit-pairs.ts:28-57
 void emitPairs(const float* projected, const uint32_t* offsets, uint32_t n, uint32_t tilesX,
                uint32_t tilesY, uint32_t maxCoverage, uint32_t* pairTiles, uint32_t* pairSplats) {
     for (uint32_t idx = 0; idx < n; idx++) {
@@ -443,7 +443,7 @@ void findBoundaries(const uint32_t* pairTiles, uint32_t numPairs, uint32_t numTi
     }
 }
 
-// rasterize.ts:135-181 — one pixel; accum is (r, g, b, T) resumed across chunks.
+// rasterize.ts:36-82 — one pixel; accum is (r, g, b, T) resumed across chunks.
 // Returns the number of slice entries examined (up to the T-break).
 template <typename T>
 uint32_t rasterPixel(const T* projected, const uint32_t* pairSplats, uint32_t sliceStart,
@@ -483,7 +483,7 @@ uint32_t rasterPixel(const T* projected, const uint32_t* pairSplats, uint32_t sl
     return examined;
 }
 
-// finalize.ts:211-224
+// finalize.ts:30-43
 inline uint32_t finalizePixel(const float* v, const float bg[4]) {
     float rgb[3];
     for (int k = 0; k < 3; k++) rgb[k] = std::min(std::max(v[k] + v[3] * bg[k], 0.0f), 1.0f);

@@ -9,7 +9,7 @@
 //   order 1 (reference): the batch list in the reference's BVH query order
 //            (a statement-by-statement port of bvh.ts).
 // The list MEMBERSHIP is the reference's in both (a Gaussian belongs to a
-// 16^3-block batch iff its f64 AABB overlaps the batch box, bvh.ts:301-316),
+// 16^3-block batch iff its f64 AABB overlaps the batch box, bvh.ts:153-168),
 // so the two orders differ only by floating-point summation order.
 #include "oracle.h"
 
@@ -28,7 +28,7 @@ double jsRound(double x) {
     return (x - f >= 0.5) ? f + 1.0 : f;
 }
 
-// aabb.ts:108-148 — f64 arithmetic on f32 inputs, result stored as f32.
+// aabb.ts:22-62 — f64 arithmetic on f32 inputs, result stored as f32.
 void computeAabbExtents(const orc_splats& d, std::vector<float>& out) {
     const uint64_t n = d.count;
     out.assign(n * 3, 0.0f);
@@ -71,7 +71,7 @@ void computeBlockAlignedBounds(const orc_splats& d, const std::vector<float>& e,
     }
 }
 
-// bvh.ts:181-331 — median-split BVH, statement by statement.
+// bvh.ts:33-183 — median-split BVH, statement by statement.
 struct BVH {
     struct Node { double mn[3], mx[3]; int start, end, left, right; };
     std::vector<Node> nodes;
@@ -172,7 +172,7 @@ inline void crossf(const float a[3], const float b[3], float o[3]) {
     o[2] = a[0] * b[1] - a[1] * b[0];
 }
 
-// shaders/voxelize.ts:368-390
+// shaders/voxelize.ts:62-84
 float evalGaussian(const float vc[3], float half, const Gauss& g) {
     float diff[3];
     for (int a = 0; a < 3; a++) diff[a] = vc[a] - g.pos[a];
@@ -333,7 +333,7 @@ extern "C" void* orc_voxelize_run(const orc_splats* data, double voxelRes, doubl
             uint32_t m[2] = {0, 0}, nm[2] = {0, 0};
             const std::vector<uint32_t>& L = blk[(size_t)fb];
             for (uint32_t vi = 0; vi < 64; vi++) {
-                // mortonToXYZ (shaders/voxelize.ts:360-366)
+                // mortonToXYZ (shaders/voxelize.ts:54-60)
                 const uint32_t lx = (vi & 1u) | ((vi >> 2) & 2u);
                 const uint32_t ly = ((vi >> 1) & 1u) | ((vi >> 3) & 2u);
                 const uint32_t lz = ((vi >> 2) & 1u) | ((vi >> 4) & 2u);

@@ -7,11 +7,11 @@ numeric pins are hand derivations of its formulas for cases with closed forms:
 
   * one isotropic splat at the origin seen head-on (test.ts:45-56,95-103):
     projected conic, radius, opacity and the centre pixel's byte
-    (project.ts:128-217, rasterize.ts:161-178, finalize.ts:211-224);
+    (project.ts:128-217, rasterize.ts:62-79, finalize.ts:30-43);
   * the order-preserving depth key (spatial/radix-sort.ts:20-24) of edge values;
   * one isotropic Gaussian voxelized alone: the solid voxel count, from the
     closest-point Mahalanobis distance and the Beer-Lambert threshold
-    (voxel/shaders/voxelize.ts:368-446), and its block-aligned bounds
+    (voxel/shaders/voxelize.ts:62-140), and its block-aligned bounds
     (voxelize.ts:278-306).
 Run: python tests/golden/make_golden.py
 """
