@@ -3,10 +3,10 @@ droplet scenes, behind droplet's public API (src/index.ts:16-38)."""
 from .types import (BackgroundRGBA, Bounds, RenderCamera, SplatData, mat4Identity, mat4LookAt,
                     numSHCoeffsPerChannel, quatRotate, splatInputStride, vec3)
 from ._lib import DropletError
-from .api import (BlockMaskBuffer, Device, Mlp, Renderer, Scene, VoxelBlock, VoxelizeResult, createDevice,
-                  voxelize)
+from .api import (BlockMaskBuffer, Device, GpuRadixSorter, Mlp, Renderer, Scene, VoxelBlock, VoxelizeResult,
+                  createDevice, mortonDecode3, mortonEncode3, voxelize)
 
 __all__ = ["BackgroundRGBA", "Bounds", "RenderCamera", "SplatData", "mat4Identity", "mat4LookAt",
            "numSHCoeffsPerChannel", "quatRotate", "splatInputStride", "vec3", "DropletError",
-           "BlockMaskBuffer", "Device", "Mlp", "Renderer", "Scene", "VoxelBlock", "VoxelizeResult", "createDevice",
-           "voxelize"]
+           "BlockMaskBuffer", "Device", "GpuRadixSorter", "Mlp", "Renderer", "Scene", "VoxelBlock", "VoxelizeResult", "createDevice",
+           "mortonDecode3", "mortonEncode3", "voxelize"]

@@ -35,6 +35,7 @@ EXPORTS = [
     "dl_renderer_launch_count", "dl_renderer_set_debug", "dl_render_many",
     "dl_render_static", "dl_mlp_create", "dl_mlp_destroy", "dl_mlp_get_params", "dl_mlp_set_params",
     "dl_mlp_predict", "dl_mlp_grad", "dl_mlp_train", "dl_renderer_set_scheduler", "dl_renderer_tile_log",
+    "dl_sorter_create", "dl_sorter_destroy", "dl_sorter_set_stream", "dl_sorter_set_digit_bits", "dl_sorter_sort",
 ]
 
 
@@ -110,6 +111,11 @@ def load():
         "dl_renderer_stage_times": [vp, P(ctypes.c_double), i],
         "dl_renderer_launch_count": [vp, P(ctypes.c_uint64)],
         "dl_renderer_set_debug": [vp, i],
+        "dl_sorter_create": [vp, P(vp)],
+        "dl_sorter_destroy": [vp],
+        "dl_sorter_set_stream": [vp, vp],
+        "dl_sorter_set_digit_bits": [vp, i],
+        "dl_sorter_sort": [vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32, P(vp), P(vp)],
     }
     for name, args in sigs.items():
         f = getattr(L, name)

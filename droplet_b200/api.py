@@ -417,3 +417,83 @@ class Mlp:
             self.destroy()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- Morton order (src/voxel/morton.ts:11-22)
+def mortonEncode3(x: int, y: int, z: int) -> int:
+    """morton.ts:11-14 — in-block index of (x, y, z) in [0, 4)^3, bits z2 y2 x2 z1 y1 x1."""
+    return (((x & 1) << 0) | ((y & 1) << 1) | ((z & 1) << 2)
+            | ((x & 2) << 2) | ((y & 2) << 3) | ((z & 2) << 4))
+
+
+def mortonDecode3(m: int):
+    """morton.ts:16-22 — inverse of mortonEncode3."""
+    return ((m & 1) | ((m >> 2) & 2), ((m >> 1) & 1) | ((m >> 3) & 2), ((m >> 2) & 1) | ((m >> 4) & 2))
+
+
+# ---------------------------------------------------------------- GpuRadixSorter (src/gpu/radix-sort.ts:91-216)
+class _DeviceArray:
+    """A library-owned device array seen through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, n: int, owner):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+        self._owner = owner
+
+
+class GpuRadixSorter:
+    """GpuRadixSorter(device).sort(keys, vals, n, keyBits=32) -> (keys, vals).
+
+    keys / vals are CUDA tensors of at least n 32-bit elements (torch.uint32 or
+    torch.int32 bit patterns); vals may be None (the values are then the input
+    positions).  The sort is stable and runs wholly on the device; the result
+    is returned as the pair of arrays that hold it (library-owned arrays come
+    back as torch.int32 tensors of the same bit patterns) — the inputs or the
+    sorter's pong buffers (valid until the next sort), as in the reference.
+    """
+
+    def __init__(self, device: Device):
+        h = ctypes.c_void_p()
+        check(_lib.load().dl_sorter_create(device.handle, ctypes.byref(h)))
+        self._h = h.value
+        self.device = device
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise DropletError(_lib.DL_E_INVALID_ARG, "sorter is destroyed")
+        return self._h
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        check(_lib.load().dl_sorter_set_stream(self.handle, stream_ptr or None))
+
+    def set_digit_bits(self, bits: int):
+        check(_lib.load().dl_sorter_set_digit_bits(self.handle, int(bits)))
+
+    def sort(self, keys, vals, n: int, keyBits: int = 32):
+        import torch
+        for t in (keys, vals):
+            if t is not None and (not t.is_cuda or t.element_size() != 4 or not t.is_contiguous() or t.numel() < n):
+                raise DropletError(_lib.DL_E_INVALID_ARG, "keys / vals must be contiguous 32-bit CUDA tensors "
+                                                           "of at least n elements")
+        ok, ov = ctypes.c_void_p(), ctypes.c_void_p()
+        check(_lib.load().dl_sorter_sort(self.handle, keys.data_ptr(), None if vals is None else vals.data_ptr(),
+                                         int(n), int(keyBits), ctypes.byref(ok), ctypes.byref(ov)))
+
+        def wrap(ptr, like):
+            if like is not None and ptr == like.data_ptr():
+                return like
+            if not ptr:
+                return None
+            return torch.as_tensor(_DeviceArray(ptr, int(n), self), device=keys.device)
+        return wrap(ok.value, keys), wrap(ov.value, vals)
+
+    def destroy(self):
+        if self._h:
+            _lib.load().dl_sorter_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

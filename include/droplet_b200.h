@@ -188,6 +188,25 @@ int dl_vox_result_info(const dl_vox_result* res, double bounds_min[3], double bo
 int dl_vox_result_copy(const dl_vox_result* res, uint32_t* block_idx, uint32_t* mask_lo, uint32_t* mask_hi);
 int dl_vox_result_free(dl_vox_result* res);
 
+/* ---- src/gpu/radix-sort.ts:91-216 GpuRadixSorter ----------------------- */
+/* Stable LSD radix sort of n u32 keys with u32 values in device memory (the
+ * reference's sorter is not stable; a stable order is one it may return).
+ * keys must be below 2^key_bits (key_bits 0 means 32), as the reference
+ * assumes.  vals may be NULL: values are then the input positions (an
+ * argsort).  On return *out_keys / *out_vals point at the sorted arrays —
+ * the inputs or the sorter's own grow-only pong buffers, valid until the next
+ * sort or destroy — as GpuRadixSorter.sort returns its buffer pair
+ * (radix-sort.ts:137-215).  Input arrays are overwritten.  The call returns
+ * after the sort has finished on the sorter's stream. */
+typedef struct dl_sorter dl_sorter;
+int dl_sorter_create(dl_device* dev, dl_sorter** out);        /* radix-sort.ts:101-123 */
+int dl_sorter_destroy(dl_sorter* s);
+int dl_sorter_set_stream(dl_sorter* s, void* cuda_stream);
+/* digit width of the passes: 6, 7 or 8 bits (default 8) */
+int dl_sorter_set_digit_bits(dl_sorter* s, int bits);
+int dl_sorter_sort(dl_sorter* s, uint32_t* keys, uint32_t* vals, uint64_t n, uint32_t key_bits,
+                   uint32_t** out_keys, uint32_t** out_vals);
+
 /* ---- instrumentation (no reference counterpart) ------------------------ */
 /* Copy a named device array of the last single-view render into dst (cap
  * bytes); *bytes receives its size.  Names: "depth_keys", "sorted_idx",

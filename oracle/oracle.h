@@ -1,4 +1,4 @@
-// ORACLE — test infrastructure only (see oracle_render.cpp).  Plain C structs
+// ORACLE — test infrastructure only; parity unpinned (see oracle_render.cpp).  Plain C structs
 // mirroring droplet's SplatData / RenderCamera (src/types.ts:23-32,74-82).
 #pragma once
 #include <stdint.h>

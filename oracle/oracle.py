@@ -4,6 +4,10 @@ ctypes front end for oracle/_build/liboracle.so, the C++ restatement of the
 reference's render and voxelize paths (oracle_render.cpp, oracle_voxel.cpp).
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it,
 always as the checker; the product package never imports it.
+
+Parity unpinned: the reference (TypeScript over WebGPU) cannot run here and publishes no
+numeric vectors; the oracle is checked by closed-form known answers
+(tests/golden/kat.json) and the reference's qualitative checks.
 """
 from __future__ import annotations
 

@@ -9,10 +9,11 @@
 // The only shared code with the product is dl_math.h (exp / atan2 / asin),
 // which the WGSL leaves implementation-defined.
 //
-// Parity pinning: the reference pins no numeric outputs (its only tests are
+// Parity unpinned: the reference pins no numeric outputs (its only tests are
 // qualitative browser checks, examples/browser/test.ts:114-273) and cannot run
-// here (WebGPU), so this oracle is pinned by those ported checks plus
-// hand-derived known answers (tests/golden/).  See the test suite.
+// here (WebGPU), so no reference output exists to pin this oracle against.  It
+// is checked by those ported qualitative checks plus hand-derived closed-form
+// known answers (tests/golden/kat.json).
 #include "oracle.h"
 
 #include <algorithm>

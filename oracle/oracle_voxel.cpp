@@ -4,6 +4,10 @@
 // tests/ and bench.py's cpu_baseline leg as the checker; the product never
 // links or calls it.
 //
+// Parity unpinned: the reference publishes no numeric voxel outputs and cannot
+// run here (WebGPU); the restatement is checked by the ported qualitative
+// checks and by closed-form known answers (tests/golden/kat.json).
+//
 // Two summation orders are offered for the per-voxel density sum:
 //   order 0 (canonical): the Gaussians of a batch list in ascending index;
 //   order 1 (reference): the batch list in the reference's BVH query order

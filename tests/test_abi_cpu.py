@@ -64,3 +64,17 @@ def test_block_mask_buffer_semantics():
     b.addBlock(9, 0, 0)
     assert b.count == 1 and b.get(5).maskLo == 3 and b.get(5).maskHi == 0x80000000
     assert b.popcount() == 3 and b.get(9) is None
+
+
+def test_morton_round_trip_and_bit_layout():
+    """morton.ts:11-22: x, y, z bits interleaved x1 y1 z1 x2 y2 z2 from bit 0."""
+    seen = set()
+    for z in range(4):
+        for y in range(4):
+            for x in range(4):
+                m = dl.mortonEncode3(x, y, z)
+                assert dl.mortonDecode3(m) == (x, y, z)
+                expect = sum(((v >> b) & 1) << (3 * b + a) for a, v in enumerate((x, y, z)) for b in range(2))
+                assert m == expect
+                seen.add(m)
+    assert seen == set(range(64))
