@@ -61,7 +61,8 @@ class DlRendererOpts(ctypes.Structure):
 class DlVoxOpts(ctypes.Structure):
     _fields_ = [("voxel_resolution", ctypes.c_double), ("opacity_cutoff", ctypes.c_double),
                 ("use_defaults", ctypes.c_int32), ("has_bounds", ctypes.c_int32),
-                ("bounds_min", ctypes.c_double * 3), ("bounds_max", ctypes.c_double * 3)]
+                ("bounds_min", ctypes.c_double * 3), ("bounds_max", ctypes.c_double * 3),
+                ("shard_index", ctypes.c_int32), ("shard_count", ctypes.c_int32)]
 
 
 _lib = None

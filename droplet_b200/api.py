@@ -322,7 +322,11 @@ class VoxelizeResult:
 
 
 def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> VoxelizeResult:
-    """voxelize.ts:59-248.  opts: {voxelResolution=0.05, opacityCutoff=0.1, bounds}."""
+    """voxelize.ts:59-248.  opts: {voxelResolution=0.05, opacityCutoff=0.1, bounds}.
+
+    opts["shard"] = (index, count) voxelizes only that shard of the grid's z rows
+    of 16^3-block batches (see droplet_b200.shard); bounds and numBlocks stay
+    those of the whole grid."""
     opts = opts or {}
     o = _lib.DlVoxOpts()
     res = opts.get("voxelResolution")
@@ -337,6 +341,9 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
         for k in range(3):
             o.bounds_min[k] = float(bmin[k])
             o.bounds_max[k] = float(bmax[k])
+    sh = opts.get("shard")
+    if sh is not None:
+        o.shard_index, o.shard_count = int(sh[0]), int(sh[1])
     L = _lib.load()
     h = ctypes.c_void_p()
     check(L.dl_voxelize(device.handle, ctypes.byref(_splats(data)), ctypes.byref(o), ctypes.byref(h)))

@@ -663,6 +663,9 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         }
     }
     for (int k = 0; k < 3; k++) R->dims[k] = js_round((R->bmax[k] - R->bmin[k]) / blockSize);
+    const int shardCount = (opts && opts->shard_count > 1) ? opts->shard_count : 1;
+    const int shardIndex = shardCount > 1 ? opts->shard_index : 0;
+    if (shardIndex < 0 || shardIndex >= shardCount) { dl_set_error("voxelize: shard_index out of range"); return fail(DL_E_INVALID_ARG); }
     const bool anyBlocks = n > 0 && R->dims[0] > 0 && R->dims[1] > 0 && R->dims[2] > 0;
     if (!anyBlocks) { *out = R; return DL_OK; }
     for (int k = 0; k < 3; k++) {
@@ -731,9 +734,12 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             dl_set_error(std::string("voxelize: ") + cudaGetErrorString(cudaGetLastError()));
             return fail(DL_E_CUDA);
         }
+        // shards: z rows split evenly by count
+        const int64_t zr0 = p.NBB[2] * shardIndex / shardCount, zr1 = p.NBB[2] * (shardIndex + 1) / shardCount;
         for (uint64_t b = 0; b < numBatches; b++) {
             if (!used[b]) continue;
             const int64_t bxI = b % p.NBB[0], byI = (b / p.NBB[0]) % p.NBB[1], bzI = b / (p.NBB[0] * p.NBB[1]);
+            if (bzI < zr0 || bzI >= zr1) continue;
             const int64_t cx = std::min<int64_t>(16, p.NB[0] - bxI * 16), cy = std::min<int64_t>(16, p.NB[1] - byI * 16);
             const int64_t cz = std::min<int64_t>(16, p.NB[2] - bzI * 16);
             for (int64_t bi = 0; bi < cx * cy * cz; bi++) {
@@ -772,8 +778,28 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             for (int64_t x = 0; x < NBX_; x++) a += bc[(z * NBY_ + y) * NBX_ + x];
             return a;
         };
-        Slab cur{0, 0, 0, NBY_, 0, NBX_, 0};                     // whole z rows being merged
-        for (int64_t z = 0; z < NBZ_; z++) {
+        // this shard's z rows: contiguous, about 1/shardCount of all pairs each
+        int64_t zr0 = 0, zr1 = NBZ_;
+        if (shardCount > 1) {
+            std::vector<unsigned long long> before((size_t)NBZ_ + 1, 0ull);
+            for (int64_t z = 0; z < NBZ_; z++) {
+                unsigned long long zs = 0;
+                for (int64_t y = 0; y < NBY_; y++) zs += rowSum(z, y);
+                before[z + 1] = before[z] + zs;
+            }
+            auto boundary = [&](int i) -> int64_t {
+                if (i <= 0) return 0;
+                if (i >= shardCount) return NBZ_;
+                const unsigned long long target = (unsigned long long)((double)before[NBZ_] * i / shardCount);
+                int64_t z = 0;
+                while (z < NBZ_ && before[z] < target) z++;
+                return z;
+            };
+            zr0 = boundary(shardIndex);
+            zr1 = std::max(zr0, boundary(shardIndex + 1));
+        }
+        Slab cur{zr0, zr0, 0, NBY_, 0, NBX_, 0};                 // whole z rows being merged
+        for (int64_t z = zr0; z < zr1; z++) {
             unsigned long long zs = 0;
             for (int64_t y = 0; y < NBY_; y++) zs += rowSum(z, y);
             if (zs <= kSlabCap) {

@@ -82,6 +82,14 @@ typedef struct dl_vox_opts {
     int32_t has_bounds;           /* 1: use bounds_min/bounds_max (opts.bounds) */
     double bounds_min[3];
     double bounds_max[3];
+    /* Multi-GPU sharding (no reference counterpart): with shard_count > 1 the
+     * call voxelizes only shard shard_index of the grid's z rows of 16^3-block
+     * batches, split into shard_count contiguous row ranges of about equal
+     * Gaussian-block pair counts (equal row counts when opacity_cutoff <= 0).  Bounds and dims stay those of the whole
+     * grid; concatenating the block lists of shards 0..count-1 gives the
+     * unsharded list in the reference's order.  0 / 0 voxelizes everything. */
+    int32_t shard_index;
+    int32_t shard_count;
 } dl_vox_opts;
 
 /* ---- errors ------------------------------------------------------------ */

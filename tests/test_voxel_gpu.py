@@ -100,3 +100,29 @@ def test_reference_order_differs_only_near_cutoff(device):
         assert ((a[0] ^ b[0]) & ~n[0]) == 0 and ((a[1] ^ b[1]) & ~n[1]) == 0
         differing += bin(a[0] ^ b[0]).count("1") + bin(a[1] ^ b[1]).count("1")
     print(f"bits differing from the reference order: {differing} (all within eps={EPS})")
+
+
+@pytest.mark.parametrize("count", [2, 3, 5])
+def test_z_row_shards_concatenate_to_the_whole_grid(device, count):
+    # each shard voxelizes a contiguous range of z rows of batches; in shard
+    # order the block lists concatenate to the unsharded list
+    from droplet_b200 import shard
+    d = synth.voxel_1m(60_000)
+    opts = {"voxelResolution": 0.04, "opacityCutoff": 0.1}
+    whole = dl.voxelize(device, d, opts)
+    parts = [shard.voxelize_sharded(device, d, opts, i, count) for i in range(count)]
+    idx = np.concatenate([p.buffer.blockIdx for p in parts])
+    lo = np.concatenate([p.buffer.maskLo for p in parts])
+    hi = np.concatenate([p.buffer.maskHi for p in parts])
+    assert np.array_equal(idx, whole.buffer.blockIdx)
+    assert np.array_equal(lo, whole.buffer.maskLo) and np.array_equal(hi, whole.buffer.maskHi)
+    for p in parts:
+        assert (p.numBlocksX, p.numBlocksY, p.numBlocksZ) == (whole.numBlocksX, whole.numBlocksY, whole.numBlocksZ)
+    assert sum(p.buffer.count > 0 for p in parts) >= 2
+    for cut in (0.0,):
+        o2 = dict(opts, opacityCutoff=cut)
+        w2 = dl.voxelize(device, d, o2)
+        p2 = [shard.voxelize_sharded(device, d, o2, i, count) for i in range(count)]
+        assert np.array_equal(np.concatenate([p.buffer.blockIdx for p in p2]), w2.buffer.blockIdx)
+    with pytest.raises(dl.DropletError):
+        dl.voxelize(device, d, dict(opts, shard=(count, count)))
