@@ -18,8 +18,9 @@ seeded clusters in [-10, 10]^3).  Synthetic, seeded data (numpy PCG64).
 --impl reference times the reference's algorithm on the host cores instead:
 the C++ restatement of droplet's CPU stages and WGSL shaders (oracle/), since
 the reference itself only runs on WebGPU, which this machine does not have.
-Multi-GPU (torchrun): every rank renders the full batch (views are
-independent, no collective on the data path); scaling is weak.
+Multi-GPU (torchrun): every rank renders a full 64-view batch of its own
+(the ring turned by rank/N of a view step, so all views are distinct); views
+are independent, so there is no collective on the data path; scaling is weak.
 """
 from __future__ import annotations
 
@@ -54,10 +55,12 @@ def parse():
     return p.parse_args()
 
 
-def workload(args):
+def workload(args, rank=0, world=1):
+    """The scene and this rank's ring: rank r of N renders the ring turned by
+    r/N of a view step, so N ranks render 64 N distinct views (weak scaling)."""
     from droplet_b200 import synth
     data = synth.sh3_3m(args.splats)
-    cams = synth.ring_cameras(args.views)
+    cams = synth.ring_cameras(args.views, phase=rank / max(world, 1))
     return data, cams
 
 
@@ -250,7 +253,7 @@ def run_ours(args, rank, world, local_rank):
     from droplet_b200 import _lib
 
     torch.cuda.set_device(local_rank)
-    data, cams = workload(args)
+    data, cams = workload(args, rank, world)
     pix = sum(c.width * c.height for c in cams)
     dev = dl.createDevice({"ordinal": local_rank})
     r = dl.Renderer(dev)
@@ -368,7 +371,8 @@ def run_ours(args, rank, world, local_rank):
             "config": config(args, cams, {"mode": "batched: one CUDA-graph replay per step for all views, f16 scene "
                                                   "SH and records, hardware exp2 (+-1 LSB), tiles rasterized in "
                                                   "decreasing cost predicted by the learned model",
-                                          "parallelism": f"views replicated per GPU x{world}"}),
+                                          "parallelism": f"views sharded: {world} rank(s) x {len(cams)} distinct "
+                                                         f"views, scene replicated"}),
             "plain_value": plain_value, "exact_value": exact_value, "static_value": static_value,
             "learned": (model.meta if model is not None else None),
             "vs_plain": (value / plain_value) if plain_value else None,

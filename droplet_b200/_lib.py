@@ -23,6 +23,7 @@ DL_BATCH_STATIC = 16
 DL_BATCH_FAST_EXP = 32
 DL_BATCH_COUNT_EVALS = 64
 DL_BATCH_LOG_TILES = 128
+DL_BATCH_F64_DEGENERATE = 256
 DL_MLP_IN, DL_MLP_HIDDEN = 12, 64
 DL_MLP_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 
@@ -36,6 +37,7 @@ EXPORTS = [
     "dl_render_static", "dl_mlp_create", "dl_mlp_destroy", "dl_mlp_get_params", "dl_mlp_set_params",
     "dl_mlp_predict", "dl_mlp_grad", "dl_mlp_train", "dl_renderer_set_scheduler", "dl_renderer_tile_log",
     "dl_sorter_create", "dl_sorter_destroy", "dl_sorter_set_stream", "dl_sorter_set_digit_bits", "dl_sorter_sort",
+    "dl_renderer_set_tuning", "dl_renderer_get_tuning", "dl_renderer_autotune",
 ]
 
 
@@ -56,6 +58,11 @@ class DlCamera(ctypes.Structure):
 
 class DlRendererOpts(ctypes.Structure):
     _fields_ = [("chunk_cap", ctypes.c_uint32), ("max_coverage_per_splat", ctypes.c_uint32)]
+
+
+class DlTuning(ctypes.Structure):
+    _fields_ = [("pair_sort_bits", ctypes.c_int32), ("raster_shape", ctypes.c_int32),
+                ("raster_ctas_per_sm", ctypes.c_int32)]
 
 
 class DlVoxOpts(ctypes.Structure):
@@ -117,6 +124,10 @@ def load():
         "dl_sorter_set_stream": [vp, vp],
         "dl_sorter_set_digit_bits": [vp, i],
         "dl_sorter_sort": [vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32, P(vp), P(vp)],
+        "dl_renderer_set_tuning": [vp, P(DlTuning)],
+        "dl_renderer_get_tuning": [vp, P(DlTuning)],
+        "dl_renderer_autotune": [vp, vp, P(DlCamera), i, P(ctypes.c_float), ctypes.c_uint32, i, P(DlTuning),
+                                 P(ctypes.c_double)],
     }
     for name, args in sigs.items():
         f = getattr(L, name)

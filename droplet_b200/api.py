@@ -184,6 +184,32 @@ class Renderer:
         check(_lib.load().dl_render_batch(self.handle, scene._h, cams, n, _bg(background), ptrs, flags))
         return host
 
+    RASTER_SHAPES = ("8x4", "16x2", "4x8")
+
+    def set_tuning(self, pair_sort_bits: int = 8, raster_shape: str = "8x4", raster_ctas_per_sm: int = 0):
+        """Timing-only knobs of rendered frames (dl_tuning); no knob changes a pixel."""
+        t = _lib.DlTuning(int(pair_sort_bits), self.RASTER_SHAPES.index(raster_shape), int(raster_ctas_per_sm))
+        check(_lib.load().dl_renderer_set_tuning(self.handle, ctypes.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = _lib.DlTuning()
+        check(_lib.load().dl_renderer_get_tuning(self.handle, ctypes.byref(t)))
+        return {"pair_sort_bits": t.pair_sort_bits, "raster_shape": self.RASTER_SHAPES[t.raster_shape],
+                "raster_ctas_per_sm": t.raster_ctas_per_sm}
+
+    def autotune(self, scene: Scene, cameras: Sequence[RenderCamera], background=None, flags: int = 0,
+                 reps: int = 3) -> dict:
+        """Pick the fastest tuning for this batch (coordinate descent over the
+        knobs, each candidate timed on the device) and keep it on the renderer."""
+        cams = (_lib.DlCamera * len(cameras))(*[_camera(c) for c in cameras])
+        best = _lib.DlTuning()
+        ms = ctypes.c_double()
+        check(_lib.load().dl_renderer_autotune(self.handle, scene._h, cams, len(cameras), _bg(background), flags,
+                                               reps, ctypes.byref(best), ctypes.byref(ms)))
+        out = self.get_tuning()
+        out["frame_ms"] = float(ms.value)
+        return out
+
     def set_scheduler(self, mlp: Optional["Mlp"]):
         """Attach the learned tile-cost model (batched frames then rasterize
         tiles longest-predicted first); None restores launch order."""

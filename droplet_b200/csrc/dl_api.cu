@@ -1,5 +1,6 @@
 // dl_api.cu — the C ABI (include/droplet_b200.h): devices, renderers, scenes,
 // status codes and the thread-local error message.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -273,5 +274,83 @@ extern "C" int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst
     if (cap < n) { dl_set_error("debug_get: destination too small"); return DL_E_INVALID_ARG; }
     if (host) std::memcpy(dst, src, n);
     else DL_CK(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t) {
+    if (!r || !t) { dl_set_error("dl_renderer_set_tuning: NULL argument"); return DL_E_INVALID_ARG; }
+    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 2 ||
+        t->raster_ctas_per_sm < 0 || t->raster_ctas_per_sm > 5) {
+        dl_set_error("dl_renderer_set_tuning: knob out of range");
+        return DL_E_INVALID_ARG;
+    }
+    r->tune.pair_bits = t->pair_sort_bits;
+    r->tune.shape = t->raster_shape;
+    r->tune.ctas_per_sm = t->raster_ctas_per_sm;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_get_tuning(dl_renderer* r, dl_tuning* t) {
+    if (!r || !t) { dl_set_error("dl_renderer_get_tuning: NULL argument"); return DL_E_INVALID_ARG; }
+    t->pair_sort_bits = r->tune.pair_bits;
+    t->raster_shape = r->tune.shape;
+    t->raster_ctas_per_sm = r->tune.ctas_per_sm;
+    return DL_OK;
+}
+
+extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
+                                    uint32_t flags, int reps, dl_tuning* best, double* best_ms) {
+    if (!r || !s || !cams || n <= 0) { dl_set_error("dl_renderer_autotune: bad argument"); return DL_E_INVALID_ARG; }
+    if (flags & DL_BATCH_PLAIN) { dl_set_error("dl_renderer_autotune: the plain path is not tuned"); return DL_E_INVALID_ARG; }
+    reps = std::max(1, std::min(reps, 50));
+    DL_CK(cudaSetDevice(r->dev->ordinal));
+    uint64_t total = 0;
+    std::vector<uint64_t> offs((size_t)n);
+    for (int i = 0; i < n; i++) { offs[i] = total; total += (uint64_t)cams[i].width * cams[i].height * 4; }
+    DL_TRY(r->tuneOut.ensure(std::max<uint64_t>(total, 256)));
+    std::vector<uint8_t*> outs((size_t)n);
+    for (int i = 0; i < n; i++) outs[i] = r->tuneOut.as<uint8_t>() + offs[i];
+    cudaEvent_t e0, e1;
+    DL_CK(cudaEventCreate(&e0));
+    DL_CK(cudaEventCreate(&e1));
+    const uint32_t fl = flags | DL_BATCH_OUT_DEVICE;
+    auto timeOne = [&](const DlTuning& t, double* ms) -> int {
+        r->tune = t;
+        DL_TRY(dl_render_batch(r, s, cams, n, bg, outs.data(), fl));          // warm-up (and graph capture)
+        std::vector<double> v;
+        for (int k = 0; k < reps; k++) {
+            cudaEventRecord(e0, r->stream);
+            DL_TRY(dl_render_batch(r, s, cams, n, bg, outs.data(), fl));
+            cudaEventRecord(e1, r->stream);
+            DL_CK(cudaEventSynchronize(e1));
+            float f = 0.0f;
+            cudaEventElapsedTime(&f, e0, e1);
+            v.push_back(f);
+        }
+        std::sort(v.begin(), v.end());
+        *ms = v[v.size() / 2];
+        return DL_OK;
+    };
+    DlTuning cur = r->tune;
+    double curMs = 0.0;
+    int rc = timeOne(cur, &curMs);
+    const int bitsC[3] = {8, 7, 6}, shapeC[3] = {0, 1, 2}, ctasC[3] = {0, 4, 3};
+    for (int knob = 0; knob < 3 && rc == DL_OK; knob++) {
+        for (int c = 0; c < 3 && rc == DL_OK; c++) {
+            DlTuning t = cur;
+            if (knob == 0) { if (t.pair_bits == bitsC[c]) continue; t.pair_bits = bitsC[c]; }
+            if (knob == 1) { if (t.shape == shapeC[c]) continue; t.shape = shapeC[c]; }
+            if (knob == 2) { if (t.ctas_per_sm == ctasC[c]) continue; t.ctas_per_sm = ctasC[c]; }
+            double ms = 0.0;
+            rc = timeOne(t, &ms);
+            if (rc == DL_OK && ms < curMs) { cur = t; curMs = ms; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    r->tune = cur;
+    if (rc != DL_OK) return rc;
+    if (best) { best->pair_sort_bits = cur.pair_bits; best->raster_shape = cur.shape; best->raster_ctas_per_sm = cur.ctas_per_sm; }
+    if (best_ms) *best_ms = curMs;
     return DL_OK;
 }

@@ -61,6 +61,13 @@ struct dl_scene {
     int precision = DL_PREC_F32;
 };
 
+// Knobs of a batched frame that change timing only (dl_tuning in the ABI).
+struct DlTuning {
+    int pair_bits = 8;        // pair-sort digit width 6..8
+    int shape = 0;            // rasterizer work item: 0 8x4, 1 16x2, 2 4x8 pixels
+    int ctas_per_sm = 0;      // persistent rasterizer CTAs per SM; 0 = occupancy limit
+};
+
 // Host-side state of the tile-binned renderer.
 struct dl_renderer {
     dl_device* dev = nullptr;
@@ -111,6 +118,9 @@ struct dl_renderer {
     dl_mlp* sched = nullptr;
     DevBuf feat, pred, skeys0, skeys1, svals0, svals1, sseg, sstatus, shist, tileCycles;
     uint32_t log_tiles = 0;
+
+    DlTuning tune;                      // dl_renderer_set_tuning / dl_renderer_autotune
+    DevBuf tuneOut;                     // autotuner's device images
 };
 
 struct dl_mlp;

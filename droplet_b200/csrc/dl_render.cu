@@ -201,7 +201,8 @@ struct FrameDims {
     uint64_t stride = 64, cap = 0;
     uint32_t depthGrid = 1, emitTilesPerView = 1, pairGrid = 1;
     int pbits = 8, ppasses = 0;
-    bool f16rec = false, fastExp = false;
+    bool f16rec = false, fastExp = false, f64deg = false;
+    int subLw = 3;                       // rasterizer work item width log2 (8x4)
 };
 
 // Persistent rasterizer grid: every SM filled to its occupancy limit.
@@ -220,8 +221,11 @@ uint32_t raster_grid(bool fastExp) {
     return (uint32_t)g;
 }
 
-FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uint32_t flags) {
+FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uint32_t flags,
+                     const DlTuning& t = DlTuning()) {
     FrameDims d;
+    d.pbits = (t.pair_bits >= 6 && t.pair_bits <= 8) ? t.pair_bits : 8;
+    d.subLw = t.shape == 1 ? 4 : t.shape == 2 ? 2 : 3;
     d.V = V;
     d.N = N;
     d.stride = round_up(std::max<uint32_t>(N, 1), 64);
@@ -235,11 +239,22 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     int keyBits = 0;
     while ((1u << keyBits) < d.maxT) keyBits++;
     d.ppasses = (keyBits + d.pbits - 1) / d.pbits;
+    if (d.ppasses > 4) {                 // the digit tables hold 4 passes
+        d.pbits = 8;
+        d.ppasses = (keyBits + 7) / 8;
+    }
     d.cap = cap;
     d.pairGrid = std::max<uint32_t>(1, (uint32_t)(V * ((cap + dlsort::kTile - 1) / dlsort::kTile)));
     d.f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
     d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
+    d.f64deg = (flags & DL_BATCH_F64_DEGENERATE) != 0;
     d.rasterGrid = raster_grid(d.fastExp);
+    if (t.ctas_per_sm > 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        d.rasterGrid = std::min<uint32_t>(d.rasterGrid, (uint32_t)(std::max(sms, 1) * t.ctas_per_sm));
+    }
     return d;
 }
 
@@ -263,6 +278,7 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
     pa.recH = d.f16rec ? f.recH : nullptr;
     pa.bbox = f.bbox;
     pa.nvis = f.nvis;
+    pa.f64_degenerate = d.f64deg ? 1 : 0;
     if (d.N) {
         dlr::project_k<<<(d.N + 255) / 256, 256, 0, st>>>(pa);
         (*launches)++;
@@ -429,6 +445,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.eval_count = f.evalCount;
     ra.tile_evals = f.tileEvals;
     ra.tile_cycles = f.tileCycles;
+    ra.sub_lw = d.subLw;
     if (d.fastExp) dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
     else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
     (*launches)++;
@@ -445,7 +462,9 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     cudaStream_t st = r->stream;
     const uint32_t N = sc.n;
     if (r->pair_cap_per_view == 0) r->pair_cap_per_view = std::max<uint64_t>(1u << 20, 4ull * N);
-    FrameDims d = frame_dims(hv, V, N, r->pair_cap_per_view, flags);
+    // the plain path keeps the default knobs
+    const DlTuning tune = (flags & DL_BATCH_PLAIN) ? DlTuning() : r->tune;
+    FrameDims d = frame_dims(hv, V, N, r->pair_cap_per_view, flags, tune);
     const bool countEvals = (flags & DL_BATCH_COUNT_EVALS) != 0;
     r->launches = 0;
 
@@ -573,7 +592,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     for (int attempt = 0; attempt < 3; attempt++) {
         const uint64_t cap = r->pair_cap_per_view;
         if (cap >= (1ull << 30)) { dl_set_error("more than 2^30 tile pairs in one view"); return DL_E_CAPACITY; }
-        d = frame_dims(hv, V, N, cap, flags);
+        d = frame_dims(hv, V, N, cap, flags, tune);
         DL_TRY(r->pkeys0.ensure(4ull * V * cap));
         DL_TRY(r->pvals0.ensure(4ull * V * cap));
         DL_TRY(r->pkeys1.ensure(4ull * V * cap));
@@ -608,7 +627,8 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             key.assign(fp, fp + sizeof(FramePtrs) / 8);
             const uint64_t* sp = reinterpret_cast<const uint64_t*>(&sc);
             key.insert(key.end(), sp, sp + sizeof(DlSceneDev) / 8);
-            key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid});
+            key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid,
+                                   (uint64_t)d.pbits, (uint64_t)d.subLw});
             if (!r->graph_exec || key != r->graph_key) {
                 if (r->graph_exec) { cudaGraphExecDestroy(r->graph_exec); r->graph_exec = nullptr; }
                 cudaGraph_t g = nullptr;

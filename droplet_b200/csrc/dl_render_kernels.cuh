@@ -36,7 +36,12 @@ struct ProjectArgs {
     uint2* bbox;              // [V][stride] (minX | minY<<16, maxX | maxY<<16), bit 15 of each max
                               // field = box entirely left of / above the image; empty if minX > maxX
     uint32_t* nvis;           // [V] visible count
+    int f64_degenerate;       // recompute det / conic / AA factor in f64 for near-degenerate splats
 };
+
+// A 2D covariance is near-degenerate when its f32 determinant has lost at
+// least 10 of its 24 bits to cancellation: det < 2^-10 * c00 * c11.
+constexpr float kDegenerateRel = 1.0f / 1024.0f;
 
 struct Cov3 { float c00, c01, c02, c11, c12, c22; };
 
@@ -220,21 +225,33 @@ __global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
             const float b02 = j00 * cc02 + j02 * cc22;
             const float b11 = j11 * cc11 + j12 * cc12;
             const float b12 = j11 * cc12 + j12 * cc22;
-            float c00 = b00 * j00 + b02 * j02;
+            const float c00o = b00 * j00 + b02 * j02;
             const float c01 = b01 * j11 + b02 * j12;
-            float c11 = b11 * j11 + b12 * j12;
-            const float detOrig = c00 * c11 - c01 * c01;
-            c00 = c00 + DL_AA_DILATION;
-            c11 = c11 + DL_AA_DILATION;
+            const float c11o = b11 * j11 + b12 * j12;
+            const float detOrig = c00o * c11o - c01 * c01;
+            const float c00 = c00o + DL_AA_DILATION;
+            const float c11 = c11o + DL_AA_DILATION;
             const float det = c00 * c11 - c01 * c01;
             aaFactor = sqrtf(fmaxf(detOrig / det, 0.0f));
             if (det <= 1.0e-6f) {
                 culled = true;
+            } else if (a.f64_degenerate && det < kDegenerateRel * (c00 * c11)) {
+                // precision variant: determinants and inverse in f64 from the f32
+                // covariance (products of two f32 are exact in f64); the cull,
+                // radius and tile decisions below keep the f32 determinant
+                const double d64 = (double)c00 * (double)c11 - (double)c01 * (double)c01;
+                const double o64 = (double)c00o * (double)c11o - (double)c01 * (double)c01;
+                conicA = (float)((double)c11 / d64);
+                conicB = (float)(-(double)c01 / d64);
+                conicC = (float)((double)c00 / d64);
+                aaFactor = (float)sqrt(fmax(o64 / d64, 0.0));
             } else {
                 const float invDet = 1.0f / det;
                 conicA = c11 * invDet;
                 conicB = -c01 * invDet;
                 conicC = c00 * invDet;
+            }
+            if (!culled) {
                 const float mid = 0.5f * (c00 + c11);
                 const float radiusEig = sqrtf(fmaxf(0.1f, mid * mid - det));
                 const float lambda1 = mid + radiusEig;
@@ -598,8 +615,8 @@ __global__ void sched_scatter_k(const uint32_t* __restrict__ bucket, uint32_t to
 }
 
 // ------------------------------------------------------------------ rasterize
-// Persistent, warp-granular rasterizer.  A work item is one 8x4-pixel
-// sub-tile (a quarter-row block) of one 16x16 tile of one view; each warp pulls
+// Persistent, warp-granular rasterizer.  A work item is one 32-pixel
+// sub-tile (8x4 by default; 16x2 or 4x8 as tuned) of one 16x16 tile of one view; each warp pulls
 // items from a queue (natural order, or the cost order of a work list) and
 // owns the item's 32 pixels, one per lane.  It walks its tile's slice 32 pairs
 // at a time: every lane loads one pair's screen record, keeps it if the
@@ -631,6 +648,7 @@ struct RasterArgs {
     unsigned long long* eval_count;   // optional: total evaluated (pixel, splat) pairs
     uint32_t* tile_evals;          // optional [total tiles] evaluated pairs per tile
     uint32_t* tile_cycles;         // optional [total tiles] SM cycles / 16 spent per tile
+    int sub_lw;                    // log2 of a work item's width: 3 (8x4), 4 (16x2) or 2 (4x8) pixels
 };
 
 constexpr int kRasterThreads = 256;
@@ -663,14 +681,16 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
     const DlView& u = a.views[v];
     const int lane = threadIdx.x & 31;
     const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
-    const uint32_t sx0 = tx * DL_TILE + (sub & 1) * 8, sy0 = ty * DL_TILE + (sub >> 1) * 4;
-    const uint32_t x = sx0 + (lane & 7), y = sy0 + (lane >> 3);
+    // a work item is sw x sh pixels (sw * sh = 32), 8 items per 16x16 tile
+    const uint32_t lw = (uint32_t)a.sub_lw, sw = 1u << lw, sh = 32u >> lw, perRow = DL_TILE >> lw;
+    const uint32_t sx0 = tx * DL_TILE + (sub % perRow) * sw, sy0 = ty * DL_TILE + (sub / perRow) * sh;
+    const uint32_t x = sx0 + (lane & (sw - 1)), y = sy0 + (lane >> lw);
     const bool inImage = x < u.W && y < u.H;
     if (__all_sync(0xffffffffu, !inImage)) return;       // sub-tile entirely outside the image
     const long long t0 = a.tile_cycles ? clock64() : 0;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
-    const float rx0 = (float)sx0 + 0.5f - 1.0f, rx1 = (float)sx0 + 7.5f + 1.0f;
-    const float ry0 = (float)sy0 + 0.5f - 1.0f, ry1 = (float)sy0 + 3.5f + 1.0f;
+    const float rx0 = (float)sx0 + 0.5f - 1.0f, rx1 = (float)(sx0 + sw) - 0.5f + 1.0f;
+    const float ry0 = (float)sy0 + 0.5f - 1.0f, ry1 = (float)(sy0 + sh) - 0.5f + 1.0f;
     const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
     const uint32_t start = to[tile], end = to[tile + 1];
     const uint32_t* vals = a.pair_vals + a.pair_base[v];

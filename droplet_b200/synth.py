@@ -99,12 +99,17 @@ def sh3_3m_cameras():
                          math.pi / 3, 0.01, 1000.0, "equirect")]
 
 
-def ring_cameras(count: int = 64, radius: float = 12.0, height: float = 2.0, resolutions=None):
-    """Cameras at angle 2*pi*k/count on a ring, looking at the origin."""
+def zipf_10m_cameras(count: int = 16):
+    """16 1920x1080 views of the 10M-Gaussian Zipf scene from a ring around it."""
+    return ring_cameras(count, radius=45.0, height=5.0, resolutions=[(1920, 1080)])
+
+
+def ring_cameras(count: int = 64, radius: float = 12.0, height: float = 2.0, resolutions=None, phase: float = 0.0):
+    """Cameras at angle 2*pi*(k + phase)/count on a ring, looking at the origin."""
     res = resolutions or RING_RESOLUTIONS
     cams = []
     for k in range(count):
-        a = 2.0 * math.pi * k / count
+        a = 2.0 * math.pi * (k + phase) / count
         w, h = res[k % len(res)]
         cams.append(pinhole(w, h, (radius * math.sin(a), height, radius * math.cos(a))))
     return cams

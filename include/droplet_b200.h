@@ -126,7 +126,9 @@ enum {
     DL_BATCH_STATIC = 16,         /* rasterize tiles in launch order, not cost order */
     DL_BATCH_FAST_EXP = 32,       /* hardware ex2 in the rasterizer (+-1 LSB) */
     DL_BATCH_COUNT_EVALS = 64,    /* count evaluated (pixel, splat) pairs ("evals") */
-    DL_BATCH_LOG_TILES = 128      /* keep per-tile features and measured cost (dl_renderer_tile_log) */
+    DL_BATCH_LOG_TILES = 128,     /* keep per-tile features and measured cost (dl_renderer_tile_log) */
+    DL_BATCH_F64_DEGENERATE = 256 /* f64 determinant and inverse for near-degenerate 2D covariances
+                                     (det < 2^-10 c00 c11); culling and tile ranges unchanged */
 };
 /* Render n views of one resident scene; outs[i] receives cams[i].width *
  * cams[i].height RGBA8 pixels (host or device memory, per flags). */
@@ -153,6 +155,26 @@ int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams,
  * max_coverage 0 selects the default 16384. */
 int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg[4], uint32_t max_coverage,
                      uint8_t* out_rgba, size_t out_len);
+
+/* ---- tuning (no reference counterpart) -----------------------------------
+ * Knobs of rendered frames that change timing only, never a pixel.  The
+ * binning tile stays 16x16 (the reference's TILE_SIZE): another tile shape
+ * changes which tiles the maxCoverage truncation keeps (it is row-major in
+ * tile space), and so changes pixels. */
+typedef struct dl_tuning {
+    int32_t pair_sort_bits;       /* digit width of the tile-pair sort: 6, 7 or 8 (default 8) */
+    int32_t raster_shape;         /* pixels of one rasterizer work item (one warp): 0 = 8x4, 1 = 16x2, 2 = 4x8 */
+    int32_t raster_ctas_per_sm;   /* persistent rasterizer CTAs per SM, 1..5; 0 = the occupancy limit */
+} dl_tuning;
+int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t);
+int dl_renderer_get_tuning(dl_renderer* r, dl_tuning* t);
+/* Autotuner: renders the n views of s (flags as dl_render_batch, outputs kept
+ * on the device) under candidate tunings — coordinate descent over the three
+ * knobs from the current tuning — timing each as the median of `reps` frames
+ * (CUDA events on the renderer's stream, after one warm-up frame), keeps the
+ * fastest on the renderer and returns it with its frame time in ms. */
+int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
+                         uint32_t flags, int reps, dl_tuning* best, double* best_ms);
 
 /* ---- learned schedule (no reference counterpart: the reference rasterizes
  * tiles in dispatch order, src/render/pipeline.ts:402-422).  A small MLP
