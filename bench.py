@@ -45,6 +45,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-tune", action="store_true", help="skip the autotuner (default knobs)")
     p.add_argument("--views", type=int, default=64)
     p.add_argument("--splats", type=int, default=3_000_000)
     p.add_argument("--no-e2e", action="store_true")
@@ -286,6 +287,9 @@ def run_ours(args, rank, world, local_rank):
             ms = float(t.item())
         return ms
 
+    # autotuner (untimed): pair-sort digit width, raster work-item shape, CTAs/SM
+    tuning = None if args.no_tune else r.autotune(scene, cams, flags=FAST, reps=2)
+
     from droplet_b200 import learned
     model = learned.load_default(dev)          # the trained tile-cost model orders the rasterizer's queue
     static_value = None
@@ -374,7 +378,7 @@ def run_ours(args, rank, world, local_rank):
                                           "parallelism": f"views sharded: {world} rank(s) x {len(cams)} distinct "
                                                          f"views, scene replicated"}),
             "plain_value": plain_value, "exact_value": exact_value, "static_value": static_value,
-            "learned": (model.meta if model is not None else None),
+            "learned": (model.meta if model is not None else None), "tuning": tuning,
             "vs_plain": (value / plain_value) if plain_value else None,
             "stage_ms": stages, "pairs_per_step": npairs, "gpu_launches": launches, "clocks": clocks,
             "roofline": roof, "e2e": e2e}

@@ -3,10 +3,11 @@ droplet scenes, behind droplet's public API (src/index.ts:16-38)."""
 from .types import (BackgroundRGBA, Bounds, RenderCamera, SplatData, mat4Identity, mat4LookAt,
                     numSHCoeffsPerChannel, quatRotate, splatInputStride, vec3)
 from ._lib import DropletError
+from .ply import loadPlySplats, splatBounds
 from .api import (BlockMaskBuffer, Device, GpuRadixSorter, Mlp, Renderer, Scene, VoxelBlock, VoxelizeResult,
                   createDevice, mortonDecode3, mortonEncode3, voxelize)
 
 __all__ = ["BackgroundRGBA", "Bounds", "RenderCamera", "SplatData", "mat4Identity", "mat4LookAt",
            "numSHCoeffsPerChannel", "quatRotate", "splatInputStride", "vec3", "DropletError",
            "BlockMaskBuffer", "Device", "GpuRadixSorter", "Mlp", "Renderer", "Scene", "VoxelBlock", "VoxelizeResult", "createDevice",
-           "mortonDecode3", "mortonEncode3", "voxelize"]
+           "mortonDecode3", "mortonEncode3", "voxelize", "loadPlySplats", "splatBounds"]
