@@ -666,6 +666,27 @@ __device__ __forceinline__ float raster_exp(float p) {
     return y;
 }
 
+// Half-extents of the box outside which every pixel of a splat has alpha = 0.
+// The rasterizer's quadratic form q(d) = A dx^2 + 2B dx dy + C dy^2 (power =
+// -q/2) exceeds 9 outside the axis-aligned box of the ellipse q <= 9, whose
+// half-extents are sqrt(9 C / det), sqrt(9 A / det) with det = A C - B^2; and
+// q > 8.4 already gives opacity * (exp(-q/2) - exp(-4.5)) < 1/255, the skip of
+// rasterize.ts:74.  With A C <= 1024 det the f32 evaluation of q and of the
+// box is accurate to well under that margin (9.01 adds 0.05% to the extents),
+// so skipping pixels outside the box changes no result.  Worse-conditioned
+// conics keep the square box of the radius.
+__device__ __forceinline__ void tight_extent(float A, float B, float C, float r, float& ex, float& ey) {
+    ex = r;
+    ey = r;
+    const float ac = A * C;
+    const float det = ac - B * B;
+    if (det > 0.0f && ac <= 1024.0f * det) {
+        const float s = 9.01f / det;
+        ex = fminf(r, sqrtf(C * s));
+        ey = fminf(r, sqrtf(A * s));
+    }
+}
+
 __device__ __forceinline__ uint32_t view_of_tile(const RasterArgs& a, uint32_t gt) {
     uint32_t lo = 0, hi = a.num_views;        // last view with tile_base <= gt
     while (hi - lo > 1) {
@@ -677,7 +698,7 @@ __device__ __forceinline__ uint32_t view_of_tile(const RasterArgs& a, uint32_t g
 
 template <bool kExactExp>
 __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, uint32_t tile, uint32_t sub,
-                                               uint32_t gt, float4* s_a, float4* s_b, float2* s_c) {
+                                               uint32_t gt, float4* s_a, float4* s_b, float4* s_c) {
     const DlView& u = a.views[v];
     const int lane = threadIdx.x & 31;
     const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
@@ -717,56 +738,66 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
             const float r = ra1.z;
             hit1 = r > 0.0f && !(ra1.x - r > rx1) && !(ra1.x + r < rx0) && !(ra1.y - r > ry1) && !(ra1.y + r < ry0);
         }
-        const uint32_t m0 = __ballot_sync(0xffffffffu, hit0);
-        const uint32_t m1 = __ballot_sync(0xffffffffu, hit1);
-        if ((m0 | m1) == 0u) continue;
+        if (__ballot_sync(0xffffffffu, hit0 || hit1) == 0u) continue;
+        // square-box hits load their record; the ellipse's box then decides
+        // (with eval counting on, the square box alone: the reference's count)
+        uint32_t n = 0;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const bool hit = h ? hit1 : hit0;
-            if (!hit) continue;
+            bool hit = h ? hit1 : hit0;
             const uint32_t g = h ? g1 : g0;
             const float4 ra = h ? ra1 : ra0;
-            const uint32_t slot = h ? __popc(m0) + __popc(m1 & lmask) : __popc(m0 & lmask);
-            float A, B, C, al, cr, cg, cb;
-            if (a.recBC) {
-                const float4 p = __ldg(a.recBC + 2 * (vo + g));
-                const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
-                A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
-            } else {
-                const uint4 hv = __ldg(a.recH + vo + g);
-                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
-                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
-                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
-                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
-                A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+            float A = 0.0f, B = 0.0f, C = 0.0f, al = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+            float ex = ra.z, ey = ra.z;
+            if (hit) {
+                if (a.recBC) {
+                    const float4 p = __ldg(a.recBC + 2 * (vo + g));
+                    const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
+                    A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
+                } else {
+                    const uint4 hv = __ldg(a.recH + vo + g);
+                    const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
+                    const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
+                    const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
+                    const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
+                    A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+                }
+                if (!a.eval_count) {
+                    tight_extent(A, B, C, ra.z, ex, ey);
+                    hit = !(ra.x - ex > rx1) && !(ra.x + ex < rx0) && !(ra.y - ey > ry1) && !(ra.y + ey < ry0);
+                }
             }
-            if (kExactExp) {
-                s_a[slot] = make_float4(ra.x, ra.y, ra.z, A);
-                s_b[slot] = make_float4(2.0f * B, C, al, cr);
-            } else {
-                // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
-                s_a[slot] = make_float4(ra.x, ra.y, ra.z, -0.72134752044448170f * A);
-                s_b[slot] = make_float4(-1.4426950408889634f * B, -0.72134752044448170f * C, al, cr);
+            const uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const uint32_t slot = n + __popc(m & lmask);
+                s_a[slot] = make_float4(ra.x, ra.y, ex, ey);
+                if (kExactExp) {
+                    s_b[slot] = make_float4(2.0f * B, C, al, cr);
+                    s_c[slot] = make_float4(cg, cb, A, 0.0f);
+                } else {
+                    // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
+                    s_b[slot] = make_float4(-1.4426950408889634f * B, -0.72134752044448170f * C, al, cr);
+                    s_c[slot] = make_float4(cg, cb, -0.72134752044448170f * A, 0.0f);
+                }
             }
-            s_c[slot] = make_float2(cg, cb);
+            n += __popc(m);
         }
         __syncwarp();
-        const uint32_t n = __popc(m0) + __popc(m1);
         if (!done && kExactExp) {
             for (uint32_t j = 0; j < n; j++) {
                 const float4 sa = s_a[j];
                 const float dx = px - sa.x;
                 const float dy = py - sa.y;
-                if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
+                if (fabsf(dx) > sa.z || fabsf(dy) > sa.w) continue;
                 const float4 sb = s_b[j];
+                const float4 sc = s_c[j];
                 evals++;
-                const float power = -0.5f * ((((sa.w * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
+                const float power = -0.5f * ((((sc.z * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
                 if (power > 0.0f || power <= DL_POWER_CUT) continue;
                 const float alpha =
                     fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
                 if (alpha < DL_MIN_ALPHA) continue;
                 const float w = T * alpha;
-                const float2 sc = s_c[j];
                 c0 = c0 + w * sb.w;
                 c1 = c1 + w * sc.x;
                 c2 = c2 + w * sc.y;
@@ -780,17 +811,17 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float4 sa = s_a[j];
                 const float dx = px - sa.x;
                 const float dy = py - sa.y;
-                if (fabsf(dx) > sa.z || fabsf(dy) > sa.z) continue;
+                if (fabsf(dx) > sa.z || fabsf(dy) > sa.w) continue;
                 const float4 sb = s_b[j];
+                const float4 sc = s_c[j];
                 evals++;
-                const float p2 = __fmaf_rn(dx, __fmaf_rn(sa.w, dx, sb.x * dy), sb.y * dy * dy);
+                const float p2 = __fmaf_rn(dx, __fmaf_rn(sc.z, dx, sb.x * dy), sb.y * dy * dy);
                 if (p2 > 0.0f || p2 <= -6.4921275f) continue;          // -4.5 * log2(e)
                 float e;
                 asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
                 const float alpha = fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, e - DL_GAUSS_FLOOR));
                 if (alpha < DL_MIN_ALPHA) continue;
                 const float w = T * alpha;
-                const float2 sc = s_c[j];
                 c0 = __fmaf_rn(w, sb.w, c0);
                 c1 = __fmaf_rn(w, sc.x, c1);
                 c2 = __fmaf_rn(w, sc.y, c2);
@@ -828,7 +859,7 @@ template <bool kExactExp>
 __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_k(RasterArgs a) {
     __shared__ float4 s_a[kRasterWarps][64];
     __shared__ float4 s_b[kRasterWarps][64];
-    __shared__ float2 s_c[kRasterWarps][64];
+    __shared__ float4 s_c[kRasterWarps][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     while (true) {
         uint32_t item = 0;
