@@ -61,7 +61,9 @@ struct DlSceneDev {
     const float* opl;      // N
     const float* dc;       // 3N
     const float* sh;       // 3MN (f32) or NULL
-    const uint16_t* sh16;  // 3MN (f16 / bf16 bits) or NULL
+    const uint16_t* sh16;  // f16 / bf16 bits, or NULL: per Gaussian a block of sh16_stride halves,
+                           // coefficient-major (entry 3k + c = coefficient k of channel c), zero-padded
+    uint32_t sh16_stride;  // round_up(3M, 8): 16-byte aligned blocks
     uint32_t n;
     int32_t bands;
     int32_t sh_kind;       // 0 f32, 1 f16, 2 bf16

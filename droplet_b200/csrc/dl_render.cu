@@ -58,9 +58,15 @@ void launch_pass_bits(int bits, const dlsort::Pass& p, uint32_t grid, cudaStream
     else launch_pass<6>(p, grid, st);
 }
 
-__global__ void sh_to_half_k(const float* in, uint16_t* out, uint64_t n, int kind) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const float f = in[i];
+// SH in 16 bits, repacked per Gaussian: in[g][c * M + k] (channel-major, as
+// SplatData) -> out[g][3 k + c], blocks of P = round_up(3M, 8) halves, zero pads.
+__global__ void sh_to_half_k(const float* in, uint16_t* out, uint64_t n, int M, int P, int kind) {
+    const uint64_t total = n * (uint64_t)P;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t g = i / P;
+        const int j = (int)(i - g * P);
+        float f = 0.0f;
+        if (j < 3 * M) f = in[g * 3 * M + (uint64_t)((j % 3) * M + j / 3)];
         out[i] = kind == 1 ? __half_as_ushort(__float2half_rn(f)) : __bfloat16_as_ushort(__float2bfloat16_rn(f));
     }
 }
@@ -121,7 +127,8 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
     const uint64_t oPos = 0, oRot = round_up(oPos + 12 * n, a), oLsc = round_up(oRot + 16 * n, a);
     const uint64_t oOpl = round_up(oLsc + 12 * n, a), oDc = round_up(oOpl + 4 * n, a);
     const uint64_t oSh = round_up(oDc + 12 * n, a);
-    const uint64_t shBytes = (uint64_t)3 * M * n * (precision == DL_PREC_F32 ? 4 : 2);
+    const uint32_t P16 = (uint32_t)round_up((uint64_t)3 * M, 8);
+    const uint64_t shBytes = precision == DL_PREC_F32 ? (uint64_t)3 * M * n * 4 : (uint64_t)P16 * n * 2;
     const uint64_t oTmp = round_up(oSh + shBytes, a);
     const uint64_t total = (precision == DL_PREC_F32 || M == 0) ? oTmp : oTmp + (uint64_t)3 * M * n * 4;
     DL_TRY(s->mem.ensure(total));
@@ -137,7 +144,7 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
                 DL_CK(cudaMemcpyAsync(b + oSh, d->colors_sh, shBytes, cudaMemcpyHostToDevice, st));
             } else {
                 DL_CK(cudaMemcpyAsync(b + oTmp, d->colors_sh, (uint64_t)3 * M * n * 4, cudaMemcpyHostToDevice, st));
-                sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp), (uint16_t*)(b + oSh), (uint64_t)3 * M * n,
+                sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp), (uint16_t*)(b + oSh), n, M, (int)P16,
                                                    precision);
                 DL_CK(cudaGetLastError());
             }
@@ -151,6 +158,7 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
     s->d.dc = (const float*)(b + oDc);
     s->d.sh = (M && precision == DL_PREC_F32) ? (const float*)(b + oSh) : nullptr;
     s->d.sh16 = (M && precision != DL_PREC_F32) ? (const uint16_t*)(b + oSh) : nullptr;
+    s->d.sh16_stride = (M && precision != DL_PREC_F32) ? P16 : 0;
     s->d.n = (uint32_t)n;
     s->d.bands = bands;
     s->d.sh_kind = M ? precision : 0;
@@ -855,7 +863,7 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
 
     DlSceneDev sc{};
     sc.pos = dPos; sc.rot = dRot; sc.lsc = dLsc; sc.opl = dOpl; sc.dc = dDc;
-    sc.sh = M ? dSh : nullptr; sc.sh16 = nullptr; sc.n = N; sc.bands = bands; sc.sh_kind = 0;
+    sc.sh = M ? dSh : nullptr; sc.sh16 = nullptr; sc.sh16_stride = 0; sc.n = N; sc.bands = bands; sc.sh_kind = 0;
 
     uint64_t launches = 0;
     uint32_t* finalVals = nullptr;

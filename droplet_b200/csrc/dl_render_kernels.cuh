@@ -74,10 +74,7 @@ __device__ __forceinline__ Cov3 make_cov3(const float rot[4], const float s[3]) 
 }
 
 __device__ __forceinline__ float sh_coef(const DlSceneDev& sc, uint64_t i) {
-    if (sc.sh_kind == 0) return __ldg(sc.sh + i);
-    const uint16_t b = __ldg(sc.sh16 + i);
-    if (sc.sh_kind == 1) return __half2float(__ushort_as_half(b));
-    return __bfloat162float(__ushort_as_bfloat16(b));
+    return __ldg(sc.sh + i);
 }
 
 // project.ts:264-331 evalSH (channel-major coefficients, camera-space direction)
@@ -122,13 +119,77 @@ __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int
     }
 }
 
+// evalSH on the 16-bit SH block of one Gaussian (same basis, same summation
+// order as eval_sh): the block is read with 128-bit loads.
+template <int BANDS>
+__device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, float x, float y, float z,
+                                          float& r, float& gr, float& b) {
+    constexpr int M = BANDS == 1 ? 3 : BANDS == 2 ? 8 : 15;
+    constexpr int CH = (3 * M + 7) / 8;
+    const uint4* blk = reinterpret_cast<const uint4*>(sc.sh16 + (uint64_t)g * sc.sh16_stride);
+    uint32_t w[CH * 4];
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+        const uint4 q = __ldg(blk + c);
+        w[4 * c] = q.x; w[4 * c + 1] = q.y; w[4 * c + 2] = q.z; w[4 * c + 3] = q.w;
+    }
+    const bool isHalf = sc.sh_kind == 1;
+    auto coef = [&](int k, int ch) -> float {
+        const int e = 3 * k + ch;
+        const uint16_t bits = (uint16_t)(w[e >> 1] >> ((e & 1) * 16));
+        return isHalf ? __half2float(__ushort_as_half(bits)) : __bfloat162float(__ushort_as_bfloat16(bits));
+    };
+    const float SH1 = 0.4886025119029199f, nSH1 = -0.4886025119029199f;
+    const float b1[3] = {nSH1 * y, SH1 * z, nSH1 * x};
+    r = 0.0f; gr = 0.0f; b = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r = r + b1[k] * coef(k, 0);
+        gr = gr + b1[k] * coef(k, 1);
+        b = b + b1[k] * coef(k, 2);
+    }
+    if (BANDS >= 2) {
+        const float xx = x * x, yy = y * y, zz = z * z;
+        const float xy = x * y, yz = y * z, xz = x * z;
+        const float b2[5] = {1.0925484305920792f * xy, -1.0925484305920792f * yz,
+                             0.31539156525252005f * (((2.0f * zz) - xx) - yy), -1.0925484305920792f * xz,
+                             0.5462742152960396f * (xx - yy)};
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            r = r + b2[k] * coef(3 + k, 0);
+            gr = gr + b2[k] * coef(3 + k, 1);
+            b = b + b2[k] * coef(3 + k, 2);
+        }
+        if (BANDS >= 3) {
+            const float b3[7] = {(-0.5900435899266435f * y) * ((3.0f * xx) - yy),
+                                 (2.890611442640554f * xy) * z,
+                                 (-0.4570457994644658f * y) * (((4.0f * zz) - xx) - yy),
+                                 (0.3731763325901154f * z) * (((2.0f * zz) - (3.0f * xx)) - (3.0f * yy)),
+                                 (-0.4570457994644658f * x) * (((4.0f * zz) - xx) - yy),
+                                 (1.445305721320277f * z) * (xx - yy),
+                                 (-0.5900435899266435f * x) * (xx - (3.0f * yy))};
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                r = r + b3[k] * coef(8 + k, 0);
+                gr = gr + b3[k] * coef(8 + k, 1);
+                b = b + b3[k] * coef(8 + k, 2);
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
     const __half2 h = __floats2half2_rn(a, b);
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
 // One splat, all views.  Thread per splat, index order (coalesced SoA reads).
-__global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
+constexpr int kProjectMaxViews = 4096;          // views per frame (per-CTA visible counters)
+
+__global__ void __launch_bounds__(256, 4) project_k(ProjectArgs a) {
+    __shared__ uint32_t s_vis[kProjectMaxViews];
+    for (uint32_t v = threadIdx.x; v < a.num_views; v += blockDim.x) s_vis[v] = 0;
+    __syncthreads();
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     const bool inRange = g < a.sc.n;
     float pos[3] = {0, 0, 0}, rot[4] = {1, 0, 0, 0}, s[3] = {1, 1, 1}, dc[3] = {0, 0, 0}, opl = 0.0f;
@@ -172,7 +233,7 @@ __global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
             a.keys[o] = visible ? dl_sortable_key(depthKey) : 0xffffffffu;
         }
         const uint32_t ballot = __ballot_sync(0xffffffffu, visible);
-        if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&a.nvis[v], (uint32_t)__popc(ballot));
+        if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&s_vis[v], (uint32_t)__popc(ballot));
         if (!visible) continue;
 
         // ---- project.ts:79-84
@@ -272,7 +333,14 @@ __global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
         if (a.sc.bands > 0) {
             const float len = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
             float sr, sg, sb;
-            eval_sh(a.sc, shBase, M, pcx / len, pcy / len, pcz / len, sr, sg, sb);
+            const float dxn = pcx / len, dyn = pcy / len, dzn = pcz / len;
+            if (a.sc.sh16) {
+                if (a.sc.bands == 1) eval_sh16<1>(a.sc, g, dxn, dyn, dzn, sr, sg, sb);
+                else if (a.sc.bands == 2) eval_sh16<2>(a.sc, g, dxn, dyn, dzn, sr, sg, sb);
+                else eval_sh16<3>(a.sc, g, dxn, dyn, dzn, sr, sg, sb);
+            } else {
+                eval_sh(a.sc, shBase, M, dxn, dyn, dzn, sr, sg, sb);
+            }
             col0 = col0 + sr; col1 = col1 + sg; col2 = col2 + sb;
         }
         col0 = fmaxf(col0 + 0.5f, 0.0f);
@@ -302,6 +370,9 @@ __global__ void __launch_bounds__(256) project_k(ProjectArgs a) {
         else
             a.bbox[o] = make_uint2(0xffffu, 0u);
     }
+    __syncthreads();
+    for (uint32_t v = threadIdx.x; v < a.num_views; v += blockDim.x)
+        if (s_vis[v]) atomicAdd(&a.nvis[v], s_vis[v]);
 }
 
 // ------------------------------------------------------------------ emit
