@@ -78,6 +78,9 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
                       &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->evalCount, &r->own_scene.mem, &r->feat, &r->pred,
                       &r->skeys0, &r->skeys1, &r->svals0, &r->svals1, &r->sseg, &r->sstatus, &r->shist, &r->tileCycles};
     for (DevBuf* b : bufs) b->release();
+    r->tuneOut.release();
+    if (r->copy_stream) { cudaStreamSynchronize(r->copy_stream); cudaStreamDestroy(r->copy_stream); }
+    if (r->copy_event) cudaEventDestroy(r->copy_event);
     if (r->h_views) cudaFreeHost(r->h_views);
     if (r->h_u64) cudaFreeHost(r->h_u64);
     for (auto& e : r->ev) if (e) cudaEventDestroy(e);
@@ -174,7 +177,8 @@ extern "C" int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_ca
                               uint8_t* const* outs, uint32_t flags) {
     if (!r || !data) { dl_set_error("dl_render_many: NULL argument"); return DL_E_INVALID_ARG; }
     DL_CK(cudaSetDevice(r->dev->ordinal));
-    DL_TRY(dl_upload_scene(&r->own_scene, data, DL_PREC_F32, r->stream));
+    const int prec = ((flags & DL_BATCH_SH16) && !(flags & DL_BATCH_PLAIN)) ? DL_PREC_F16 : DL_PREC_F32;
+    DL_TRY(dl_upload_scene(&r->own_scene, data, prec, r->stream));
     return dl_render_batch(r, &r->own_scene, cams, n, bg, outs, flags & ~(uint32_t)DL_BATCH_OUT_DEVICE);
 }
 
@@ -207,6 +211,25 @@ extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cam
             DL_TRY(dl_render_views(r, s->d, &views[i], 1, &dOuts[i], flags & ~DL_BATCH_F16_RECORDS));
             launches += r->launches;
         }
+    } else if (!outDev && n >= 8) {
+        // host outputs: render in four view groups; each group is copied back on
+        // a second stream while the next one renders
+        if (!r->copy_stream) DL_CK(cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking));
+        if (!r->copy_event) DL_CK(cudaEventCreateWithFlags(&r->copy_event, cudaEventDisableTiming));
+        const int per = (n + 3) / 4;
+        for (int g0 = 0; g0 < n; g0 += per) {
+            const int cnt = std::min(per, n - g0);
+            DL_TRY(dl_render_views(r, s->d, &views[g0], (uint32_t)cnt, &dOuts[g0], flags | DL_BATCH_NO_GRAPH));
+            launches += r->launches;
+            DL_CK(cudaEventRecord(r->copy_event, r->stream));
+            DL_CK(cudaStreamWaitEvent(r->copy_stream, r->copy_event, 0));
+            for (int i = g0; i < g0 + cnt; i++)
+                DL_CK(cudaMemcpyAsync(outs[i], dOuts[i], (uint64_t)views[i].W * views[i].H * 4, cudaMemcpyDeviceToHost,
+                                      r->copy_stream));
+        }
+        DL_CK(cudaStreamSynchronize(r->copy_stream));
+        r->launches = launches;
+        return DL_OK;
     } else {
         DL_TRY(dl_render_views(r, s->d, views.data(), (uint32_t)n, dOuts.data(), flags));
         launches = r->launches;

@@ -121,6 +121,10 @@ struct dl_renderer {
 
     DlTuning tune;                      // dl_renderer_set_tuning / dl_renderer_autotune
     DevBuf tuneOut;                     // autotuner's device images
+
+    // read-back of host-output batches, overlapped with rendering
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_event = nullptr;
 };
 
 struct dl_mlp;

@@ -127,8 +127,9 @@ enum {
     DL_BATCH_FAST_EXP = 32,       /* hardware ex2 in the rasterizer (+-1 LSB) */
     DL_BATCH_COUNT_EVALS = 64,    /* count evaluated (pixel, splat) pairs ("evals") */
     DL_BATCH_LOG_TILES = 128,     /* keep per-tile features and measured cost (dl_renderer_tile_log) */
-    DL_BATCH_F64_DEGENERATE = 256 /* f64 determinant and inverse for near-degenerate 2D covariances
+    DL_BATCH_F64_DEGENERATE = 256,/* f64 determinant and inverse for near-degenerate 2D covariances
                                      (det < 2^-10 c00 c11); culling and tile ranges unchanged */
+    DL_BATCH_SH16 = 512           /* dl_render_many: keep the uploaded SH coefficients in f16 */
 };
 /* Render n views of one resident scene; outs[i] receives cams[i].width *
  * cams[i].height RGBA8 pixels (host or device memory, per flags). */
@@ -138,7 +139,9 @@ int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, c
 /* Renderer.render(data, camera, bg) (src/render/pipeline.ts:181-426) for n
  * cameras of one host SplatData in one call: the splats are uploaded into the
  * renderer's own grow-only scene buffer, all views are rendered as one batch,
- * and each RGBA8 image is copied to outs[i] (host memory). */
+ * and each RGBA8 image is copied to outs[i] (host memory).  With host outputs
+ * and 8 or more views, dl_render_batch renders the views in four groups and
+ * copies each group back on a second stream while the next one renders. */
 int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
                    uint8_t* const* outs, uint32_t flags);
 

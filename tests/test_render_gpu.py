@@ -234,3 +234,22 @@ def renderer_single(device, d, cam):
         return r.render(d, cam)
     finally:
         r.destroy()
+
+
+def test_render_many_groups_and_sh16_match_the_batch(device):
+    # host outputs of 8+ views are rendered in groups with overlapped read-back;
+    # DL_BATCH_SH16 keeps the uploaded SH in f16 like a Scene uploaded as "f16"
+    d = synth.cluster_scene(120_000, seed=17, clusters=24, extent=10.0, bands=3)
+    cams = synth.ring_cameras(10, resolutions=[(320, 180), (200, 120), (640, 360)])
+    r2 = dl.Renderer(device)
+    sc32, sc16 = r2.upload(d), r2.upload(d, "f16")
+    # references: batches of fewer than 8 views take the ungrouped path
+    ref32 = r2.render_batch(sc32, cams[:5]) + r2.render_batch(sc32, cams[5:])
+    got32 = r2.render_many(d, cams)
+    for a, b in zip(ref32, got32):
+        assert np.array_equal(a, b)
+    fl = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
+    ref16 = r2.render_batch(sc16, cams[:5], flags=fl) + r2.render_batch(sc16, cams[5:], flags=fl)
+    got16 = r2.render_many(d, cams, flags=fl | _lib.DL_BATCH_SH16)
+    for a, b in zip(ref16, got16):
+        assert np.array_equal(a, b)
