@@ -51,26 +51,49 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-plain", action="store_true")
-    p.add_argument("--workload", default="ring64", choices=["ring64", "voxel1m", "zipf10m"],
-                   help="ring64: the headline render batch; voxel1m / zipf10m: voxelize lines")
+    p.add_argument("--workload", default="ring64",
+                   choices=["ring64", "plain100k", "sh3-1080p", "sh3-equirect", "zipf10m-16v", "voxel1m", "zipf10m"],
+                   help="ring64: the headline render batch; plain100k / sh3-1080p / sh3-equirect / zipf10m-16v: "
+                        "the other render configurations; voxel1m / zipf10m: voxelize lines")
     return p.parse_args()
 
 
+RENDER = {
+    "plain100k": "100k Gaussians U[-1,1]^3, SH0, one 1280x720 pinhole view from (0,0,4)",
+    "sh3-1080p": "3M-Gaussian SH3 scene (256 clusters in [-10,10]^3), one 1920x1080 pinhole view from (0,2,12)",
+    "sh3-equirect": "3M-Gaussian SH3 scene, one 2048x1024 equirect view from the origin",
+    "zipf10m-16v": "10M Gaussians, 1024 Zipf(1.2) clusters in [-20,20]^3, SH1, 16 ring views 1920x1080",
+}
+
+
 def workload(args, rank=0, world=1):
-    """The scene and this rank's ring: rank r of N renders the ring turned by
-    r/N of a view step, so N ranks render 64 N distinct views (weak scaling)."""
+    """The scene and this rank's cameras.  ring64: rank r of N renders the ring
+    turned by r/N of a view step, so N ranks render 64 N distinct views (weak
+    scaling); the single-scene configurations give every rank the same views."""
     from droplet_b200 import synth
+    if args.workload == "plain100k":
+        return synth.plain_100k(), [synth.plain_100k_camera()]
+    if args.workload in ("sh3-1080p", "sh3-equirect"):
+        return synth.sh3_3m(args.splats), [synth.sh3_3m_cameras()[0 if args.workload == "sh3-1080p" else 1]]
+    if args.workload == "zipf10m-16v":
+        return synth.zipf_10m(), synth.zipf_10m_cameras(16)
     data = synth.sh3_3m(args.splats)
     cams = synth.ring_cameras(args.views, phase=rank / max(world, 1))
     return data, cams
 
 
-def config(args, cams, extra=None):
+def config(args, cams, extra=None, data=None):
     pix = sum(c.width * c.height for c in cams)
-    c = {"workload": f"ring{len(cams)}: {len(cams)} views cycling 640x360/1280x720/1920x1080/2560x1440 "
-                     f"({pix / 1e6:.1f} Mpix) of a {args.splats / 1e6:g}M-Gaussian SH3 scene",
-         "splats": args.splats, "views": len(cams), "pixels_per_step": pix, "sh_bands": 3, "tile": "16x16",
-         "l2": "inputs larger than L2 (scene 708 MB, per-view intermediates > 1 GB)"}
+    if args.workload in RENDER:
+        c = {"workload": f"{args.workload}: {RENDER[args.workload]} ({pix / 1e6:.2f} Mpix)",
+             "splats": data.count if data is not None else None, "views": len(cams), "pixels_per_step": pix,
+             "sh_bands": data.shBands if data is not None else None, "tile": "16x16",
+             "l2": "L2 flushed between timed steps" if args.workload == "plain100k" else "inputs larger than L2"}
+    else:
+        c = {"workload": f"ring{len(cams)}: {len(cams)} views cycling 640x360/1280x720/1920x1080/2560x1440 "
+                         f"({pix / 1e6:.1f} Mpix) of a {args.splats / 1e6:g}M-Gaussian SH3 scene",
+             "splats": args.splats, "views": len(cams), "pixels_per_step": pix, "sh_bands": 3, "tile": "16x16",
+             "l2": "inputs larger than L2 (scene 708 MB, per-view intermediates > 1 GB)"}
     if extra:
         c.update(extra)
     return c
@@ -146,14 +169,14 @@ def profile_traffic():
 def cpu_baseline(data, cams):
     """Bounded sample on the host cores: the oracle renders the 1920x1080 view."""
     from oracle import oracle as O
-    cam = next(c for c in cams if c.width == 1920)
+    cam = next((c for c in cams if c.width == 1920), cams[0])
     t = time.perf_counter()
     O.render(data, cam)
     dt = time.perf_counter() - t
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": cam.width * cam.height / dt / 1e6, "unit": "Mpix/s", "cores": cores, "kind": "port",
             "sample": f"oracle (C++ restatement, OpenMP) renders 1 view {cam.width}x{cam.height} of the "
-                      f"{data.count}-Gaussian SH3 scene in {dt:.2f} s"}
+                      f"{data.count}-Gaussian SH{data.shBands} scene in {dt:.2f} s"}
 
 
 def run_reference(args, rank, world):
@@ -270,17 +293,31 @@ def run_ours(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
+    # inputs that fit in L2 (126 MB): a 256 MB buffer is rewritten before every timed step
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if args.workload == "plain100k" else None
+
     def timed(fn, steps):
         barrier()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
+        if flush is None:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+        else:
+            ms = 0.0
+            for _ in range(steps):
+                flush.fill_(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
         barrier()
-        ms = e0.elapsed_time(e1)
         if world > 1:
             t = torch.tensor([ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -333,6 +370,8 @@ def run_ours(args, rank, world, local_rank):
         # host SplatData in pinned memory, images back into pinned memory, every step
         keep, fields = [], {}
         for k in ("positions", "rotations", "logScales", "opacityLogits", "colorsDC", "colorsSH"):
+            if getattr(data, k) is None:
+                continue
             t = torch.from_numpy(np.ascontiguousarray(getattr(data, k))).pin_memory()
             keep.append(t)
             fields[k] = t.numpy()
@@ -373,11 +412,12 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
-            "config": config(args, cams, {"mode": "batched: one CUDA-graph replay per step for all views, f16 scene "
-                                                  "SH and records, hardware exp2 (+-1 LSB), tiles rasterized in "
-                                                  "decreasing cost predicted by the learned model",
+            "config": config(args, cams, {"mode": "batched: one launch sequence for all views (a CUDA-graph "
+                                                  "replay when there are several), f16 scene SH and records, "
+                                                  "hardware exp2 (+-1 LSB), tiles rasterized in decreasing cost "
+                                                  "predicted by the learned model",
                                           "parallelism": f"views sharded: {world} rank(s) x {len(cams)} distinct "
-                                                         f"views, scene replicated"}),
+                                                         f"views, scene replicated"}, data),
             "plain_value": plain_value, "exact_value": exact_value, "static_value": static_value,
             "learned": (model.meta if model is not None else None), "tuning": tuning,
             "vs_plain": (value / plain_value) if plain_value else None,
@@ -396,7 +436,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload != "ring64":
+    if args.workload in VOXEL:
         run_voxel(args, rank, world, local_rank)
         return
     if world > 1:

@@ -1,6 +1,7 @@
 """The learned tile-cost model: its hand-written GPU kernels against a float64
 NumPy restatement, and the guarantee that the schedule it produces changes no
-pixel.  The gain it brings is measured in bench.py (value vs static_value)."""
+pixel.  Its gain is judged against measured tile costs (list-scheduling makespan)
+and timed in bench.py (value vs static_value)."""
 import numpy as np
 import pytest
 
@@ -100,3 +101,46 @@ def test_tile_log_covers_every_tile(device):
     # feature 0 is log1p(pairs in the tile) / 10: recover the per-tile counts
     off = r.debug_get("tile_off", np.uint32)
     assert np.allclose(np.expm1(f[:, 0] * 10), np.diff(off.astype(np.int64)), rtol=1e-3, atol=1e-2)
+
+
+def _makespan(costs, order, workers):
+    """Greedy list scheduling: each job in `order` goes to the earliest-free worker."""
+    import heapq
+    free = [0.0] * workers
+    heapq.heapify(free)
+    for j in order:
+        heapq.heappush(free, heapq.heappop(free) + float(costs[j]))
+    return max(free)
+
+
+def test_learned_order_against_measured_tile_costs(device):
+    # What the trained network buys, judged by measured cost: on a held-out
+    # scene, the per-tile costs the rasterizer logs are list-scheduled onto
+    # the persistent CTAs in natural order, in predicted-cost order and in the
+    # ideal (measured) order.  The prediction must rank tiles well, and its
+    # order must not schedule worse than the natural one.
+    model = learned.load_default(device)
+    if model is None:
+        pytest.skip("no trained model file")
+    d = synth.cluster_scene(1_000_000, seed=21, clusters=256, extent=10.0, bands=3)
+    r = dl.Renderer(device)
+    sc = r.upload(d)
+    lines = []
+    for w, h in ((640, 360), (1920, 1080)):
+        cam = synth.pinhole(w, h, (0.0, 2.0, 12.0))
+        r.render_batch(sc, [cam], flags=_lib.DL_BATCH_PLAIN | _lib.DL_BATCH_LOG_TILES)
+        f, c = r.tile_log()
+        pred = model.predict(f)
+        rank = lambda a: np.argsort(np.argsort(a))
+        rho = float(np.corrcoef(rank(pred), rank(c))[0, 1])
+        workers = 148 * 5                              # persistent rasterizer CTAs
+        nat = _makespan(c, range(len(c)), workers)
+        lrn = _makespan(c, np.argsort(-pred, kind="stable"), workers)
+        ide = _makespan(c, np.argsort(-c, kind="stable"), workers)
+        lb = max(c.sum() / workers, c.max())
+        lines.append(f"{w}x{h}: {len(c)} tiles, Spearman {rho:.3f}; makespan natural {nat / lb:.3f}, "
+                     f"learned {lrn / lb:.3f}, ideal {ide / lb:.3f} (x lower bound)")
+        assert rho > 0.75
+        assert lrn <= nat * 1.001
+    r.destroy()
+    print("\n" + "\n".join(lines))
