@@ -229,6 +229,25 @@ def run_voxel(args, rank, world, local_rank):
     desc, res = VOXEL[args.workload]
     opts = {"voxelResolution": res, "opacityCutoff": 0.1}
     dev = dl.createDevice({"ordinal": local_rank})
+    from droplet_b200 import learned
+    model = learned.load_default_voxel(dev)         # block-cost model ordering the block queue
+
+    def run_steps(steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            dl.voxelize(dev, data, opts)            # synchronous: returns with the block list on the host
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    learned_ms = None
+    if model is not None:                          # the learned block order, timed beside the natural one
+        dev.set_voxel_scheduler(model)
+        dl.voxelize(dev, data, opts)
+        learned_ms = run_steps(max(1, args.steps // 2))
+        dev.set_voxel_scheduler(None)
     out = None
     for _ in range(args.warmup):
         out = dl.voxelize(dev, data, opts)
@@ -236,12 +255,7 @@ def run_voxel(args, rank, world, local_rank):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
-        e0.record()
-        for _ in range(args.steps):
-            dl.voxelize(dev, data, opts)        # synchronous: returns with the block list on the host
-        e1.record()
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+        ms = run_steps(args.steps)
     value = world * vox / (ms / 1e3) / 1e6
     line = {"metric": "Mvox/s (voxels of the block grid per second), voxelize", "value": value, "unit": "Mvox/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -250,6 +264,8 @@ def run_voxel(args, rank, world, local_rank):
                                                                                out.numBlocksZ],
                        "blocks_out": out.buffer.count, "solid_voxels": out.buffer.popcount()},
             "clocks": clk.summary(),
+            "learned_value": (world * vox / (learned_ms / 1e3) / 1e6) if learned_ms else None,
+            "learned": (model.meta if model is not None else None),
             "e2e": {"value": value, "unit": "Mvox/s", "h2d_bytes_per_step": int(data.count * 44),
                     "d2h_bytes_per_step": int(out.buffer.count * 12)}}
     if rank == 0 and world == 1 and not args.no_cpu:

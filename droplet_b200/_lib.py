@@ -39,6 +39,7 @@ EXPORTS = [
     "dl_mlp_predict", "dl_mlp_grad", "dl_mlp_train", "dl_renderer_set_scheduler", "dl_renderer_tile_log",
     "dl_sorter_create", "dl_sorter_destroy", "dl_sorter_set_stream", "dl_sorter_set_digit_bits", "dl_sorter_sort",
     "dl_renderer_set_tuning", "dl_renderer_get_tuning", "dl_renderer_autotune",
+    "dl_device_set_voxel_scheduler", "dl_vox_result_block_log",
 ]
 
 
@@ -70,7 +71,7 @@ class DlVoxOpts(ctypes.Structure):
     _fields_ = [("voxel_resolution", ctypes.c_double), ("opacity_cutoff", ctypes.c_double),
                 ("use_defaults", ctypes.c_int32), ("has_bounds", ctypes.c_int32),
                 ("bounds_min", ctypes.c_double * 3), ("bounds_max", ctypes.c_double * 3),
-                ("shard_index", ctypes.c_int32), ("shard_count", ctypes.c_int32)]
+                ("shard_index", ctypes.c_int32), ("shard_count", ctypes.c_int32), ("log_blocks", ctypes.c_int32)]
 
 
 _lib = None
@@ -126,6 +127,8 @@ def load():
         "dl_sorter_set_digit_bits": [vp, i],
         "dl_sorter_sort": [vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32, P(vp), P(vp)],
         "dl_renderer_set_tuning": [vp, P(DlTuning)],
+        "dl_device_set_voxel_scheduler": [vp, vp],
+        "dl_vox_result_block_log": [vp, vp, vp, ctypes.c_uint64, P(ctypes.c_uint64)],
         "dl_renderer_get_tuning": [vp, P(DlTuning)],
         "dl_renderer_autotune": [vp, vp, P(DlCamera), i, P(ctypes.c_float), ctypes.c_uint32, i, P(DlTuning),
                                  P(ctypes.c_double)],

@@ -69,6 +69,12 @@ class Device:
             raise DropletError(_lib.DL_E_INVALID_ARG, "device is closed")
         return self._h
 
+    def set_voxel_scheduler(self, mlp: Optional["Mlp"]):
+        """Attach (or with None detach) the block-cost model that orders voxelize's
+        block queue on this device; the order changes timing only."""
+        check(_lib.load().dl_device_set_voxel_scheduler(self.handle, mlp.handle if mlp is not None else None))
+        self._vox_sched = mlp
+
     def destroy(self):
         if self._h:
             _lib.load().dl_device_close(self._h)
@@ -345,6 +351,7 @@ class VoxelizeResult:
     numBlocksX: float
     numBlocksY: float
     numBlocksZ: float
+    blockLog: Optional[tuple] = None           # (features [n, 12], cost [n]) with opts["logBlocks"]
 
 
 def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> VoxelizeResult:
@@ -370,6 +377,7 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
     sh = opts.get("shard")
     if sh is not None:
         o.shard_index, o.shard_count = int(sh[0]), int(sh[1])
+    o.log_blocks = 1 if opts.get("logBlocks") else 0
     L = _lib.load()
     h = ctypes.c_void_p()
     check(L.dl_voxelize(device.handle, ctypes.byref(_splats(data)), ctypes.byref(o), ctypes.byref(h)))
@@ -385,10 +393,19 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
         hi = np.empty(n, np.uint32)
         if n:
             check(L.dl_vox_result_copy(h, idx.ctypes.data, lo.ctypes.data, hi.ctypes.data))
+        log = None
+        if o.log_blocks:
+            m = ctypes.c_uint64()
+            check(L.dl_vox_result_block_log(h, None, None, 0, ctypes.byref(m)))
+            f = np.empty((int(m.value), _lib.DL_MLP_IN), np.float32)
+            c = np.empty(int(m.value), np.float32)
+            if m.value:
+                check(L.dl_vox_result_block_log(h, f.ctypes.data, c.ctypes.data, m.value, ctypes.byref(m)))
+            log = (f, c)
     finally:
         L.dl_vox_result_free(h)
     return VoxelizeResult(BlockMaskBuffer(idx, lo, hi), Bounds(tuple(bmin), tuple(bmax)),
-                          o.voxel_resolution, dims[0], dims[1], dims[2])
+                          o.voxel_resolution, dims[0], dims[1], dims[2], log)
 
 
 # ---------------------------------------------------------------- learned tile-cost model

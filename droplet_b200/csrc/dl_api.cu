@@ -46,6 +46,8 @@ extern "C" int dl_device_open(int ordinal, dl_device** out) {
 extern "C" int dl_device_close(dl_device* d) {
     if (!d) return DL_OK;
     cudaSetDevice(d->ordinal);
+    if (d->stream) cudaStreamSynchronize(d->stream);
+    dl_vox_release(d);
     if (d->stream) cudaStreamDestroy(d->stream);
     delete d;
     return DL_OK;

@@ -48,11 +48,19 @@ struct DevBuf {
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+struct dl_mlp;
+struct VoxBufs;
+
 struct dl_device {
     int ordinal = 0;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
+    VoxBufs* vox = nullptr;             // the voxelizer's grow-only device buffers
+    dl_mlp* vox_sched = nullptr;        // block-cost model ordering the voxel work queue
 };
+
+// dl_voxel.cu: releases the voxelizer's buffers of a device
+void dl_vox_release(dl_device* dev);
 
 struct dl_scene {
     dl_device* dev = nullptr;

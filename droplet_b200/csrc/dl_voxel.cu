@@ -34,12 +34,16 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "dl_internal.h"
+#include "dl_mlp.cuh"
 #include "dl_sort.cuh"
 
 struct dl_vox_result {
     double bmin[3], bmax[3], dims[3];
     std::vector<uint32_t> idx, lo, hi;
+    std::vector<float> log_feat, log_cost;         // per evaluated block, with log_blocks
 };
 
 namespace {
@@ -427,6 +431,8 @@ struct EvalArgs {
     uint2* masks;
     uint32_t* counter;
     unsigned long long* evals;
+    const uint32_t* work;          // optional block order (learned); NULL: block order
+    uint32_t* cycles;              // optional [block] SM cycles / 16 spent on the block
 };
 
 __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, const VoxRec& g) {
@@ -448,7 +454,7 @@ __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, co
     return g.opacity * dl_expf(-0.5f * d2s);
 }
 
-__global__ void __launch_bounds__(64) vox_eval_k(EvalArgs a) {
+__global__ void __launch_bounds__(64, 24) vox_eval_k(EvalArgs a) {
     __shared__ VoxRec s_g[64];
     __shared__ uint32_t s_b;
     __shared__ uint32_t s_mask[2];
@@ -459,11 +465,15 @@ __global__ void __launch_bounds__(64) vox_eval_k(EvalArgs a) {
     const int64_t NX = a.p.NB[0], NY = a.p.NB[1], NBX = a.p.NBB[0], NBY = a.p.NBB[1];
     uint64_t evals = 0;
     while (true) {
-        if (tid == 0) s_b = atomicAdd(a.counter, 1u);
+        if (tid == 0) {
+            const uint32_t k = atomicAdd(a.counter, 1u);
+            s_b = (k < nb && a.work) ? a.work[k] : k;
+        }
         __syncthreads();
         const uint32_t b = s_b;
         __syncthreads();
         if (b >= nb) break;
+        const long long t0 = a.cycles ? clock64() : 0;
         const uint32_t key = a.bkey[b];
         const uint32_t batch = key >> 12, bi = key & 4095u;
         const int64_t bxI = batch % NBX, byI = (batch / NBX) % NBY, bzI = batch / (NBX * NBY);
@@ -497,11 +507,105 @@ __global__ void __launch_bounds__(64) vox_eval_k(EvalArgs a) {
         const uint32_t bal = __ballot_sync(0xffffffffu, solid);
         if ((tid & 31) == 0) s_mask[tid >> 5] = bal;
         __syncthreads();
-        if (tid == 0) a.masks[b] = make_uint2(s_mask[0], s_mask[1]);
+        if (tid == 0) {
+            a.masks[b] = make_uint2(s_mask[0], s_mask[1]);
+            if (a.cycles) a.cycles[b] = (uint32_t)((clock64() - t0) >> 4);
+        }
     }
     if (a.evals) {
         if (evals) atomicAdd(a.evals, (unsigned long long)evals);
     }
+}
+
+// ---- learned block order.  The 12 inputs of the block-cost model: the list
+// lengths of the block and its neighbours in list order, a sample of up to 8
+// of its Gaussians (mean and max opacity, mean and min extent in voxels: dense
+// opaque lists reach sigma >= 7 early), the block's place in its batch and
+// the cutoff.  vox_sched_pred_k: features, prediction, 8-bit bucket that
+// decreases with the predicted cost; vox_sched_scan_k: bucket offsets;
+// vox_sched_scatter_k: blocks into the work list.  Every block writes its own
+// mask, so any order gives the same result.
+struct VoxSchedArgs {
+    VoxParams p;
+    const VoxRec* rec;
+    const uint32_t* vals;
+    const uint32_t* bkey;
+    const uint32_t* bstart;
+    const uint32_t* nblocks;
+    const __nv_bfloat16* w;        // model parameters (NULL: features only)
+    float* feat;                   // optional [block][12]
+    uint32_t* bucket;              // [block]
+    uint32_t* hist;                // [256] (zeroed)
+    uint32_t* work;                // [block]
+};
+
+__device__ __forceinline__ void vox_block_features(const VoxSchedArgs& a, uint32_t b, uint32_t nb, float* x) {
+    const uint32_t s0 = a.bstart[b], s1 = a.bstart[b + 1];
+    const uint32_t L = s1 - s0;
+    const uint32_t Lp = b > 0 ? s0 - a.bstart[b - 1] : L;
+    const uint32_t Ln = b + 1 < nb ? a.bstart[b + 2] - s1 : L;
+    float om = 0.0f, ox = 0.0f, em = 0.0f, en = 1e30f;
+    const uint32_t k = L < 8u ? L : 8u;
+    const float inv = 1.0f / a.p.res;
+    for (uint32_t i = 0; i < k; i++) {
+        const VoxRec g = a.rec[a.vals[s0 + (uint32_t)(((uint64_t)i * L) / k)]];
+        om += g.opacity;
+        ox = fmaxf(ox, g.opacity);
+        const float e = log1pf(((g.ehx + g.ehy) + g.ehz) * (1.0f / 3.0f) * inv);
+        em += e;
+        en = fminf(en, e);
+    }
+    const float ik = k ? 1.0f / (float)k : 0.0f;
+    const uint32_t key = a.bkey[b];
+    const uint32_t batch = key >> 12, bi = key & 4095u;
+    const int64_t NBX = a.p.NBB[0], NBY = a.p.NBB[1];
+    const int64_t bxI = batch % NBX, byI = (batch / NBX) % NBY;
+    const int64_t cx = min((int64_t)16, a.p.NB[0] - bxI * 16), cy = min((int64_t)16, a.p.NB[1] - byI * 16);
+    x[0] = log1pf((float)L) * 0.1f;
+    x[1] = log1pf((float)Lp) * 0.1f;
+    x[2] = log1pf((float)Ln) * 0.1f;
+    x[3] = om * ik;
+    x[4] = ox;
+    x[5] = em * ik;
+    x[6] = k ? en : 0.0f;
+    x[7] = log1pf((float)L / 64.0f);
+    x[8] = (float)(bi % cx) * (1.0f / 16.0f);
+    x[9] = (float)((bi / cx) % cy) * (1.0f / 16.0f);
+    x[10] = (float)(bi / (cx * cy)) * (1.0f / 16.0f);
+    x[11] = a.p.cutoff;
+}
+
+constexpr int kVSchedThreads = 128;
+__global__ void __launch_bounds__(kVSchedThreads) vox_sched_pred_k(VoxSchedArgs a) {
+    __shared__ float P[dlmlp::kParams];
+    if (a.w) dlmlp::load_params(a.w, P);
+    const uint32_t nb = *a.nblocks;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        float x[12];
+        vox_block_features(a, b, nb, x);
+        if (a.feat)
+            for (int i = 0; i < 12; i++) a.feat[(uint64_t)b * 12 + i] = x[i];
+        if (a.w) {
+            const float y = dlmlp::forward(P, x, nullptr, nullptr);
+            const float q = (y == y) ? fminf(fmaxf((y + 4.0f) * 32.0f, 0.0f), 255.0f) : 0.0f;
+            const uint32_t bk = 255u - (uint32_t)q;                  // 0 = most expensive
+            a.bucket[b] = bk;
+            atomicAdd(&a.hist[bk], 1u);
+        }
+    }
+}
+
+__global__ void vox_sched_scan_k(uint32_t* hist) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int i = 0; i < 256; i++) { const uint32_t c = hist[i]; hist[i] = acc; acc += c; }
+    }
+}
+
+__global__ void vox_sched_scatter_k(VoxSchedArgs a) {
+    const uint32_t nb = *a.nblocks;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+        a.work[atomicAdd(&a.hist[a.bucket[b]], 1u)] = b;
 }
 
 // Keep non-zero masks, in block order; write flat indices (voxelize.ts:170-177).
@@ -581,17 +685,28 @@ double js_round(double x) {
     return (x - f >= 0.5) ? f + 1.0 : f;
 }
 
+}  // namespace
+
+// The voxelizer's grow-only device buffers, kept on the device between calls.
 struct VoxBufs {
     std::vector<DevBuf*> all;
     DevBuf scene, ext, rec, part, bounds, axes, scratch, keys0, keys1, vals0, vals1, status, hist, segs, bkey, bstart,
-        masks, oidx, olo, ohi;
+        masks, oidx, olo, ohi, used, bcount, sfeat, sbucket, shist, swork, scycles;
     VoxBufs() {
         DevBuf* l[] = {&scene, &ext, &rec, &part, &bounds, &axes, &scratch, &keys0, &keys1, &vals0, &vals1, &status,
-                       &hist, &segs, &bkey, &bstart, &masks, &oidx, &olo, &ohi};
+                       &hist, &segs, &bkey, &bstart, &masks, &oidx, &olo, &ohi, &used, &bcount, &sfeat, &sbucket,
+                       &shist, &swork, &scycles};
         all.assign(l, l + sizeof(l) / sizeof(l[0]));
     }
     ~VoxBufs() { for (DevBuf* b : all) b->release(); }
 };
+
+void dl_vox_release(dl_device* dev) {
+    delete dev->vox;
+    dev->vox = nullptr;
+}
+
+namespace {
 
 enum { VS_EMIT = 0, VS_SORT = 1, VS_HEADS = 5, VS_EVAL = 6, VS_COMPACT = 7, VS_ERR = 8, VS_OVF = 9, VS_TILES = 10,
        VS_NBLK = 11, VS_NOUT = 12, VS_WORDS = 16 };
@@ -613,7 +728,9 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     DL_CK(cudaSetDevice(dev->ordinal));
     cudaStream_t st = dev->stream;
     dl_vox_result* R = new dl_vox_result();
-    VoxBufs B;
+    if (!dev->vox) dev->vox = new VoxBufs();
+    VoxBufs& B = *dev->vox;
+    const bool logBlocks = opts && opts->log_blocks;
     const double blockSize = 4 * voxelRes;
     VoxParams p;
     std::memset(&p, 0, sizeof(p));
@@ -724,7 +841,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     // ---- cutoff <= 0: 1 - exp(-sigma) >= cutoff holds for every voxel, so every
     // voxel of every batch with a non-empty batch list is solid
     if (!(p.cutoff > 0.0f) && p.cutoff <= 0.0f) {
-        DevBuf usedD;
+        DevBuf& usedD = B.used;
         if ((s = usedD.ensure(4ull * numBatches)) != DL_OK) return fail(s);
         cudaMemsetAsync(usedD.p, 0, 4ull * numBatches, st);
         vox_batchused_k<<<prepGrid, 256, 0, st>>>(p, B.ext.as<float>(), usedD.as<uint32_t>());
@@ -755,7 +872,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     const int64_t NBX_ = p.NBB[0], NBY_ = p.NBB[1], NBZ_ = p.NBB[2];
     std::vector<unsigned long long> bc((size_t)(NBX_ * NBY_ * NBZ_), 0ull);     // pairs per batch
     {
-        DevBuf cnt;
+        DevBuf& cnt = B.bcount;
         if ((s = cnt.ensure(8ull * bc.size())) != DL_OK) return fail(s);
         cudaMemsetAsync(cnt.p, 0, 8ull * bc.size(), st);
         p.zlo = 0; p.zhi = p.NB[2] - 1;
@@ -927,10 +1044,33 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         ha.counter = scr + VS_HEADS; ha.err = scr + VS_ERR;
         vox_heads_k<<<headTiles, kVT, 0, st>>>(ha);
 
+        // learned block order (and per-block features for cost logging)
+        const uint32_t* work = nullptr;
+        if (dev->vox_sched || logBlocks) {
+            if ((s = B.sbucket.ensure(4 * maxBlocks)) != DL_OK || (s = B.swork.ensure(4 * maxBlocks)) != DL_OK ||
+                (s = B.shist.ensure(1024)) != DL_OK ||
+                (logBlocks && ((s = B.sfeat.ensure(48 * maxBlocks)) != DL_OK || (s = B.scycles.ensure(4 * maxBlocks)) != DL_OK)))
+                return fail(s);
+            VoxSchedArgs sa;
+            sa.p = p; sa.rec = B.rec.as<VoxRec>(); sa.vals = valsF; sa.bkey = B.bkey.as<uint32_t>();
+            sa.bstart = B.bstart.as<uint32_t>(); sa.nblocks = scr + VS_NBLK;
+            sa.w = dev->vox_sched ? (const __nv_bfloat16*)dl_mlp_weights(dev->vox_sched) : nullptr;
+            sa.feat = logBlocks ? B.sfeat.as<float>() : nullptr;
+            sa.bucket = B.sbucket.as<uint32_t>(); sa.hist = B.shist.as<uint32_t>(); sa.work = B.swork.as<uint32_t>();
+            const uint32_t sg = (uint32_t)std::min<uint64_t>((maxBlocks + kVSchedThreads - 1) / kVSchedThreads, 4096);
+            if (sa.w) cudaMemsetAsync(B.shist.p, 0, 1024, st);
+            vox_sched_pred_k<<<sg, kVSchedThreads, 0, st>>>(sa);
+            if (sa.w) {
+                vox_sched_scan_k<<<1, 32, 0, st>>>(sa.hist);
+                vox_sched_scatter_k<<<sg, kVSchedThreads, 0, st>>>(sa);
+                work = sa.work;
+            }
+        }
         EvalArgs va;
         va.p = p; va.rec = B.rec.as<VoxRec>(); va.vals = valsF; va.bkey = B.bkey.as<uint32_t>();
         va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
         va.counter = scr + VS_EVAL; va.evals = nullptr;
+        va.work = work; va.cycles = logBlocks ? B.scycles.as<uint32_t>() : nullptr;
         vox_eval_k<<<dev->sm_count * 24, 64, 0, st>>>(va);
 
         uint32_t hn[2] = {0, 0};
@@ -940,6 +1080,18 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             return fail(DL_E_CUDA);
         }
         const uint32_t nblk = hn[0];
+        if (logBlocks && nblk) {
+            const size_t f0 = R->log_cost.size();
+            R->log_feat.resize((f0 + nblk) * 12);
+            R->log_cost.resize(f0 + nblk);
+            std::vector<uint32_t> cyc(nblk);
+            if (cudaMemcpy(R->log_feat.data() + f0 * 12, B.sfeat.p, 48ull * nblk, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                cudaMemcpy(cyc.data(), B.scycles.p, 4ull * nblk, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                dl_set_error("voxelize: block log copy failed");
+                return fail(DL_E_CUDA);
+            }
+            for (uint32_t i = 0; i < nblk; i++) R->log_cost[f0 + i] = (float)cyc[i];
+        }
         if ((s = B.oidx.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK ||
             (s = B.olo.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK ||
             (s = B.ohi.ensure(4ull * std::max<uint32_t>(nblk, 1))) != DL_OK)
@@ -997,5 +1149,23 @@ extern "C" int dl_vox_result_copy(const dl_vox_result* r, uint32_t* idx, uint32_
 
 extern "C" int dl_vox_result_free(dl_vox_result* r) {
     delete r;
+    return DL_OK;
+}
+
+extern "C" int dl_device_set_voxel_scheduler(dl_device* dev, dl_mlp* mlp) {
+    if (!dev) { dl_set_error("device is NULL"); return DL_E_INVALID_ARG; }
+    dev->vox_sched = mlp;
+    return DL_OK;
+}
+
+extern "C" int dl_vox_result_block_log(const dl_vox_result* r, float* features, float* cost, uint64_t cap,
+                                       uint64_t* n) {
+    if (!r) { dl_set_error("result is NULL"); return DL_E_INVALID_ARG; }
+    const uint64_t T = r->log_cost.size();
+    if (n) *n = T;
+    if (T == 0 || (!features && !cost)) return DL_OK;
+    if (cap < T) { dl_set_error("dl_vox_result_block_log: capacity smaller than the block count"); return DL_E_INVALID_ARG; }
+    if (features) std::memcpy(features, r->log_feat.data(), 48ull * T);
+    if (cost) std::memcpy(cost, r->log_cost.data(), 4ull * T);
     return DL_OK;
 }

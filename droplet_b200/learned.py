@@ -9,7 +9,13 @@ Training runs on the GPU through the library's own kernels (dl_mlp_train).
 The trained parameters are stored in models/tile_cost_mlp.npz and loaded by
 load_default(); with no file, scheduling falls back to launch order.
 
+The block-cost model of the voxelizer is trained the same way on per-block
+features and measured cost (SM cycles / 16 of vox_eval_k per 4x4x4 block)
+logged from voxelizations of seeded 1M-Gaussian cluster scenes (seeds 3..10,
+three resolutions, two cutoffs); models/voxel_block_cost_mlp.npz.
+
   python -m droplet_b200.learned [--splats N] [--epochs E] [--out PATH]
+  python -m droplet_b200.learned --voxel [--epochs E] [--out PATH]
 """
 from __future__ import annotations
 
@@ -22,10 +28,12 @@ import time
 import numpy as np
 
 from . import _lib, synth
-from .api import Mlp, Renderer, createDevice
+from .api import Mlp, Renderer, createDevice, voxelize
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_PATH = os.path.join(HERE, "models", "tile_cost_mlp.npz")
+VOXEL_MODEL_PATH = os.path.join(HERE, "models", "voxel_block_cost_mlp.npz")
+VOXEL_SETTINGS = ((0.04, 0.1), (0.05, 0.3), (0.07, 0.1))
 TRAIN_SEEDS = tuple(range(3, 11))
 
 
@@ -61,6 +69,27 @@ def collect(renderer: Renderer, seeds=TRAIN_SEEDS, splats: int = 3_000_000, view
     return np.concatenate(X), np.concatenate(Y).astype(np.float32), np.concatenate(S)
 
 
+def voxel_scene(seed: int, n: int = 1_000_000):
+    """A seeded 1M-Gaussian cluster scene drawn like the voxelize configuration."""
+    return synth.cluster_scene(n, seed=seed, clusters=64, extent=5.0, log_lo=0.01, log_hi=0.1, op_mu=1.0,
+                               op_sigma=1.5)
+
+
+def collect_voxel(device, seeds=TRAIN_SEEDS, splats: int = 1_000_000, log=print):
+    """Voxelize every training scene / setting and log its blocks."""
+    X, Y, S = [], [], []
+    for seed in seeds:
+        t = time.time()
+        d = voxel_scene(seed, splats)
+        for res, cut in VOXEL_SETTINGS:
+            f, c = voxelize(device, d, {"voxelResolution": res, "opacityCutoff": cut, "logBlocks": True}).blockLog
+            X.append(f)
+            Y.append(np.log1p(c))
+            S.append(np.full(len(c), seed, np.int16))
+        log(f"seed {seed}: {sum(len(y) for y in Y)} blocks so far ({time.time() - t:.1f} s)")
+    return np.concatenate(X), np.concatenate(Y).astype(np.float32), np.concatenate(S)
+
+
 def spearman(a, b) -> float:
     ra = np.argsort(np.argsort(a)).astype(np.float64)
     rb = np.argsort(np.argsort(b)).astype(np.float64)
@@ -90,17 +119,26 @@ def load_default(device):
     return load(device, MODEL_PATH) if os.path.exists(MODEL_PATH) else None
 
 
+def load_default_voxel(device):
+    return load(device, VOXEL_MODEL_PATH) if os.path.exists(VOXEL_MODEL_PATH) else None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--splats", type=int, default=3_000_000)
     ap.add_argument("--views", type=int, default=40)
     ap.add_argument("--epochs", type=int, default=8)
-    ap.add_argument("--out", default=MODEL_PATH)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--voxel", action="store_true", help="train the voxelizer's block-cost model")
     a = ap.parse_args()
     dev = createDevice()
-    r = Renderer(dev)
     t = time.time()
-    X, y, seeds = collect(r, splats=a.splats, views=a.views)
+    if a.voxel:
+        X, y, seeds = collect_voxel(dev)
+        out = a.out or VOXEL_MODEL_PATH
+    else:
+        X, y, seeds = collect(Renderer(dev), splats=a.splats, views=a.views)
+        out = a.out or MODEL_PATH
     t_collect = time.time() - t
     val = seeds == TRAIN_SEEDS[-1]                  # held-out seed for the prediction error
     mlp = Mlp(dev, seed=0)
@@ -115,7 +153,7 @@ def main():
             "val_spearman": spearman(pred, y[val]),
             "val_r2": float(1 - (err ** 2).mean() / y[val].var()),
             "collect_s": t_collect, "train_s": t_train}
-    save(mlp, a.out, meta)
+    save(mlp, out, meta)
     print(json.dumps(meta))
 
 

@@ -90,6 +90,8 @@ typedef struct dl_vox_opts {
      * unsharded list in the reference's order.  0 / 0 voxelizes everything. */
     int32_t shard_index;
     int32_t shard_count;
+    /* 1: keep per-block features and measured cost (dl_vox_result_block_log) */
+    int32_t log_blocks;
 } dl_vox_opts;
 
 /* ---- errors ------------------------------------------------------------ */
@@ -220,6 +222,16 @@ int dl_vox_result_info(const dl_vox_result* res, double bounds_min[3], double bo
  * flat block index, low 32 voxel bits, high 32 voxel bits. */
 int dl_vox_result_copy(const dl_vox_result* res, uint32_t* block_idx, uint32_t* mask_lo, uint32_t* mask_hi);
 int dl_vox_result_free(dl_vox_result* res);
+/* Learned block order (no reference counterpart: the reference evaluates
+ * batches in dispatch order, voxelize.ts:186-248).  With a model attached,
+ * dl_voxelize on this device evaluates blocks in decreasing cost predicted
+ * from DL_MLP_IN per-block features (the block's and its neighbours' list
+ * lengths, a sample of its Gaussians' opacity and size, its place in the
+ * batch, the cutoff); the order changes timing only, never a bit.  NULL detaches. */
+int dl_device_set_voxel_scheduler(dl_device* dev, dl_mlp* mlp);
+/* After dl_voxelize with log_blocks: per evaluated block, in block order of
+ * each slab, its DL_MLP_IN features and measured cost (SM cycles / 16). */
+int dl_vox_result_block_log(const dl_vox_result* res, float* features, float* cost, uint64_t cap, uint64_t* n);
 
 /* ---- src/gpu/radix-sort.ts:91-216 GpuRadixSorter ----------------------- */
 /* Stable LSD radix sort of n u32 keys with u32 values in device memory (the

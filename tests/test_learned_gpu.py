@@ -144,3 +144,45 @@ def test_learned_order_against_measured_tile_costs(device):
         assert lrn <= nat * 1.001
     r.destroy()
     print("\n" + "\n".join(lines))
+
+
+def test_voxel_block_order_changes_no_bit(device):
+    # any block order (here: a randomly initialised model's) yields the same masks
+    d = learned.voxel_scene(30, 150_000)
+    opts = {"voxelResolution": 0.05, "opacityCutoff": 0.1}
+    base = dl.voxelize(device, d, opts)
+    m = dl.Mlp(device, seed=7)
+    device.set_voxel_scheduler(m)
+    try:
+        got = dl.voxelize(device, d, dict(opts, logBlocks=True))
+    finally:
+        device.set_voxel_scheduler(None)
+    assert np.array_equal(base.buffer.blockIdx, got.buffer.blockIdx)
+    assert np.array_equal(base.buffer.maskLo, got.buffer.maskLo) and np.array_equal(base.buffer.maskHi, got.buffer.maskHi)
+    f, c = got.blockLog
+    assert f.shape[1] == IN and len(c) >= base.buffer.count and np.all(np.isfinite(f)) and np.all(c > 0)
+
+
+def test_voxel_learned_order_against_measured_block_costs(device):
+    model = learned.load_default_voxel(device)
+    if model is None:
+        pytest.skip("no trained voxel model file")
+    d = learned.voxel_scene(21)
+    f, c = dl.voxelize(device, d, {"voxelResolution": 0.05, "opacityCutoff": 0.1, "logBlocks": True}).blockLog
+    pred = model.predict(f)
+    rank = lambda a: np.argsort(np.argsort(a))
+    rho = float(np.corrcoef(rank(pred), rank(c))[0, 1])
+    workers = 148 * 24                                  # persistent vox_eval_k CTAs
+    nat = _makespan(c, range(len(c)), workers)
+    lrn = _makespan(c, np.argsort(-pred, kind="stable"), workers)
+    ide = _makespan(c, np.argsort(-c, kind="stable"), workers)
+    lb = max(c.sum() / workers, c.max())
+    print(f"\nvoxel blocks {len(c)}: Spearman {rho:.3f}; makespan natural {nat / lb:.3f}, learned {lrn / lb:.3f}, "
+          f"ideal {ide / lb:.3f} (x lower bound)")
+    # The prediction must rank blocks well.  Its longest-first order is not
+    # required to beat the natural order: the lower bound here is the largest
+    # block, many blocks come close to it, and a ranking error among them
+    # delays a large block into the second wave, while the natural order
+    # already lands within a few percent of the ideal schedule.
+    assert rho > 0.7
+    assert ide <= nat <= 1.2 * lb
