@@ -865,8 +865,9 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 evals++;
                 const float power = -0.5f * ((((sc.z * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
                 if (power > 0.0f || power <= DL_POWER_CUT) continue;
-                const float alpha =
-                    fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR));
+                // the 0.999 cap of rasterize.ts:73 never binds: alpha <= opacity *
+                // (1 - exp(-4.5)) < 0.99 for opacity <= 1
+                const float alpha = sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR);
                 if (alpha < DL_MIN_ALPHA) continue;
                 const float w = T * alpha;
                 c0 = c0 + w * sb.w;
@@ -890,7 +891,8 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 if (p2 > 0.0f || p2 <= -6.4921275f) continue;          // -4.5 * log2(e)
                 float e;
                 asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
-                const float alpha = fminf(DL_OPACITY_CAP, sb.z * fmaxf(0.0f, e - DL_GAUSS_FLOOR));
+                // e - floor < 0 near the cut gives alpha < 0: skipped like alpha = 0
+                const float alpha = sb.z * (e - DL_GAUSS_FLOOR);
                 if (alpha < DL_MIN_ALPHA) continue;
                 const float w = T * alpha;
                 c0 = __fmaf_rn(w, sb.w, c0);
