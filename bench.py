@@ -300,7 +300,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream()              # a real stream: CUDA graphs cannot capture the legacy one
     torch.cuda.set_stream(stream)
     r.set_stream(stream.cuda_stream)
-    FAST = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
+    FAST = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP | _lib.DL_BATCH_CULL_OFFSCREEN
     scene = r.upload(data, "f16")
     outs = [torch.empty(c.width * c.height * 4, dtype=torch.uint8, device="cuda") for c in cams]
     ptrs = [o.data_ptr() for o in outs]
@@ -429,7 +429,8 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
             "config": config(args, cams, {"mode": "batched: one launch sequence for all views (a CUDA-graph "
-                                                  "replay when there are several), f16 scene SH and records, "
+                                                  "replay when there are several), splats without on-image tiles "
+                                                  "left out of the depth sort, f16 scene SH and records, "
                                                   "hardware exp2 (+-1 LSB), tiles rasterized in decreasing cost "
                                                   "predicted by the learned model",
                                           "parallelism": f"views sharded: {world} rank(s) x {len(cams)} distinct "

@@ -25,6 +25,7 @@ DL_BATCH_COUNT_EVALS = 64
 DL_BATCH_LOG_TILES = 128
 DL_BATCH_F64_DEGENERATE = 256
 DL_BATCH_SH16 = 512
+DL_BATCH_CULL_OFFSCREEN = 1024
 DL_MLP_IN, DL_MLP_HIDDEN = 12, 64
 DL_MLP_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 

@@ -28,7 +28,8 @@ enum {
     SC_PAIR_TILES = 12,
     SC_OVF = 13,
     SC_SCHED_CTR = 14,     // 4 counters
-    SC_SCHED_TILES = 18
+    SC_SCHED_TILES = 18,
+    SC_DEPTH_TILES2 = 19   // tiles of the depth sort after its first pass
 };
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
@@ -209,7 +210,7 @@ struct FrameDims {
     uint64_t stride = 64, cap = 0;
     uint32_t depthGrid = 1, emitTilesPerView = 1, pairGrid = 1;
     int pbits = 8, ppasses = 0;
-    bool f16rec = false, fastExp = false, f64deg = false;
+    bool f16rec = false, fastExp = false, f64deg = false, cullOff = false;
     int subLw = 3;                       // rasterizer work item width log2 (8x4)
 };
 
@@ -256,6 +257,7 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     d.f16rec = (flags & DL_BATCH_F16_RECORDS) != 0;
     d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
     d.f64deg = (flags & DL_BATCH_F64_DEGENERATE) != 0;
+    d.cullOff = (flags & DL_BATCH_CULL_OFFSCREEN) != 0;
     d.rasterGrid = raster_grid(d.fastExp);
     if (t.ctas_per_sm > 0) {
         int dev = 0, sms = 148;
@@ -287,6 +289,7 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
     pa.bbox = f.bbox;
     pa.nvis = f.nvis;
     pa.f64_degenerate = d.f64deg ? 1 : 0;
+    pa.cull_offscreen = d.cullOff ? 1 : 0;
     if (d.N) {
         dlr::project_k<<<(d.N + 255) / 256, 256, 0, st>>>(pa);
         (*launches)++;
@@ -299,19 +302,25 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
         ds.start = f.segStart; ds.len = f.segLen; ds.tile_base = f.segTileBase;
         ds.total_tiles = f.scr + SC_DEPTH_TILES; ds.num = d.V;
         dlsort::prepare_k<<<1, 32, 0, st>>>(ds);
+        // the first pass drops the culled keys (0xffffffff) and compacts the
+        // visible ones, in a stable order, to each view's segment start; the
+        // other passes sort the nvis[v] visible keys only
+        dlsort::Segs ds2 = ds;
+        ds2.len = f.nvis; ds2.tile_base = f.segTileBase + d.V; ds2.total_tiles = f.scr + SC_DEPTH_TILES2;
+        dlsort::prepare_k<<<1, 32, 0, st>>>(ds2);
         DL_CK(cudaMemsetAsync(f.depthHist, 0, 4ull * d.V * 4 * 256, st));
         dlsort::hist_k<8><<<std::min<uint32_t>(d.depthGrid, 4096), dlsort::kThreads, 0, st>>>(f.keys0, ds, 4, 0,
-                                                                                               f.depthHist);
+                                                                                               f.depthHist, 1);
         dlsort::scan_hist_k<8><<<std::min<uint32_t>(4 * d.V, 1024), 256, 0, st>>>(f.depthHist, 4 * d.V);
-        *launches += 3;
+        *launches += 4;
         uint32_t *kin = f.keys0, *kout = f.keys1, *vin = nullptr, *vout = f.vals1;
         for (int p = 0; p < 4; p++) {
             DL_CK(cudaMemsetAsync(f.sortStatus, 0, 4ull * 256 * d.depthGrid, st));
             dlsort::Pass sp;
             sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
-            sp.segs = ds; sp.glob_off = f.depthHist;
+            sp.segs = p == 0 ? ds : ds2; sp.glob_off = f.depthHist;
             sp.status = f.sortStatus; sp.counter = f.scr + SC_DEPTH_CTR + p; sp.err = f.scr + SC_ERR;
-            sp.shift = 8 * p; sp.pass = p; sp.passes = 4;
+            sp.shift = 8 * p; sp.pass = p; sp.passes = 4; sp.drop_max = p == 0 ? 1 : 0;
             launch_pass_bits(8, sp, d.depthGrid, st);
             (*launches)++;
             std::swap(kin, kout);
@@ -482,7 +491,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     DL_TRY(r->tileBase.ensure(4ull * (V + 1)));
     DL_TRY(r->segStart.ensure(8ull * V));
     DL_TRY(r->segLen.ensure(4ull * V));
-    DL_TRY(r->segTileBase.ensure(4ull * V));
+    DL_TRY(r->segTileBase.ensure(8ull * V));
     DL_TRY(r->scratch.ensure(4ull * kScratchWords));
     DL_TRY(r->keys0.ensure(4ull * V * d.stride));
     DL_TRY(r->keys1.ensure(4ull * V * d.stride));
@@ -807,7 +816,7 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     f.tileBase = c.take<uint32_t>(8);
     f.segStart = c.take<uint64_t>(8);
     f.segLen = c.take<uint32_t>(4);
-    f.segTileBase = c.take<uint32_t>(4);
+    f.segTileBase = c.take<uint32_t>(8);
     f.scr = c.take<uint32_t>(4ull * kScratchWords);
     f.keys0 = c.take<uint32_t>(4ull * kStaticMaxSplats);
     f.keys1 = c.take<uint32_t>(4ull * kStaticMaxSplats);

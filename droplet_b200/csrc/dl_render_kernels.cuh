@@ -37,6 +37,7 @@ struct ProjectArgs {
                               // field = box entirely left of / above the image; empty if minX > maxX
     uint32_t* nvis;           // [V] visible count
     int f64_degenerate;       // recompute det / conic / AA factor in f64 for near-degenerate splats
+    int cull_offscreen;       // also cull splats with no tile on the image (no pair can touch a pixel)
 };
 
 // A 2D covariance is near-degenerate when its f32 determinant has lost at
@@ -230,10 +231,12 @@ __global__ void __launch_bounds__(256, 4) project_k(ProjectArgs a) {
                 visible = r2 > u.near_d * u.near_d;
                 depthKey = (float)sqrt(r2);
             }
-            a.keys[o] = visible ? dl_sortable_key(depthKey) : 0xffffffffu;
+            if (!a.cull_offscreen || !visible) a.keys[o] = visible ? dl_sortable_key(depthKey) : 0xffffffffu;
         }
-        const uint32_t ballot = __ballot_sync(0xffffffffu, visible);
-        if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&s_vis[v], (uint32_t)__popc(ballot));
+        if (!a.cull_offscreen) {
+            const uint32_t ballot = __ballot_sync(0xffffffffu, visible);
+            if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&s_vis[v], (uint32_t)__popc(ballot));
+        }
         if (!visible) continue;
 
         // ---- project.ts:79-84
@@ -325,9 +328,32 @@ __global__ void __launch_bounds__(256, 4) project_k(ProjectArgs a) {
             }
         }
         if (culled) {
-            a.recA[o] = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
-            a.bbox[o] = make_uint2(0xffffu, 0u);
+            if (a.cull_offscreen) {
+                a.keys[o] = 0xffffffffu;
+            } else {
+                a.recA[o] = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
+                a.bbox[o] = make_uint2(0xffffu, 0u);
+            }
             continue;
+        }
+        // project.ts:224-233 tile AABB (u32() saturates: off-screen left/top splats land in row/col 0)
+        const uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
+        const uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
+        const float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
+        const uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
+        const uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        // A box right edge left of x = 0 (or bottom edge above y = 0) still counts
+        // column (row) 0 after the saturation, but no pixel centre can pass its
+        // box test there: flag it so the rasterizer skips these pairs unread.
+        const uint32_t phantom = ((fx1 < 0.0f) ? 0x8000u : 0u) | ((fy1 < 0.0f) ? 0x80000000u : 0u);
+        const bool hasTiles = maxTX >= minTX && maxTY >= minTY;
+        if (a.cull_offscreen) {
+            // a splat with no tile, or only phantom tiles, touches no pixel:
+            // leaving it out of the depth order changes no tile list's order
+            if (!hasTiles || phantom) { a.keys[o] = 0xffffffffu; continue; }
+            a.keys[o] = dl_sortable_key(depthKey);
+            const uint32_t m = __activemask();
+            if ((threadIdx.x & 31) == (uint32_t)(__ffs(m) - 1)) atomicAdd(&s_vis[v], (uint32_t)__popc(m));
         }
         float col0 = dc[0], col1 = dc[1], col2 = dc[2];
         if (a.sc.bands > 0) {
@@ -355,17 +381,7 @@ __global__ void __launch_bounds__(256, 4) project_k(ProjectArgs a) {
             a.recH[o] = make_uint4(pack_h2(conicA, conicB), pack_h2(conicC, alpha), pack_h2(col0, col1),
                                    pack_h2(col2, 0.0f));
         }
-        // project.ts:224-233 tile AABB (u32() saturates: off-screen left/top splats land in row/col 0)
-        const uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
-        const uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
-        const float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
-        const uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
-        const uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
-        // A box right edge left of x = 0 (or bottom edge above y = 0) still counts
-        // column (row) 0 after the saturation, but no pixel centre can pass its
-        // box test there: flag it so the rasterizer skips these pairs unread.
-        const uint32_t phantom = ((fx1 < 0.0f) ? 0x8000u : 0u) | ((fy1 < 0.0f) ? 0x80000000u : 0u);
-        if (maxTX >= minTX && maxTY >= minTY)
+        if (hasTiles)
             a.bbox[o] = make_uint2(minTX | (minTY << 16), (maxTX | (maxTY << 16)) | phantom);
         else
             a.bbox[o] = make_uint2(0xffffu, 0u);

@@ -66,9 +66,10 @@ static __global__ void prepare_k(Segs s) {
 }
 
 // Digit histograms of all passes: hist[seg][pass][radix] (must be zeroed).
+// drop_max: keys equal to 0xffffffff are left out (see Pass::drop_max).
 template <int BITS>
 __global__ void __launch_bounds__(kThreads) hist_k(const uint32_t* __restrict__ keys, Segs s, int passes,
-                                                   int first_shift, uint32_t* __restrict__ hist) {
+                                                   int first_shift, uint32_t* __restrict__ hist, int drop_max = 0) {
     constexpr int RADIX = 1 << BITS;
     __shared__ uint32_t sh[4 * RADIX];
     const uint32_t total = *s.total_tiles;
@@ -83,6 +84,7 @@ __global__ void __launch_bounds__(kThreads) hist_k(const uint32_t* __restrict__ 
             const uint32_t e = lt * kTile + j * kThreads + threadIdx.x;
             if (e < len) {
                 const uint32_t k = keys[base + e];
+                if (drop_max && k == 0xffffffffu) continue;
                 for (int p = 0; p < passes; p++)
                     atomicAdd(&sh[p * RADIX + ((k >> (first_shift + p * BITS)) & (RADIX - 1))], 1u);
             }
@@ -124,6 +126,10 @@ struct Pass {
     uint32_t* counter;           // dynamic tile counter, zeroed before the pass
     uint32_t* err;
     int shift, pass, passes;
+    // 1: elements whose key is 0xffffffff are dropped (neither ranked nor
+    // written); the others keep their relative order, so the output is the
+    // stable pass over the remaining elements, compacted to the segment start
+    int drop_max = 0;
 };
 
 constexpr int kLookback = 4;                 // predecessor tiles read per look-back step
@@ -140,6 +146,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     __shared__ uint32_t s_glob[RADIX];
     __shared__ uint32_t s_wsum[WARPS];
     __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_nkeep;                 // elements of the tile that are written
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(p.counter, 1u);
@@ -166,7 +173,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
         const bool ok = e < nValid;
         key[j] = ok ? p.keys_in[base + t0 + e] : 0u;
         val[j] = ok ? (p.vals_in ? p.vals_in[base + t0 + e] : t0 + e) : 0u;
-        dig[j] = ok ? (int)((key[j] >> p.shift) & MASK) : RADIX;
+        const bool keep = ok && !(p.drop_max && key[j] == 0xffffffffu);
+        dig[j] = keep ? (int)((key[j] >> p.shift) & MASK) : RADIX;
     }
 #pragma unroll
     for (int j = 0; j < kItems; j++) {
@@ -205,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
         uint32_t wpre = 0;
         for (int w = 0; w < warp; w++) wpre += s_wsum[w];
         if (tid < RADIX) s_toff[tid] = wpre + inc - v;
+        if (tid == RADIX - 1) s_nkeep = wpre + inc;
     }
     // decoupled look-back for this digit's prefix over earlier tiles of the segment
     if (tid < RADIX) {
@@ -259,7 +268,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     }
     __syncthreads();
     // coalesced write-out: consecutive threads write consecutive slots of a digit run
-    for (uint32_t i = tid; i < nValid; i += kThreads) {
+    const uint32_t nKeep = s_nkeep;
+    for (uint32_t i = tid; i < nKeep; i += kThreads) {
         const uint32_t k = s_keys[i];
         const uint32_t d = (k >> p.shift) & MASK;
         const uint64_t dst = base + s_glob[d] + (i - s_toff[d]);

@@ -253,3 +253,20 @@ def test_render_many_groups_and_sh16_match_the_batch(device):
     got16 = r2.render_many(d, cams, flags=fl | _lib.DL_BATCH_SH16)
     for a, b in zip(ref16, got16):
         assert np.array_equal(a, b)
+
+
+def test_offscreen_cull_changes_no_pixel(device, renderer):
+    # splats whose tile box misses the image (or only has phantom tiles) leave
+    # the depth order; every tile list keeps its order, so pixels are unchanged
+    d = synth.cluster_scene(150_000, seed=19, clusters=32, extent=10.0, bands=2)
+    cams = synth.ring_cameras(5, resolutions=[(320, 180), (500, 280)]) + [synth.pinhole(256, 256, (0.0, 0.0, 0.5))]
+    r2 = dl.Renderer(device)
+    sc = r2.upload(d)
+    for flags in (0, _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP):
+        a = r2.render_batch(sc, cams, flags=flags)
+        b = r2.render_batch(sc, cams, flags=flags | _lib.DL_BATCH_CULL_OFFSCREEN)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    one = r2.render_batch(sc, cams[:1], flags=_lib.DL_BATCH_CULL_OFFSCREEN)[0]
+    assert np.array_equal(one, renderer.render(d, cams[0]))
+    assert int(r2.debug_get("nvis", np.uint64)[0]) < d.count
