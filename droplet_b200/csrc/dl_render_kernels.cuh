@@ -187,7 +187,7 @@ __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
 // One splat, all views.  Thread per splat, index order (coalesced SoA reads).
 constexpr int kProjectMaxViews = 4096;          // views per frame (per-CTA visible counters)
 
-__global__ void __launch_bounds__(256, 4) project_k(ProjectArgs a) {
+__global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
     __shared__ uint32_t s_vis[kProjectMaxViews];
     for (uint32_t v = threadIdx.x; v < a.num_views; v += blockDim.x) s_vis[v] = 0;
     __syncthreads();
