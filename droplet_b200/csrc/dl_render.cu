@@ -50,7 +50,8 @@ int ensure_pinned(void** p, size_t* cap, size_t need) {
 
 template <int BITS>
 void launch_pass(const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
-    dlsort::pass_k<BITS><<<grid, dlsort::kThreads, 0, st>>>(p);
+    if (p.drop_max) dlsort::pass_k<BITS, true><<<grid, dlsort::kThreads, 0, st>>>(p);
+    else dlsort::pass_k<BITS><<<grid, dlsort::kThreads, 0, st>>>(p);
 }
 
 void launch_pass_bits(int bits, const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {

@@ -128,13 +128,15 @@ struct Pass {
     int shift, pass, passes;
     // 1: elements whose key is 0xffffffff are dropped (neither ranked nor
     // written); the others keep their relative order, so the output is the
-    // stable pass over the remaining elements, compacted to the segment start
+    // stable pass over the remaining elements, compacted to the segment start.
+    // Launch pass_k<BITS, true> for such a pass.
     int drop_max = 0;
 };
 
 constexpr int kLookback = 4;                 // predecessor tiles read per look-back step
 
-template <int BITS>
+// DROP: compiled in only for passes with Pass::drop_max set.
+template <int BITS, bool DROP = false>
 __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     constexpr int RADIX = 1 << BITS;
     constexpr int WARPS = kThreads / 32;
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
         const bool ok = e < nValid;
         key[j] = ok ? p.keys_in[base + t0 + e] : 0u;
         val[j] = ok ? (p.vals_in ? p.vals_in[base + t0 + e] : t0 + e) : 0u;
-        const bool keep = ok && !(p.drop_max && key[j] == 0xffffffffu);
+        const bool keep = ok && !(DROP && key[j] == 0xffffffffu);
         dig[j] = keep ? (int)((key[j] >> p.shift) & MASK) : RADIX;
     }
 #pragma unroll
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
         uint32_t wpre = 0;
         for (int w = 0; w < warp; w++) wpre += s_wsum[w];
         if (tid < RADIX) s_toff[tid] = wpre + inc - v;
-        if (tid == RADIX - 1) s_nkeep = wpre + inc;
+        if (DROP && tid == RADIX - 1) s_nkeep = wpre + inc;
     }
     // decoupled look-back for this digit's prefix over earlier tiles of the segment
     if (tid < RADIX) {
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     }
     __syncthreads();
     // coalesced write-out: consecutive threads write consecutive slots of a digit run
-    const uint32_t nKeep = s_nkeep;
+    const uint32_t nKeep = DROP ? s_nkeep : nValid;
     for (uint32_t i = tid; i < nKeep; i += kThreads) {
         const uint32_t k = s_keys[i];
         const uint32_t d = (k >> p.shift) & MASK;
