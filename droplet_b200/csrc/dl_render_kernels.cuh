@@ -337,11 +337,35 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             continue;
         }
         // project.ts:224-233 tile AABB (u32() saturates: off-screen left/top splats land in row/col 0)
-        const uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
-        const uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
-        const float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
-        const uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
-        const uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
+        uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
+        float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
+        uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
+        uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        if (a.cull_offscreen && maxTX >= minTX && maxTY >= minTY &&
+            (maxTX - minTX + 1u) * (maxTY - minTY + 1u) <= u.maxCoverage) {
+            // Bin by the box of the ellipse q <= 9.5 (q: the rasterizer's quadratic
+            // form, from the conic as it is stored) when the reference's square
+            // box is not truncated: its other tiles hold only pixels with q > 9,
+            // where alpha < 1/255 is skipped.
+            float cA = conicA, cB = conicB, cC = conicC;
+            if (!a.recBC) {
+                cA = __half2float(__float2half_rn(cA));
+                cB = __half2float(__float2half_rn(cB));
+                cC = __half2float(__float2half_rn(cC));
+            }
+            const float ac = cA * cC, dt = ac - cB * cB;
+            if (dt > 0.0f && ac <= 1024.0f * dt) {
+                const float s = 9.5f / dt;
+                const float ex = fminf(radius, sqrtf(cC * s)), ey = fminf(radius, sqrtf(cA * s));
+                minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - ex) / 16.0f)));
+                minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - ey) / 16.0f)));
+                fx1 = floorf((screenX + ex) / 16.0f);
+                fy1 = floorf((screenY + ey) / 16.0f);
+                maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
+                maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+            }
+        }
         // A box right edge left of x = 0 (or bottom edge above y = 0) still counts
         // column (row) 0 after the saturation, but no pixel centre can pass its
         // box test there: flag it so the rasterizer skips these pairs unread.
