@@ -187,10 +187,22 @@ __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
 // One splat, all views.  Thread per splat, index order (coalesced SoA reads).
 constexpr int kProjectMaxViews = 4096;          // views per frame (per-CTA visible counters)
 
+constexpr uint32_t kProjectSmemViews = 64;      // view tables staged in shared memory up to this count
+static_assert(sizeof(DlView) % 4 == 0, "DlView is copied as 32-bit words");
+
 __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
     __shared__ uint32_t s_vis[kProjectMaxViews];
+    __shared__ DlView s_views[kProjectSmemViews];
     for (uint32_t v = threadIdx.x; v < a.num_views; v += blockDim.x) s_vis[v] = 0;
+    const bool staged = a.num_views <= kProjectSmemViews;
+    if (staged) {
+        const uint32_t words = a.num_views * (uint32_t)(sizeof(DlView) / 4);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.views);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(s_views);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+    }
     __syncthreads();
+    const DlView* vtab = staged ? s_views : a.views;
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     const bool inRange = g < a.sc.n;
     float pos[3] = {0, 0, 0}, rot[4] = {1, 0, 0, 0}, s[3] = {1, 1, 1}, dc[3] = {0, 0, 0}, opl = 0.0f;
@@ -210,7 +222,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
     const uint64_t shBase = (uint64_t)g * 3 * M;
 
     for (uint32_t v = 0; v < a.num_views; v++) {
-        const DlView& u = a.views[v];
+        const DlView& u = vtab[v];
         const float* V = u.view;
         const uint64_t o = (uint64_t)v * a.view_stride + g;
         // ---- camera.ts:56-99: f64 cull and depth key
