@@ -464,6 +464,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.tile_evals = f.tileEvals;
     ra.tile_cycles = f.tileCycles;
     ra.sub_lw = d.subLw;
+    ra.rec_box = d.cullOff ? 1 : 0;
     if (d.fastExp) dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
     else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
     (*launches)++;

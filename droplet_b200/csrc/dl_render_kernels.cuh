@@ -354,6 +354,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
         uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
         uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        float boxX = radius, boxY = radius;          // half-extents the rasterizer tests (cull mode)
         if (a.cull_offscreen && maxTX >= minTX && maxTY >= minTY &&
             (maxTX - minTX + 1u) * (maxTY - minTY + 1u) <= u.maxCoverage) {
             // Bin by the box of the ellipse q <= 9.5 (q: the rasterizer's quadratic
@@ -370,6 +371,8 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             if (dt > 0.0f && ac <= 1024.0f * dt) {
                 const float s = 9.5f / dt;
                 const float ex = fminf(radius, sqrtf(cC * s)), ey = fminf(radius, sqrtf(cA * s));
+                boxX = ex;
+                boxY = ey;
                 minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - ex) / 16.0f)));
                 minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - ey) / 16.0f)));
                 fx1 = floorf((screenX + ex) / 16.0f);
@@ -409,7 +412,11 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         col1 = fmaxf(col1 + 0.5f, 0.0f);
         col2 = fmaxf(col2 + 0.5f, 0.0f);
         const float alpha = (sig * radiusFade) * aaFactor;
-        a.recA[o] = make_float4(screenX, screenY, radius, depth);
+        // cull mode: the screen record carries the half-extents of the box the
+        // rasterizer tests (the ellipse's box, or the radius square) instead of
+        // (radius, depth), which it does not read there
+        a.recA[o] = a.cull_offscreen ? make_float4(screenX, screenY, boxX, boxY)
+                                     : make_float4(screenX, screenY, radius, depth);
         if (a.recBC) {
             a.recBC[2 * o] = make_float4(conicA, conicB, conicC, alpha);
             a.recBC[2 * o + 1] = make_float4(col0, col1, col2, 0.0f);
@@ -772,6 +779,7 @@ struct RasterArgs {
     uint32_t* tile_evals;          // optional [total tiles] evaluated pairs per tile
     uint32_t* tile_cycles;         // optional [total tiles] SM cycles / 16 spent per tile
     int sub_lw;                    // log2 of a work item's width: 3 (8x4), 4 (16x2) or 2 (4x8) pixels
+    int rec_box;                   // 1: recA.zw are the half-extents to test (cull mode), else (radius, depth)
 };
 
 constexpr int kRasterThreads = 256;
@@ -853,13 +861,13 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
         float4 ra0 = make_float4(0, 0, 0, 0), ra1 = make_float4(0, 0, 0, 0);
         if (!(g0 & kPhantomBit)) {
             ra0 = __ldg(a.recA + vo + g0);
-            const float r = ra0.z;
-            hit0 = r > 0.0f && !(ra0.x - r > rx1) && !(ra0.x + r < rx0) && !(ra0.y - r > ry1) && !(ra0.y + r < ry0);
+            const float rx = ra0.z, ry = a.rec_box ? ra0.w : ra0.z;
+            hit0 = rx > 0.0f && !(ra0.x - rx > rx1) && !(ra0.x + rx < rx0) && !(ra0.y - ry > ry1) && !(ra0.y + ry < ry0);
         }
         if (!(g1 & kPhantomBit)) {
             ra1 = __ldg(a.recA + vo + g1);
-            const float r = ra1.z;
-            hit1 = r > 0.0f && !(ra1.x - r > rx1) && !(ra1.x + r < rx0) && !(ra1.y - r > ry1) && !(ra1.y + r < ry0);
+            const float rx = ra1.z, ry = a.rec_box ? ra1.w : ra1.z;
+            hit1 = rx > 0.0f && !(ra1.x - rx > rx1) && !(ra1.x + rx < rx0) && !(ra1.y - ry > ry1) && !(ra1.y + ry < ry0);
         }
         if (__ballot_sync(0xffffffffu, hit0 || hit1) == 0u) continue;
         // square-box hits load their record; the ellipse's box then decides
@@ -871,7 +879,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
             const uint32_t g = h ? g1 : g0;
             const float4 ra = h ? ra1 : ra0;
             float A = 0.0f, B = 0.0f, C = 0.0f, al = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
-            float ex = ra.z, ey = ra.z;
+            float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
             if (hit) {
                 if (a.recBC) {
                     const float4 p = __ldg(a.recBC + 2 * (vo + g));
@@ -885,7 +893,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                     const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
                     A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
                 }
-                if (!a.eval_count) {
+                if (!a.eval_count && !a.rec_box) {
                     tight_extent(A, B, C, ra.z, ex, ey);
                     hit = !(ra.x - ex > rx1) && !(ra.x + ex < rx0) && !(ra.y - ey > ry1) && !(ra.y + ey < ry0);
                 }
