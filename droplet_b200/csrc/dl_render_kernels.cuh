@@ -901,15 +901,17 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (hit) {
                 const uint32_t slot = n + __popc(m & lmask);
+                // s_b: conic and opacity (read for every pixel inside the box),
+                // s_c: colour (read only by pixels that composite the splat)
                 s_a[slot] = make_float4(ra.x, ra.y, ex, ey);
                 if (kExactExp) {
-                    s_b[slot] = make_float4(2.0f * B, C, al, cr);
-                    s_c[slot] = make_float4(cg, cb, A, 0.0f);
+                    s_b[slot] = make_float4(A, 2.0f * B, C, al);
                 } else {
                     // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
-                    s_b[slot] = make_float4(-1.4426950408889634f * B, -0.72134752044448170f * C, al, cr);
-                    s_c[slot] = make_float4(cg, cb, -0.72134752044448170f * A, 0.0f);
+                    s_b[slot] = make_float4(-0.72134752044448170f * A, -1.4426950408889634f * B,
+                                            -0.72134752044448170f * C, al);
                 }
+                s_c[slot] = make_float4(cr, cg, cb, 0.0f);
             }
             n += __popc(m);
         }
@@ -921,18 +923,18 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float dy = py - sa.y;
                 if (fabsf(dx) > sa.z || fabsf(dy) > sa.w) continue;
                 const float4 sb = s_b[j];
-                const float4 sc = s_c[j];
                 evals++;
-                const float power = -0.5f * ((((sc.z * dx) * dx) + ((sb.x * dx) * dy)) + ((sb.y * dy) * dy));
+                const float power = -0.5f * ((((sb.x * dx) * dx) + ((sb.y * dx) * dy)) + ((sb.z * dy) * dy));
                 if (power > 0.0f || power <= DL_POWER_CUT) continue;
                 // the 0.999 cap of rasterize.ts:73 never binds: alpha <= opacity *
                 // (1 - exp(-4.5)) < 0.99 for opacity <= 1
-                const float alpha = sb.z * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR);
+                const float alpha = sb.w * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR);
                 if (alpha < DL_MIN_ALPHA) continue;
                 const float w = T * alpha;
-                c0 = c0 + w * sb.w;
-                c1 = c1 + w * sc.x;
-                c2 = c2 + w * sc.y;
+                const float4 sc = s_c[j];
+                c0 = c0 + w * sc.x;
+                c1 = c1 + w * sc.y;
+                c2 = c2 + w * sc.z;
                 T = T * (1.0f - alpha);
                 if (T < DL_MIN_T) { done = true; break; }
             }
@@ -945,19 +947,19 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float dy = py - sa.y;
                 if (fabsf(dx) > sa.z || fabsf(dy) > sa.w) continue;
                 const float4 sb = s_b[j];
-                const float4 sc = s_c[j];
                 evals++;
-                const float p2 = __fmaf_rn(dx, __fmaf_rn(sc.z, dx, sb.x * dy), sb.y * dy * dy);
+                const float p2 = __fmaf_rn(dx, __fmaf_rn(sb.x, dx, sb.y * dy), sb.z * dy * dy);
                 if (p2 > 0.0f || p2 <= -6.4921275f) continue;          // -4.5 * log2(e)
                 float e;
                 asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
                 // e - floor < 0 near the cut gives alpha < 0: skipped like alpha = 0
-                const float alpha = sb.z * (e - DL_GAUSS_FLOOR);
+                const float alpha = sb.w * (e - DL_GAUSS_FLOOR);
                 if (alpha < DL_MIN_ALPHA) continue;
                 const float w = T * alpha;
-                c0 = __fmaf_rn(w, sb.w, c0);
-                c1 = __fmaf_rn(w, sc.x, c1);
-                c2 = __fmaf_rn(w, sc.y, c2);
+                const float4 sc = s_c[j];
+                c0 = __fmaf_rn(w, sc.x, c0);
+                c1 = __fmaf_rn(w, sc.y, c1);
+                c2 = __fmaf_rn(w, sc.z, c2);
                 T = __fmaf_rn(-T, alpha, T);
                 if (T < DL_MIN_T) { done = true; break; }
             }
