@@ -477,7 +477,7 @@ __device__ __forceinline__ uint32_t bbox_count(uint2 bb, uint32_t maxCov) {
     return c > maxCov ? maxCov : c;
 }
 
-__global__ void __launch_bounds__(kEmitThreads) emit_k(EmitArgs a) {
+__global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
     __shared__ uint32_t s_excl[kEmitRanks + 1];
     __shared__ uint32_t s_g[kEmitRanks];
     __shared__ uint32_t s_min[kEmitRanks];
