@@ -991,7 +991,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
 }
 
 template <bool kExactExp>
-__global__ void __launch_bounds__(kRasterThreads, 5) rasterize_k(RasterArgs a) {
+__global__ void __launch_bounds__(kRasterThreads, 6) rasterize_k(RasterArgs a) {
     __shared__ float4 s_a[kRasterWarps][64];
     __shared__ float4 s_b[kRasterWarps][64];
     __shared__ float4 s_c[kRasterWarps][64];
