@@ -454,7 +454,7 @@ __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, co
     return g.opacity * dl_expf(-0.5f * d2s);
 }
 
-__global__ void __launch_bounds__(64, 24) vox_eval_k(EvalArgs a) {
+__global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
     __shared__ VoxRec s_g[64];
     __shared__ uint32_t s_b;
     __shared__ uint32_t s_mask[2];
@@ -1071,7 +1071,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
         va.counter = scr + VS_EVAL; va.evals = nullptr;
         va.work = work; va.cycles = logBlocks ? B.scycles.as<uint32_t>() : nullptr;
-        vox_eval_k<<<dev->sm_count * 24, 64, 0, st>>>(va);
+        vox_eval_k<<<dev->sm_count * 32, 64, 0, st>>>(va);
 
         uint32_t hn[2] = {0, 0};
         if (cudaMemcpyAsync(hn, scr + VS_NBLK, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
