@@ -132,8 +132,12 @@ enum {
     DL_BATCH_F64_DEGENERATE = 256,/* f64 determinant and inverse for near-degenerate 2D covariances
                                      (det < 2^-10 c00 c11); culling and tile ranges unchanged */
     DL_BATCH_SH16 = 512,          /* dl_render_many: keep the uploaded SH coefficients in f16 */
-    DL_BATCH_CULL_OFFSCREEN = 1024 /* leave splats with no tile on the image out of the depth order
-                                      (pixels unchanged; depth ranks then count on-image splats only) */
+    DL_BATCH_CULL_OFFSCREEN = 1024 /* work that cannot change a pixel is left out: splats with no tile on
+                                      the image leave the depth order, untruncated splats are binned by
+                                      the box of their ellipse q <= 9.5, and the screen record ("recA")
+                                      holds (x, y, half-width, half-height) of the box the rasterizer
+                                      tests.  Pixels are unchanged; tile lists and depth ranks then
+                                      differ from the reference's. */
 };
 /* Render n views of one resident scene; outs[i] receives cams[i].width *
  * cams[i].height RGBA8 pixels (host or device memory, per flags). */
