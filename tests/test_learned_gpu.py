@@ -133,7 +133,7 @@ def test_learned_order_against_measured_tile_costs(device):
         pred = model.predict(f)
         rank = lambda a: np.argsort(np.argsort(a))
         rho = float(np.corrcoef(rank(pred), rank(c))[0, 1])
-        workers = 148 * 5                              # persistent rasterizer CTAs
+        workers = 148 * 6                              # persistent rasterizer CTAs (6 per SM)
         nat = _makespan(c, range(len(c)), workers)
         lrn = _makespan(c, np.argsort(-pred, kind="stable"), workers)
         ide = _makespan(c, np.argsort(-c, kind="stable"), workers)
