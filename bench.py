@@ -254,8 +254,15 @@ def run_voxel(args, rank, world, local_rank):
     vox = out.numBlocksX * out.numBlocksY * out.numBlocksZ * 64
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     with ClockSampler(local_rank) as clk:
         ms = run_steps(args.steps)
+    if world > 1:                                  # the slowest rank's time
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
     value = world * vox / (ms / 1e3) / 1e6
     line = {"metric": "Mvox/s (voxels of the block grid per second), voxelize", "value": value, "unit": "Mvox/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -453,9 +460,6 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload in VOXEL:
-        run_voxel(args, rank, world, local_rank)
-        return
     if world > 1:
         import datetime
 
@@ -464,7 +468,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload in VOXEL:
+            run_voxel(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
