@@ -465,8 +465,14 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.tile_cycles = f.tileCycles;
     ra.sub_lw = d.subLw;
     ra.rec_box = d.cullOff ? 1 : 0;
-    if (d.fastExp) dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
-    else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+    const bool count = ra.eval_count || ra.tile_evals;
+    if (d.fastExp) {
+        if (count) dlr::rasterize_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+        else dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+    } else {
+        if (count) dlr::rasterize_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+        else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+    }
     (*launches)++;
     DL_CK(cudaGetLastError());
     rec_event(ev, 7, st);

@@ -827,7 +827,8 @@ __device__ __forceinline__ uint32_t view_of_tile(const RasterArgs& a, uint32_t g
     return lo;
 }
 
-template <bool kExactExp>
+// kCount: count the evaluated (pixel, splat) pairs (eval_count / tile_evals).
+template <bool kExactExp, bool kCount>
 __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, uint32_t tile, uint32_t sub,
                                                uint32_t gt, float4* s_a, float4* s_b, float4* s_c) {
     const DlView& u = a.views[v];
@@ -923,7 +924,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float dy = py - sa.y;
                 if (fabsf(dx) > sa.z || fabsf(dy) > sa.w) continue;
                 const float4 sb = s_b[j];
-                evals++;
+                if (kCount) evals++;
                 const float power = -0.5f * ((((sb.x * dx) * dx) + ((sb.y * dx) * dy)) + ((sb.z * dy) * dy));
                 if (power > 0.0f || power <= DL_POWER_CUT) continue;
                 // the 0.999 cap of rasterize.ts:73 never binds: alpha <= opacity *
@@ -947,7 +948,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float dy = py - sa.y;
                 if (fabsf(dx) > sa.z || fabsf(dy) > sa.w) continue;
                 const float4 sb = s_b[j];
-                evals++;
+                if (kCount) evals++;
                 const float p2 = __fmaf_rn(dx, __fmaf_rn(sb.x, dx, sb.y * dy), sb.z * dy * dy);
                 if (p2 > 0.0f || p2 <= -6.4921275f) continue;          // -4.5 * log2(e)
                 float e;
@@ -967,7 +968,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
         if (__all_sync(0xffffffffu, done)) break;
         __syncwarp();                                   // staging area is reused by the next step
     }
-    if (a.tile_evals || a.eval_count) {
+    if (kCount) {
         uint32_t s = evals;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -990,7 +991,7 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
     if (a.tile_cycles && lane == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
 }
 
-template <bool kExactExp>
+template <bool kExactExp, bool kCount = false>
 __global__ void __launch_bounds__(kRasterThreads, 6) rasterize_k(RasterArgs a) {
     __shared__ float4 s_a[kRasterWarps][64];
     __shared__ float4 s_b[kRasterWarps][64];
@@ -1003,7 +1004,7 @@ __global__ void __launch_bounds__(kRasterThreads, 6) rasterize_k(RasterArgs a) {
         if (item >= a.num_items) return;
         const uint32_t gt = a.work ? a.work[item >> 3] : (item >> 3);
         const uint32_t v = view_of_tile(a, gt);
-        raster_subtile<kExactExp>(a, v, gt - a.tile_base[v], item & 7u, gt, s_a[warp], s_b[warp], s_c[warp]);
+        raster_subtile<kExactExp, kCount>(a, v, gt - a.tile_base[v], item & 7u, gt, s_a[warp], s_b[warp], s_c[warp]);
         __syncwarp();
     }
 }
