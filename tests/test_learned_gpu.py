@@ -1,6 +1,6 @@
 """The learned tile-cost model: its hand-written GPU kernels against a float64
 NumPy restatement, and the guarantee that the schedule it produces changes no
-pixel.  Its gain is judged against measured tile costs (list-scheduling makespan)
+pixel.  Its gain is measured against the logged tile costs (list-scheduling makespan)
 and timed in bench.py (value vs static_value)."""
 import numpy as np
 import pytest
@@ -114,7 +114,7 @@ def _makespan(costs, order, workers):
 
 
 def test_learned_order_against_measured_tile_costs(device):
-    # What the trained network buys, judged by measured cost: on a held-out
+    # What the trained network buys, measured against logged cost: on a held-out
     # scene, the per-tile costs the rasterizer logs are list-scheduled onto
     # the persistent CTAs in natural order, in predicted-cost order and in the
     # ideal (measured) order.  The prediction must rank tiles well, and its
