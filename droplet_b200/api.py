@@ -190,7 +190,7 @@ class Renderer:
         check(_lib.load().dl_render_batch(self.handle, scene._h, cams, n, _bg(background), ptrs, flags))
         return host
 
-    RASTER_SHAPES = ("8x4", "16x2", "4x8")
+    RASTER_SHAPES = ("8x4", "16x2", "4x8", "8x8x2")
 
     def set_tuning(self, pair_sort_bits: int = 8, raster_shape: str = "8x4", raster_ctas_per_sm: int = 0):
         """Timing-only knobs of rendered frames (dl_tuning); no knob changes a pixel."""

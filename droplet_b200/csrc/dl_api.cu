@@ -304,7 +304,7 @@ extern "C" int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst
 
 extern "C" int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t) {
     if (!r || !t) { dl_set_error("dl_renderer_set_tuning: NULL argument"); return DL_E_INVALID_ARG; }
-    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 2 ||
+    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 3 ||
         t->raster_ctas_per_sm < 0 || t->raster_ctas_per_sm > 5) {
         dl_set_error("dl_renderer_set_tuning: knob out of range");
         return DL_E_INVALID_ARG;
@@ -359,9 +359,10 @@ extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera
     DlTuning cur = r->tune;
     double curMs = 0.0;
     int rc = timeOne(cur, &curMs);
-    const int bitsC[3] = {8, 7, 6}, shapeC[3] = {0, 1, 2}, ctasC[3] = {0, 4, 3};
+    const int bitsC[4] = {8, 7, 6, 8}, shapeC[4] = {0, 1, 2, 3}, ctasC[4] = {0, 4, 3, 0};
+    const int nC[3] = {3, 4, 3};
     for (int knob = 0; knob < 3 && rc == DL_OK; knob++) {
-        for (int c = 0; c < 3 && rc == DL_OK; c++) {
+        for (int c = 0; c < nC[knob] && rc == DL_OK; c++) {
             DlTuning t = cur;
             if (knob == 0) { if (t.pair_bits == bitsC[c]) continue; t.pair_bits = bitsC[c]; }
             if (knob == 1) { if (t.shape == shapeC[c]) continue; t.shape = shapeC[c]; }

@@ -72,7 +72,7 @@ struct dl_scene {
 // Knobs of a batched frame that change timing only (dl_tuning in the ABI).
 struct DlTuning {
     int pair_bits = 8;        // pair-sort digit width 6..8
-    int shape = 0;            // rasterizer work item: 0 8x4, 1 16x2, 2 4x8 pixels
+    int shape = 0;            // rasterizer work item: 0 8x4, 1 16x2, 2 4x8, 3 8x8 (two pixels per lane)
     int ctas_per_sm = 0;      // persistent rasterizer CTAs per SM; 0 = occupancy limit
 };
 

@@ -213,19 +213,26 @@ struct FrameDims {
     int pbits = 8, ppasses = 0;
     bool f16rec = false, fastExp = false, f64deg = false, cullOff = false;
     int subLw = 3;                       // rasterizer work item width log2 (8x4)
+    bool ppl2 = false;                   // two pixels per lane (8x8 work items)
 };
 
 // Persistent rasterizer grid: every SM filled to its occupancy limit.
-uint32_t raster_grid(bool fastExp) {
-    static int cached[64][2] = {};
+uint32_t raster_grid(bool fastExp, bool ppl2) {
+    static int cached[64][4] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    int* c = (dev >= 0 && dev < 64) ? &cached[dev][fastExp ? 1 : 0] : nullptr;
+    int* c = (dev >= 0 && dev < 64) ? &cached[dev][(fastExp ? 1 : 0) + (ppl2 ? 2 : 0)] : nullptr;
     if (c && *c) return (uint32_t)*c;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (fastExp) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_k<false>, dlr::kRasterThreads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_k<true>, dlr::kRasterThreads, 0);
+    if (ppl2) {
+        if (fastExp) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize2_k<false>, dlr::kRasterThreads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize2_k<true>, dlr::kRasterThreads, 0);
+    } else if (fastExp) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_k<false>, dlr::kRasterThreads, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_k<true>, dlr::kRasterThreads, 0);
+    }
     const int g = std::max(sms, 1) * std::max(per, 1);
     if (c) *c = g;
     return (uint32_t)g;
@@ -236,6 +243,7 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     FrameDims d;
     d.pbits = (t.pair_bits >= 6 && t.pair_bits <= 8) ? t.pair_bits : 8;
     d.subLw = t.shape == 1 ? 4 : t.shape == 2 ? 2 : 3;
+    d.ppl2 = t.shape == 3;
     d.V = V;
     d.N = N;
     d.stride = round_up(std::max<uint32_t>(N, 1), 64);
@@ -259,7 +267,7 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
     d.f64deg = (flags & DL_BATCH_F64_DEGENERATE) != 0;
     d.cullOff = (flags & DL_BATCH_CULL_OFFSCREEN) != 0;
-    d.rasterGrid = raster_grid(d.fastExp);
+    d.rasterGrid = raster_grid(d.fastExp, d.ppl2);
     if (t.ctas_per_sm > 0) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -458,7 +466,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.outs = f.outs;
     ra.accum = f.accum;
     ra.work = work;
-    ra.num_items = 8u * d.totalTiles;
+    ra.num_items = (d.ppl2 ? 4u : 8u) * d.totalTiles;
     ra.work_counter = f.scr + SC_WORK_CTR;
     ra.eval_count = f.evalCount;
     ra.tile_evals = f.tileEvals;
@@ -466,7 +474,15 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.sub_lw = d.subLw;
     ra.rec_box = d.cullOff ? 1 : 0;
     const bool count = ra.eval_count || ra.tile_evals;
-    if (d.fastExp) {
+    if (d.ppl2) {
+        if (d.fastExp) {
+            if (count) dlr::rasterize2_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+            else dlr::rasterize2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+        } else {
+            if (count) dlr::rasterize2_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+            else dlr::rasterize2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+        }
+    } else if (d.fastExp) {
         if (count) dlr::rasterize_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
         else dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
     } else {
@@ -653,7 +669,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             const uint64_t* sp = reinterpret_cast<const uint64_t*>(&sc);
             key.insert(key.end(), sp, sp + sizeof(DlSceneDev) / 8);
             key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid,
-                                   (uint64_t)d.pbits, (uint64_t)d.subLw});
+                                   (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2});
             if (!r->graph_exec || key != r->graph_key) {
                 if (r->graph_exec) { cudaGraphExecDestroy(r->graph_exec); r->graph_exec = nullptr; }
                 cudaGraph_t g = nullptr;

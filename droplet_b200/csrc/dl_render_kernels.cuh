@@ -827,6 +827,79 @@ __device__ __forceinline__ uint32_t view_of_tile(const RasterArgs& a, uint32_t g
     return lo;
 }
 
+// Stage the next 64 pairs of a tile's slice [b, end) that can reach the
+// rectangle [rx0, rx1] x [ry0, ry1] into the warp's shared arrays, in slice
+// order; returns how many (warp-uniform).
+template <bool kExactExp>
+__device__ __forceinline__ uint32_t stage_chunk(const RasterArgs& a, const uint32_t* vals, uint32_t b, uint32_t end,
+                                                uint64_t vo, float rx0, float rx1, float ry0, float ry1,
+                                                uint32_t lmask, float4* s_a, float4* s_b, float4* s_c) {
+    const int lane = threadIdx.x & 31;
+    // two chunks of 32 pairs per step: independent load chains in flight
+    const uint32_t e0 = b + lane, e1 = b + 32 + lane;
+    const uint32_t g0 = e0 < end ? __ldg(vals + e0) : kPhantomBit;
+    const uint32_t g1 = e1 < end ? __ldg(vals + e1) : kPhantomBit;
+    bool hit0 = false, hit1 = false;
+    float4 ra0 = make_float4(0, 0, 0, 0), ra1 = make_float4(0, 0, 0, 0);
+    if (!(g0 & kPhantomBit)) {
+        ra0 = __ldg(a.recA + vo + g0);
+        const float rx = ra0.z, ry = a.rec_box ? ra0.w : ra0.z;
+        hit0 = rx > 0.0f && !(ra0.x - rx > rx1) && !(ra0.x + rx < rx0) && !(ra0.y - ry > ry1) && !(ra0.y + ry < ry0);
+    }
+    if (!(g1 & kPhantomBit)) {
+        ra1 = __ldg(a.recA + vo + g1);
+        const float rx = ra1.z, ry = a.rec_box ? ra1.w : ra1.z;
+        hit1 = rx > 0.0f && !(ra1.x - rx > rx1) && !(ra1.x + rx < rx0) && !(ra1.y - ry > ry1) && !(ra1.y + ry < ry0);
+    }
+    if (__ballot_sync(0xffffffffu, hit0 || hit1) == 0u) return 0u;
+    // square-box hits load their record; the ellipse's box then decides
+    // (with eval counting on, the square box alone: the reference's count)
+    uint32_t n = 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        bool hit = h ? hit1 : hit0;
+        const uint32_t g = h ? g1 : g0;
+        const float4 ra = h ? ra1 : ra0;
+        float A = 0.0f, B = 0.0f, C = 0.0f, al = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+        float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
+        if (hit) {
+            if (a.recBC) {
+                const float4 p = __ldg(a.recBC + 2 * (vo + g));
+                const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
+                A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
+            } else {
+                const uint4 hv = __ldg(a.recH + vo + g);
+                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
+                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
+                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
+                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
+                A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+            }
+            if (!a.eval_count && !a.rec_box) {
+                tight_extent(A, B, C, ra.z, ex, ey);
+                hit = !(ra.x - ex > rx1) && !(ra.x + ex < rx0) && !(ra.y - ey > ry1) && !(ra.y + ey < ry0);
+            }
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const uint32_t slot = n + __popc(m & lmask);
+            // s_b: conic and opacity (read for every pixel inside the box),
+            // s_c: colour (read only by pixels that composite the splat)
+            s_a[slot] = make_float4(ra.x, ra.y, ex, ey);
+            if (kExactExp) {
+                s_b[slot] = make_float4(A, 2.0f * B, C, al);
+            } else {
+                // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
+                s_b[slot] = make_float4(-0.72134752044448170f * A, -1.4426950408889634f * B,
+                                        -0.72134752044448170f * C, al);
+            }
+            s_c[slot] = make_float4(cr, cg, cb, 0.0f);
+        }
+        n += __popc(m);
+    }
+    return n;
+}
+
 // kCount: count the evaluated (pixel, splat) pairs (eval_count / tile_evals).
 template <bool kExactExp, bool kCount>
 __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, uint32_t tile, uint32_t sub,
@@ -854,68 +927,8 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
     bool done = !inImage;
     uint32_t evals = 0;
     for (uint32_t b = start; b < end; b += 64) {
-        // two chunks of 32 pairs per step: independent load chains in flight
-        const uint32_t e0 = b + lane, e1 = b + 32 + lane;
-        const uint32_t g0 = e0 < end ? __ldg(vals + e0) : kPhantomBit;
-        const uint32_t g1 = e1 < end ? __ldg(vals + e1) : kPhantomBit;
-        bool hit0 = false, hit1 = false;
-        float4 ra0 = make_float4(0, 0, 0, 0), ra1 = make_float4(0, 0, 0, 0);
-        if (!(g0 & kPhantomBit)) {
-            ra0 = __ldg(a.recA + vo + g0);
-            const float rx = ra0.z, ry = a.rec_box ? ra0.w : ra0.z;
-            hit0 = rx > 0.0f && !(ra0.x - rx > rx1) && !(ra0.x + rx < rx0) && !(ra0.y - ry > ry1) && !(ra0.y + ry < ry0);
-        }
-        if (!(g1 & kPhantomBit)) {
-            ra1 = __ldg(a.recA + vo + g1);
-            const float rx = ra1.z, ry = a.rec_box ? ra1.w : ra1.z;
-            hit1 = rx > 0.0f && !(ra1.x - rx > rx1) && !(ra1.x + rx < rx0) && !(ra1.y - ry > ry1) && !(ra1.y + ry < ry0);
-        }
-        if (__ballot_sync(0xffffffffu, hit0 || hit1) == 0u) continue;
-        // square-box hits load their record; the ellipse's box then decides
-        // (with eval counting on, the square box alone: the reference's count)
-        uint32_t n = 0;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            bool hit = h ? hit1 : hit0;
-            const uint32_t g = h ? g1 : g0;
-            const float4 ra = h ? ra1 : ra0;
-            float A = 0.0f, B = 0.0f, C = 0.0f, al = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
-            float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
-            if (hit) {
-                if (a.recBC) {
-                    const float4 p = __ldg(a.recBC + 2 * (vo + g));
-                    const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
-                    A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
-                } else {
-                    const uint4 hv = __ldg(a.recH + vo + g);
-                    const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
-                    const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
-                    const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
-                    const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
-                    A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
-                }
-                if (!a.eval_count && !a.rec_box) {
-                    tight_extent(A, B, C, ra.z, ex, ey);
-                    hit = !(ra.x - ex > rx1) && !(ra.x + ex < rx0) && !(ra.y - ey > ry1) && !(ra.y + ey < ry0);
-                }
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const uint32_t slot = n + __popc(m & lmask);
-                // s_b: conic and opacity (read for every pixel inside the box),
-                // s_c: colour (read only by pixels that composite the splat)
-                s_a[slot] = make_float4(ra.x, ra.y, ex, ey);
-                if (kExactExp) {
-                    s_b[slot] = make_float4(A, 2.0f * B, C, al);
-                } else {
-                    // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
-                    s_b[slot] = make_float4(-0.72134752044448170f * A, -1.4426950408889634f * B,
-                                            -0.72134752044448170f * C, al);
-                }
-                s_c[slot] = make_float4(cr, cg, cb, 0.0f);
-            }
-            n += __popc(m);
-        }
+        const uint32_t n = stage_chunk<kExactExp>(a, vals, b, end, vo, rx0, rx1, ry0, ry1, lmask, s_a, s_b, s_c);
+        if (n == 0u) continue;
         __syncwarp();
         if (!done && kExactExp) {
             for (uint32_t j = 0; j < n; j++) {
@@ -989,6 +1002,151 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
         if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c0, c1, c2, T);
     }
     if (a.tile_cycles && lane == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
+}
+
+// Two pixels per lane: a work item is an 8x8-pixel quarter of a 16x16 tile;
+// lane l owns pixels (l % 8, l / 8) and (l % 8, l / 8 + 4) of it.  The two
+// pixels share each staged record's shared-memory reads, and a tile's slice is
+// scanned by 4 warps instead of 8.  Per pixel, the same arithmetic in the same
+// splat order as raster_subtile.
+template <bool kExactExp, bool kCount>
+__device__ __forceinline__ void raster_subtile2(const RasterArgs& a, uint32_t v, uint32_t tile, uint32_t sub,
+                                                uint32_t gt, float4* s_a, float4* s_b, float4* s_c) {
+    const DlView& u = a.views[v];
+    const int lane = threadIdx.x & 31;
+    const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
+    const uint32_t sx0 = tx * DL_TILE + (sub & 1u) * 8u, sy0 = ty * DL_TILE + (sub >> 1) * 8u;
+    const uint32_t x = sx0 + (lane & 7), y0 = sy0 + (lane >> 3), y1 = y0 + 4u;
+    const bool in0 = x < u.W && y0 < u.H, in1 = x < u.W && y1 < u.H;
+    if (__all_sync(0xffffffffu, !in0)) return;            // y1 > y0: no pixel of the item is inside
+    const long long t0 = a.tile_cycles ? clock64() : 0;
+    const float px = (float)x + 0.5f, py0 = (float)y0 + 0.5f, py1 = (float)y1 + 0.5f;
+    const float rx0 = (float)sx0 + 0.5f - 1.0f, rx1 = (float)(sx0 + 8u) - 0.5f + 1.0f;
+    const float ry0 = (float)sy0 + 0.5f - 1.0f, ry1 = (float)(sy0 + 8u) - 0.5f + 1.0f;
+    const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    const uint32_t start = to[tile], end = to[tile + 1];
+    const uint32_t* vals = a.pair_vals + a.pair_base[v];
+    const uint64_t vo = (uint64_t)v * a.view_stride;
+    const uint32_t lmask = dl_lanemask_lt();
+
+    float c[2][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}}, T[2] = {1.0f, 1.0f};
+    bool done[2] = {!in0, !in1};
+    const float py[2] = {py0, py1};
+    uint32_t evals = 0;
+    for (uint32_t b = start; b < end; b += 64) {
+        const uint32_t n = stage_chunk<kExactExp>(a, vals, b, end, vo, rx0, rx1, ry0, ry1, lmask, s_a, s_b, s_c);
+        if (n == 0u) continue;
+        __syncwarp();
+        if (!(done[0] && done[1])) {
+            for (uint32_t j = 0; j < n; j++) {
+                const float4 sa = s_a[j];
+                const float dx = px - sa.x;
+                if (fabsf(dx) > sa.z) continue;
+                float dy[2];
+                bool box[2];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    dy[k] = py[k] - sa.y;
+                    box[k] = !done[k] && !(fabsf(dy[k]) > sa.w);
+                }
+                if (!(box[0] || box[1])) continue;
+                const float4 sb = s_b[j];
+                float alpha[2];
+                bool use[2];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    use[k] = false;
+                    alpha[k] = 0.0f;
+                    if (box[k]) {
+                        if (kCount) evals++;
+                        if (kExactExp) {
+                            const float power = -0.5f * ((((sb.x * dx) * dx) + ((sb.y * dx) * dy[k])) +
+                                                         ((sb.z * dy[k]) * dy[k]));
+                            if (!(power > 0.0f || power <= DL_POWER_CUT)) {
+                                alpha[k] = sb.w * fmaxf(0.0f, raster_exp<kExactExp>(power) - DL_GAUSS_FLOOR);
+                                use[k] = !(alpha[k] < DL_MIN_ALPHA);
+                            }
+                        } else {
+                            const float p2 = __fmaf_rn(dx, __fmaf_rn(sb.x, dx, sb.y * dy[k]), sb.z * dy[k] * dy[k]);
+                            if (!(p2 > 0.0f || p2 <= -6.4921275f)) {
+                                float e;
+                                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
+                                alpha[k] = sb.w * (e - DL_GAUSS_FLOOR);
+                                use[k] = !(alpha[k] < DL_MIN_ALPHA);
+                            }
+                        }
+                    }
+                }
+                if (!(use[0] || use[1])) continue;
+                const float4 sc = s_c[j];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    if (use[k]) {
+                        const float w = T[k] * alpha[k];
+                        if (kExactExp) {
+                            c[k][0] = c[k][0] + w * sc.x;
+                            c[k][1] = c[k][1] + w * sc.y;
+                            c[k][2] = c[k][2] + w * sc.z;
+                            T[k] = T[k] * (1.0f - alpha[k]);
+                        } else {
+                            c[k][0] = __fmaf_rn(w, sc.x, c[k][0]);
+                            c[k][1] = __fmaf_rn(w, sc.y, c[k][1]);
+                            c[k][2] = __fmaf_rn(w, sc.z, c[k][2]);
+                            T[k] = __fmaf_rn(-T[k], alpha[k], T[k]);
+                        }
+                        if (T[k] < DL_MIN_T) done[k] = true;
+                    }
+                }
+                if (done[0] && done[1]) break;
+            }
+        }
+        if (__all_sync(0xffffffffu, done[0] && done[1])) break;
+        __syncwarp();                                   // staging area is reused by the next step
+    }
+    if (kCount) {
+        uint32_t s = evals;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0 && s) {
+            if (a.tile_evals) atomicAdd(&a.tile_evals[gt], s);
+            if (a.eval_count) atomicAdd(a.eval_count, (unsigned long long)s);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const uint32_t y = k ? y1 : y0;
+        if (k ? in1 : in0) {
+            // finalize.ts:30-43
+            const float rr = fminf(fmaxf(c[k][0] + T[k] * u.bg[0], 0.0f), 1.0f);
+            const float gg = fminf(fmaxf(c[k][1] + T[k] * u.bg[1], 0.0f), 1.0f);
+            const float bb = fminf(fmaxf(c[k][2] + T[k] * u.bg[2], 0.0f), 1.0f);
+            const float aa = fminf(fmaxf((1.0f - T[k]) + T[k] * u.bg[3], 0.0f), 1.0f);
+            const uint32_t out = dl_sat_u32(rr * 255.0f + 0.5f) | (dl_sat_u32(gg * 255.0f + 0.5f) << 8) |
+                                 (dl_sat_u32(bb * 255.0f + 0.5f) << 16) | (dl_sat_u32(aa * 255.0f + 0.5f) << 24);
+            a.outs[v][(uint64_t)y * u.W + x] = out;
+            if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c[k][0], c[k][1], c[k][2], T[k]);
+        }
+    }
+    if (a.tile_cycles && lane == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
+}
+
+// The two-pixels-per-lane rasterizer: 4 work items per tile.
+template <bool kExactExp, bool kCount = false>
+__global__ void __launch_bounds__(kRasterThreads, 5) rasterize2_k(RasterArgs a) {
+    __shared__ float4 s_a[kRasterWarps][64];
+    __shared__ float4 s_b[kRasterWarps][64];
+    __shared__ float4 s_c[kRasterWarps][64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    while (true) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.num_items) return;
+        const uint32_t gt = a.work ? a.work[item >> 2] : (item >> 2);
+        const uint32_t v = view_of_tile(a, gt);
+        raster_subtile2<kExactExp, kCount>(a, v, gt - a.tile_base[v], item & 3u, gt, s_a[warp], s_b[warp], s_c[warp]);
+        __syncwarp();
+    }
 }
 
 template <bool kExactExp, bool kCount = false>

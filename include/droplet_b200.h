@@ -174,7 +174,8 @@ int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg
  * tile space), and so changes pixels. */
 typedef struct dl_tuning {
     int32_t pair_sort_bits;       /* digit width of the tile-pair sort: 6, 7 or 8 (default 8) */
-    int32_t raster_shape;         /* pixels of one rasterizer work item (one warp): 0 = 8x4, 1 = 16x2, 2 = 4x8 */
+    int32_t raster_shape;         /* pixels of one rasterizer work item (one warp): 0 = 8x4, 1 = 16x2, 2 = 4x8,
+                                     3 = 8x8 with two pixels per lane */
     int32_t raster_ctas_per_sm;   /* persistent rasterizer CTAs per SM, 1..5; 0 = the occupancy limit */
 } dl_tuning;
 int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t);

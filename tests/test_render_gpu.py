@@ -209,18 +209,24 @@ def test_tuning_knobs_change_no_pixel_and_autotune_keeps_one(device):
     flags = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
     base = r2.render_batch(sc, cams, flags=flags)
     for kw in ({"pair_sort_bits": 7}, {"pair_sort_bits": 6}, {"raster_shape": "16x2"}, {"raster_shape": "4x8"},
+               {"raster_shape": "8x8x2"},
                {"raster_ctas_per_sm": 3}, {"raster_ctas_per_sm": 1},
                {"pair_sort_bits": 6, "raster_shape": "4x8", "raster_ctas_per_sm": 2}):
         r2.set_tuning(**kw)
         for a, b in zip(base, r2.render_batch(sc, cams, flags=flags)):
             assert np.array_equal(a, b), kw
-    sc32 = r2.upload(d)                    # exact path under the last tuning == the single-view render
+    r2.set_tuning(raster_shape="8x8x2")
+    sc32 = r2.upload(d)
+    for a, c in zip(r2.render_batch(sc32, cams), cams):     # exact path, two pixels per lane
+        assert np.array_equal(a, renderer_single(device, d, c))
+    r2.set_tuning(pair_sort_bits=6, raster_shape="4x8", raster_ctas_per_sm=2)
+                                           # exact path under the last tuning == the single-view render
     exact = r2.render_batch(sc32, cams)
     for a, c in zip(exact, cams):
         assert np.array_equal(a, renderer_single(device, d, c))
     r2.set_tuning()
     t = r2.autotune(sc, cams, flags=flags, reps=2)
-    assert t["pair_sort_bits"] in (6, 7, 8) and t["raster_shape"] in ("8x4", "16x2", "4x8") and t["frame_ms"] > 0
+    assert t["pair_sort_bits"] in (6, 7, 8) and t["raster_shape"] in ("8x4", "16x2", "4x8", "8x8x2") and t["frame_ms"] > 0
     assert r2.get_tuning() == {k: t[k] for k in ("pair_sort_bits", "raster_shape", "raster_ctas_per_sm")}
     for a, b in zip(base, r2.render_batch(sc, cams, flags=flags)):
         assert np.array_equal(a, b)
