@@ -73,6 +73,7 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
     if (!r) return DL_OK;
     cudaSetDevice(r->dev->ordinal);
     cudaStreamSynchronize(r->stream);
+    if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
     DevBuf* bufs[] = {&r->views, &r->tileBase, &r->segStart, &r->segLen, &r->segTileBase, &r->scratch, &r->keys0, &r->keys1,
                       &r->vals0, &r->vals1, &r->recA, &r->recBC, &r->recH, &r->bbox, &r->nvis, &r->depthHist,
                       &r->sortStatus, &r->pairBase, &r->pairCap, &r->pkeys0, &r->pkeys1, &r->pvals0, &r->pvals1,
@@ -83,6 +84,7 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
     r->tuneOut.release();
     if (r->copy_stream) { cudaStreamSynchronize(r->copy_stream); cudaStreamDestroy(r->copy_stream); }
     if (r->copy_event) cudaEventDestroy(r->copy_event);
+    for (auto& e : r->upload_events) if (e) cudaEventDestroy(e);
     if (r->h_views) cudaFreeHost(r->h_views);
     if (r->h_u64) cudaFreeHost(r->h_u64);
     for (auto& e : r->ev) if (e) cudaEventDestroy(e);
@@ -172,20 +174,60 @@ extern "C" int dl_scene_free(dl_scene* s) {
     return DL_OK;
 }
 
+namespace {
+
+int ensure_copy_stream(dl_renderer* r) {
+    if (!r->copy_stream) DL_CK(cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking));
+    if (!r->copy_event) DL_CK(cudaEventCreateWithFlags(&r->copy_event, cudaEventDisableTiming));
+    return DL_OK;
+}
+
+// Multi-view render of a scene; `upload` (NULL: the scene is resident) is an
+// upload still running on the copy stream.
+int render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4], uint8_t* const* outs,
+                 uint32_t flags, const DlUploadChunks* upload);
+
+}  // namespace
+
 extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
-                               uint8_t* const* outs, uint32_t flags);
+                               uint8_t* const* outs, uint32_t flags) {
+    return render_batch(r, s, cams, n, bg, outs, flags, nullptr);
+}
 
 extern "C" int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
                               uint8_t* const* outs, uint32_t flags) {
     if (!r || !data) { dl_set_error("dl_render_many: NULL argument"); return DL_E_INVALID_ARG; }
     DL_CK(cudaSetDevice(r->dev->ordinal));
     const int prec = ((flags & DL_BATCH_SH16) && !(flags & DL_BATCH_PLAIN)) ? DL_PREC_F16 : DL_PREC_F32;
-    DL_TRY(dl_upload_scene(&r->own_scene, data, prec, r->stream));
-    return dl_render_batch(r, &r->own_scene, cams, n, bg, outs, flags & ~(uint32_t)DL_BATCH_OUT_DEVICE);
+    flags &= ~(uint32_t)DL_BATCH_OUT_DEVICE;
+    if (n < 8 || r->profiling || (flags & DL_BATCH_PLAIN)) {
+        DL_TRY(dl_upload_scene(&r->own_scene, data, prec, r->stream));
+        return render_batch(r, &r->own_scene, cams, n, bg, outs, flags, nullptr);
+    }
+    // the upload runs in splat ranges on the copy stream and projection of
+    // each range starts when it has arrived
+    DL_TRY(ensure_copy_stream(r));
+    DlUploadChunks up;
+    for (int k = 0; k < kUploadChunks; k++) {
+        if (!r->upload_events[k]) DL_CK(cudaEventCreateWithFlags(&r->upload_events[k], cudaEventDisableTiming));
+        up.events[k] = r->upload_events[k];
+    }
+    // the previous frame's kernels may still read the scene buffer
+    DL_CK(cudaEventRecord(r->copy_event, r->stream));
+    DL_CK(cudaStreamWaitEvent(r->copy_stream, r->copy_event, 0));
+    int rc = dl_upload_scene(&r->own_scene, data, prec, r->copy_stream, &up);
+    if (rc == DL_OK) rc = render_batch(r, &r->own_scene, cams, n, bg, outs, flags, &up);
+    // every return path leaves no copy running
+    const cudaError_t ce = cudaStreamSynchronize(r->copy_stream);
+    if (rc != DL_OK) return rc;
+    DL_CK(ce);
+    return DL_OK;
 }
 
-extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4],
-                               uint8_t* const* outs, uint32_t flags) {
+namespace {
+
+int render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, const float bg[4], uint8_t* const* outs,
+                 uint32_t flags, const DlUploadChunks* upload) {
     if (!r || !s || !cams || !outs || n < 0) { dl_set_error("dl_render_batch: bad argument"); return DL_E_INVALID_ARG; }
     if (n == 0) return DL_OK;
     if (n > 4096) { dl_set_error("at most 4096 views per batch"); return DL_E_CAPACITY; }
@@ -207,30 +249,25 @@ extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cam
         for (int i = 0; i < n; i++) { dOuts[i] = r->rgba.as<uint32_t>() + off; off += (uint64_t)views[i].W * views[i].H; }
     }
     uint64_t launches = 0;
+    const bool overlapped = !outDev && n >= 8 && !r->profiling && !(flags & DL_BATCH_PLAIN);
+    // an upload still in flight: frames that do not overlap it wait for all of it
+    if (upload && !overlapped) DL_CK(cudaStreamWaitEvent(r->stream, upload->events[upload->count - 1], 0));
     if (flags & DL_BATCH_PLAIN) {
         for (int i = 0; i < n; i++) {
             if ((uint64_t)views[i].W * views[i].H == 0) continue;
             DL_TRY(dl_render_views(r, s->d, &views[i], 1, &dOuts[i], flags & ~DL_BATCH_F16_RECORDS));
             launches += r->launches;
         }
-    } else if (!outDev && n >= 8) {
-        // host outputs: render in four view groups; each group is copied back on
-        // a second stream while the next one renders
-        if (!r->copy_stream) DL_CK(cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking));
-        if (!r->copy_event) DL_CK(cudaEventCreateWithFlags(&r->copy_event, cudaEventDisableTiming));
-        const int per = (n + 3) / 4;
-        for (int g0 = 0; g0 < n; g0 += per) {
-            const int cnt = std::min(per, n - g0);
-            DL_TRY(dl_render_views(r, s->d, &views[g0], (uint32_t)cnt, &dOuts[g0], flags | DL_BATCH_NO_GRAPH));
-            launches += r->launches;
-            DL_CK(cudaEventRecord(r->copy_event, r->stream));
-            DL_CK(cudaStreamWaitEvent(r->copy_stream, r->copy_event, 0));
-            for (int i = g0; i < g0 + cnt; i++)
-                DL_CK(cudaMemcpyAsync(outs[i], dOuts[i], (uint64_t)views[i].W * views[i].H * 4, cudaMemcpyDeviceToHost,
-                                      r->copy_stream));
-        }
-        DL_CK(cudaStreamSynchronize(r->copy_stream));
-        r->launches = launches;
+    } else if (overlapped) {
+        // host outputs: one frame whose rasterizer runs as kReadBackGroups view
+        // ranges; each range is copied back on a second stream while the next
+        // rasterizes
+        DL_TRY(ensure_copy_stream(r));
+        const DlOverlap ov = {kReadBackGroups, outs, r->copy_stream, r->copy_event, upload};
+        const int rc = dl_render_views(r, s->d, views.data(), (uint32_t)n, dOuts.data(), flags, &ov);
+        const cudaError_t ce = cudaStreamSynchronize(r->copy_stream);
+        if (rc != DL_OK) return rc;
+        DL_CK(ce);
         return DL_OK;
     } else {
         DL_TRY(dl_render_views(r, s->d, views.data(), (uint32_t)n, dOuts.data(), flags));
@@ -244,6 +281,8 @@ extern "C" int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cam
     DL_CK(cudaStreamSynchronize(r->stream));
     return DL_OK;
 }
+
+}  // namespace
 
 extern "C" int dl_renderer_set_scheduler(dl_renderer* r, dl_mlp* mlp) {
     if (!r) { dl_set_error("renderer is NULL"); return DL_E_INVALID_ARG; }

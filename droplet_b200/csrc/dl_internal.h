@@ -76,6 +76,9 @@ struct DlTuning {
     int ctas_per_sm = 0;      // persistent rasterizer CTAs per SM; 0 = occupancy limit
 };
 
+constexpr int kUploadChunks = 8;   // splat ranges of an upload that overlaps projection
+constexpr int kReadBackGroups = 8; // view ranges of a rasterizer whose images are read back meanwhile
+
 // Host-side state of the tile-binned renderer.
 struct dl_renderer {
     dl_device* dev = nullptr;
@@ -133,6 +136,7 @@ struct dl_renderer {
     // read-back of host-output batches, overlapped with rendering
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_event = nullptr;
+    cudaEvent_t upload_events[kUploadChunks] = {};
 };
 
 struct dl_mlp;
@@ -140,7 +144,26 @@ int dl_mlp_infer_launch(const dl_mlp* mlp, const float* X, uint32_t n, float* ou
 const void* dl_mlp_weights(const dl_mlp* mlp);   // device BF16 parameters
 
 // dl_render.cu
+// A scene upload issued in splat ranges on a second stream: chunk c holds
+// splats [bounds[c], bounds[c+1]) and is complete when events[c] has fired.
+struct DlUploadChunks {
+    int count;
+    uint32_t bounds[kUploadChunks + 1];
+    cudaEvent_t events[kUploadChunks];
+};
+// Copies that overlap a frame's kernels: projection of each uploaded splat
+// range starts when its chunk has arrived, and the rasterizer runs as `groups`
+// launches over view ranges, each range's images copied to host[v] on `stream`
+// while the next range rasterizes.  The caller synchronises `stream`.
+struct DlOverlap {
+    int groups;
+    uint8_t* const* host;
+    cudaStream_t stream;
+    cudaEvent_t event;
+    const DlUploadChunks* upload;  // NULL: the scene is resident
+};
 int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hviews, uint32_t V,
-                    uint32_t* const* d_outs, uint32_t flags);
-int dl_upload_scene(dl_scene* s, const dl_splats* data, int precision, cudaStream_t stream);
+                    uint32_t* const* d_outs, uint32_t flags, const DlOverlap* overlap = nullptr);
+int dl_upload_scene(dl_scene* s, const dl_splats* data, int precision, cudaStream_t stream,
+                    DlUploadChunks* chunks = nullptr);
 int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlView* out);

@@ -29,7 +29,8 @@ enum {
     SC_OVF = 13,
     SC_SCHED_CTR = 14,     // 4 counters
     SC_SCHED_TILES = 18,
-    SC_DEPTH_TILES2 = 19   // tiles of the depth sort after its first pass
+    SC_DEPTH_TILES2 = 19,  // tiles of the depth sort after its first pass
+    SC_RASTER_CTR = 20     // kReadBackGroups work counters of view-range rasterizer launches
 };
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
@@ -111,7 +112,7 @@ int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlVie
     return DL_OK;
 }
 
-int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t st) {
+int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t st, DlUploadChunks* chunks) {
     if (!d) { dl_set_error("splats is NULL"); return DL_E_INVALID_ARG; }
     if (d->sh_bands < 0 || d->sh_bands > 3) { dl_set_error("sh_bands must be 0..3"); return DL_E_INVALID_ARG; }
     if (d->count >= (1ull << 30)) { dl_set_error("at most 2^30 - 1 splats"); return DL_E_CAPACITY; }
@@ -135,22 +136,41 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
     const uint64_t total = (precision == DL_PREC_F32 || M == 0) ? oTmp : oTmp + (uint64_t)3 * M * n * 4;
     DL_TRY(s->mem.ensure(total));
     char* b = s->mem.as<char>();
-    if (n) {
-        DL_CK(cudaMemcpyAsync(b + oPos, d->positions, 12 * n, cudaMemcpyHostToDevice, st));
-        DL_CK(cudaMemcpyAsync(b + oRot, d->rotations, 16 * n, cudaMemcpyHostToDevice, st));
-        DL_CK(cudaMemcpyAsync(b + oLsc, d->log_scales, 12 * n, cudaMemcpyHostToDevice, st));
-        DL_CK(cudaMemcpyAsync(b + oOpl, d->opacity_logits, 4 * n, cudaMemcpyHostToDevice, st));
-        DL_CK(cudaMemcpyAsync(b + oDc, d->colors_dc, 12 * n, cudaMemcpyHostToDevice, st));
+    // one splat range [g0, g1) of every array
+    auto upload = [&](uint64_t g0, uint64_t g1) -> int {
+        const uint64_t c = g1 - g0;
+        auto h2d = [&](uint64_t off, const void* src, uint64_t elem) {
+            return cudaMemcpyAsync(b + off + elem * g0, (const char*)src + elem * g0, elem * c,
+                                   cudaMemcpyHostToDevice, st);
+        };
+        DL_CK(h2d(oPos, d->positions, 12));
+        DL_CK(h2d(oRot, d->rotations, 16));
+        DL_CK(h2d(oLsc, d->log_scales, 12));
+        DL_CK(h2d(oOpl, d->opacity_logits, 4));
+        DL_CK(h2d(oDc, d->colors_dc, 12));
         if (M) {
             if (precision == DL_PREC_F32) {
-                DL_CK(cudaMemcpyAsync(b + oSh, d->colors_sh, shBytes, cudaMemcpyHostToDevice, st));
+                DL_CK(h2d(oSh, d->colors_sh, 12ull * M));
             } else {
-                DL_CK(cudaMemcpyAsync(b + oTmp, d->colors_sh, (uint64_t)3 * M * n * 4, cudaMemcpyHostToDevice, st));
-                sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp), (uint16_t*)(b + oSh), n, M, (int)P16,
+                DL_CK(h2d(oTmp, d->colors_sh, 12ull * M));
+                sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp) + 3ull * M * g0,
+                                                   (uint16_t*)(b + oSh) + (uint64_t)P16 * g0, c, M, (int)P16,
                                                    precision);
                 DL_CK(cudaGetLastError());
             }
         }
+        return DL_OK;
+    };
+    if (chunks) {
+        // equal splat ranges, each followed by its event
+        chunks->count = kUploadChunks;
+        for (int k = 0; k <= kUploadChunks; k++) chunks->bounds[k] = (uint32_t)(n * (uint64_t)k / kUploadChunks);
+        for (int k = 0; k < kUploadChunks; k++) {
+            if (chunks->bounds[k + 1] > chunks->bounds[k]) DL_TRY(upload(chunks->bounds[k], chunks->bounds[k + 1]));
+            DL_CK(cudaEventRecord(chunks->events[k], st));
+        }
+    } else if (n) {
+        DL_TRY(upload(0, n));
     }
     s->precision = precision;
     s->d.pos = (const float*)(b + oPos);
@@ -197,6 +217,16 @@ struct FramePtrs {
     const uint32_t* work;          // optional tile order for the rasterizer
     uint32_t* tileEvals;           // optional per-tile counters (cost logging)
     uint32_t* tileCycles;
+    // a scene upload still in flight: projection per splat range after its event
+    const DlUploadChunks* upload;
+    // host outputs read back per view range while the next range rasterizes
+    int rbGroups;                  // 0: one rasterizer launch, no read-back here
+    uint8_t* const* rbHost;        // [V] host destinations
+    uint32_t* const* rbDev;        // [V] device images
+    const DlView* rbViews;         // host view table (sizes)
+    const uint32_t* rbTileBase;    // host [V+1] first global tile of each view
+    cudaStream_t rbStream;
+    cudaEvent_t rbEvent;
     // learned schedule: features -> MLP -> longest-first tile order
     float* feat;                   // [total tiles][12], or NULL
     float* pred;
@@ -299,7 +329,20 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
     pa.nvis = f.nvis;
     pa.f64_degenerate = d.f64deg ? 1 : 0;
     pa.cull_offscreen = d.cullOff ? 1 : 0;
-    if (d.N) {
+    pa.g_begin = 0;
+    pa.g_end = d.N;
+    if (f.upload) {
+        for (int k = 0; k < f.upload->count; k++) {
+            DL_CK(cudaStreamWaitEvent(st, f.upload->events[k], 0));
+            pa.g_begin = f.upload->bounds[k];
+            pa.g_end = f.upload->bounds[k + 1];
+            if (pa.g_end > pa.g_begin) {
+                dlr::project_k<<<(pa.g_end - pa.g_begin + 255) / 256, 256, 0, st>>>(pa);
+                (*launches)++;
+                DL_CK(cudaGetLastError());
+            }
+        }
+    } else if (d.N) {
         dlr::project_k<<<(d.N + 255) / 256, 256, 0, st>>>(pa);
         (*launches)++;
     }
@@ -466,6 +509,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.outs = f.outs;
     ra.accum = f.accum;
     ra.work = work;
+    ra.item_base = 0;
     ra.num_items = (d.ppl2 ? 4u : 8u) * d.totalTiles;
     ra.work_counter = f.scr + SC_WORK_CTR;
     ra.eval_count = f.evalCount;
@@ -474,22 +518,49 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     ra.sub_lw = d.subLw;
     ra.rec_box = d.cullOff ? 1 : 0;
     const bool count = ra.eval_count || ra.tile_evals;
-    if (d.ppl2) {
-        if (d.fastExp) {
-            if (count) dlr::rasterize2_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
-            else dlr::rasterize2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+    auto raster = [&](const dlr::RasterArgs& x) {
+        if (d.ppl2) {
+            if (d.fastExp) {
+                if (count) dlr::rasterize2_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                else dlr::rasterize2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            } else {
+                if (count) dlr::rasterize2_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                else dlr::rasterize2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            }
+        } else if (d.fastExp) {
+            if (count) dlr::rasterize_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            else dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
         } else {
-            if (count) dlr::rasterize2_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
-            else dlr::rasterize2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+            if (count) dlr::rasterize_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
         }
-    } else if (d.fastExp) {
-        if (count) dlr::rasterize_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
-        else dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+        (*launches)++;
+    };
+    if (f.rbGroups > 1 && d.V > 1) {
+        // One launch per view range (the work queue is view-major in both
+        // orders, so a range of views is a range of items); each range's images
+        // go back to the host on the read-back stream while the next rasterizes.
+        const uint32_t per = (d.V + (uint32_t)f.rbGroups - 1) / (uint32_t)f.rbGroups;
+        const uint32_t ipt = d.ppl2 ? 4u : 8u;
+        static_assert(SC_RASTER_CTR + kReadBackGroups <= kScratchWords, "scratch words");
+        DL_CK(cudaMemsetAsync(f.scr + SC_RASTER_CTR, 0, 4ull * kReadBackGroups, st));
+        for (uint32_t v0 = 0, g = 0; v0 < d.V; v0 += per, g++) {
+            const uint32_t v1 = std::min(d.V, v0 + per);
+            dlr::RasterArgs x = ra;
+            x.item_base = ipt * f.rbTileBase[v0];
+            x.num_items = ipt * f.rbTileBase[v1];
+            x.work_counter = f.scr + SC_RASTER_CTR + g;      // g < rbGroups <= kReadBackGroups
+            raster(x);
+            DL_CK(cudaGetLastError());
+            DL_CK(cudaEventRecord(f.rbEvent, st));
+            DL_CK(cudaStreamWaitEvent(f.rbStream, f.rbEvent, 0));
+            for (uint32_t v = v0; v < v1; v++)
+                DL_CK(cudaMemcpyAsync(f.rbHost[v], f.rbDev[v], (uint64_t)f.rbViews[v].W * f.rbViews[v].H * 4,
+                                      cudaMemcpyDeviceToHost, f.rbStream));
+        }
     } else {
-        if (count) dlr::rasterize_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
-        else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(ra);
+        raster(ra);
     }
-    (*launches)++;
     DL_CK(cudaGetLastError());
     rec_event(ev, 7, st);
     *finalVals = vals;
@@ -499,7 +570,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
 }  // namespace
 
 int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint32_t V, uint32_t* const* d_outs,
-                    uint32_t flags) {
+                    uint32_t flags, const DlOverlap* overlap) {
     cudaStream_t st = r->stream;
     const uint32_t N = sc.n;
     if (r->pair_cap_per_view == 0) r->pair_cap_per_view = std::max<uint64_t>(1u << 20, 4ull * N);
@@ -627,8 +698,23 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     DL_CK(cudaMemcpyAsync(f.outs, hOuts, sizeof(void*) * V, cudaMemcpyHostToDevice, st));
     cudaEvent_t* ev = r->profiling ? r->ev : nullptr;
     f.sortStatus = r->sortStatus.as<uint32_t>();
+    // frames that overlap copies with their kernels run outside a graph
+    std::vector<uint32_t> rbTileBase;
+    if (overlap) {
+        f.upload = overlap->upload;
+        if (overlap->groups > 1 && V > 1) {
+            rbTileBase.assign(hTileBase, hTileBase + V + 1);
+            f.rbGroups = std::min(overlap->groups, kReadBackGroups);
+            f.rbHost = overlap->host;
+            f.rbDev = d_outs;
+            f.rbViews = hv;
+            f.rbTileBase = rbTileBase.data();
+            f.rbStream = overlap->stream;
+            f.rbEvent = overlap->event;
+        }
+    }
     const bool useGraph = !(flags & DL_BATCH_NO_GRAPH) && !(flags & DL_BATCH_PLAIN) && V > 1 && !r->profiling &&
-                          st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+                          !overlap && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
 
     for (int attempt = 0; attempt < 3; attempt++) {
         const uint64_t cap = r->pair_cap_per_view;

@@ -38,6 +38,7 @@ struct ProjectArgs {
     uint32_t* nvis;           // [V] visible count
     int f64_degenerate;       // recompute det / conic / AA factor in f64 for near-degenerate splats
     int cull_offscreen;       // also cull splats with no tile on the image (no pair can touch a pixel)
+    uint32_t g_begin, g_end;  // this launch projects splats [g_begin, g_end)
 };
 
 // A 2D covariance is near-degenerate when its f32 determinant has lost at
@@ -203,8 +204,8 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
     }
     __syncthreads();
     const DlView* vtab = staged ? s_views : a.views;
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool inRange = g < a.sc.n;
+    const uint32_t g = a.g_begin + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool inRange = g < a.g_end;
     float pos[3] = {0, 0, 0}, rot[4] = {1, 0, 0, 0}, s[3] = {1, 1, 1}, dc[3] = {0, 0, 0}, opl = 0.0f;
     if (inRange) {
         pos[0] = __ldg(a.sc.pos + 3ull * g); pos[1] = __ldg(a.sc.pos + 3ull * g + 1); pos[2] = __ldg(a.sc.pos + 3ull * g + 2);
@@ -773,7 +774,8 @@ struct RasterArgs {
     uint32_t* const* outs;         // [V] packed RGBA8 per pixel
     float4* accum;                 // optional [W*H] (single view debug)
     const uint32_t* work;          // optional tile order (global tile ids); NULL: natural order
-    uint32_t num_items;            // 8 x total tiles
+    uint32_t item_base;            // this launch takes items [item_base, num_items)
+    uint32_t num_items;            // 8 x total tiles (4 with two pixels per lane), or a view range's end
     uint32_t* work_counter;
     unsigned long long* eval_count;   // optional: total evaluated (pixel, splat) pairs
     uint32_t* tile_evals;          // optional [total tiles] evaluated pairs per tile
@@ -1139,7 +1141,7 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize2_k(RasterArgs a) 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     while (true) {
         uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        if (lane == 0) item = a.item_base + atomicAdd(a.work_counter, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= a.num_items) return;
         const uint32_t gt = a.work ? a.work[item >> 2] : (item >> 2);
@@ -1157,7 +1159,7 @@ __global__ void __launch_bounds__(kRasterThreads, 6) rasterize_k(RasterArgs a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     while (true) {
         uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        if (lane == 0) item = a.item_base + atomicAdd(a.work_counter, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= a.num_items) return;
         const uint32_t gt = a.work ? a.work[item >> 3] : (item >> 3);

@@ -147,9 +147,12 @@ int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, c
 /* Renderer.render(data, camera, bg) (src/render/pipeline.ts:181-426) for n
  * cameras of one host SplatData in one call: the splats are uploaded into the
  * renderer's own grow-only scene buffer, all views are rendered as one batch,
- * and each RGBA8 image is copied to outs[i] (host memory).  With host outputs
- * and 8 or more views, dl_render_batch renders the views in four groups and
- * copies each group back on a second stream while the next one renders. */
+ * and each RGBA8 image is copied to outs[i] (host memory).  With 8 or more
+ * views the copies overlap the frame on a second stream: the splats upload in
+ * 8 ranges, each projected as soon as it has arrived, and the rasterizer runs
+ * over 8 view ranges, each range's images copied back while the next range
+ * rasterizes (dl_render_batch with host outputs and 8+ views does the same
+ * read-back). */
 int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
                    uint8_t* const* outs, uint32_t flags);
 

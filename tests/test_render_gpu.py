@@ -243,9 +243,11 @@ def renderer_single(device, d, cam):
 
 
 def test_render_many_groups_and_sh16_match_the_batch(device):
-    # host outputs of 8+ views are rendered in groups with overlapped read-back;
-    # DL_BATCH_SH16 keeps the uploaded SH in f16 like a Scene uploaded as "f16"
-    d = synth.cluster_scene(120_000, seed=17, clusters=24, extent=10.0, bands=3)
+    # host outputs of 8+ views: the scene uploads in four splat ranges, each
+    # projected when it has arrived, and the rasterizer runs per view range with
+    # overlapped read-back; DL_BATCH_SH16 keeps the uploaded SH in f16 like a
+    # Scene uploaded as "f16".  The splat count is not a multiple of 4.
+    d = synth.cluster_scene(120_003, seed=17, clusters=24, extent=10.0, bands=3)
     cams = synth.ring_cameras(10, resolutions=[(320, 180), (200, 120), (640, 360)])
     r2 = dl.Renderer(device)
     sc32, sc16 = r2.upload(d), r2.upload(d, "f16")
@@ -258,6 +260,13 @@ def test_render_many_groups_and_sh16_match_the_batch(device):
     ref16 = r2.render_batch(sc16, cams[:5], flags=fl) + r2.render_batch(sc16, cams[5:], flags=fl)
     got16 = r2.render_many(d, cams, flags=fl | _lib.DL_BATCH_SH16)
     for a, b in zip(ref16, got16):
+        assert np.array_equal(a, b)
+    fl |= _lib.DL_BATCH_CULL_OFFSCREEN
+    got = r2.render_batch(sc16, cams, flags=fl)
+    for a, b in zip(ref16, got):
+        assert np.array_equal(a, b)
+    got = r2.render_many(d, cams, flags=fl | _lib.DL_BATCH_SH16)
+    for a, b in zip(ref16, got):
         assert np.array_equal(a, b)
 
 
