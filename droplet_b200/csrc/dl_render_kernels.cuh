@@ -355,13 +355,25 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
         uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
         uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        const float alpha = (sig * radiusFade) * aaFactor;
         float boxX = radius, boxY = radius;          // half-extents the rasterizer tests (cull mode)
+        // the rasterizer's alpha is opacity * (exp(-q/2) - exp(-4.5)) with the
+        // opacity as stored; below 1/255 it is skipped
+        const float alSt = a.recBC ? alpha : __half2float(__float2half_rn(alpha));
+        if (a.cull_offscreen && alSt * (1.0f - DL_GAUSS_FLOOR) < 0.999f * DL_MIN_ALPHA) {
+            // alpha < 1/255 at every pixel (exp(-q/2) <= 1): no pixel composites it
+            a.keys[o] = 0xffffffffu;
+            continue;
+        }
         if (a.cull_offscreen && maxTX >= minTX && maxTY >= minTY &&
             (maxTX - minTX + 1u) * (maxTY - minTY + 1u) <= u.maxCoverage) {
-            // Bin by the box of the ellipse q <= 9.5 (q: the rasterizer's quadratic
-            // form, from the conic as it is stored) when the reference's square
-            // box is not truncated: its other tiles hold only pixels with q > 9,
-            // where alpha < 1/255 is skipped.
+            // Bin by the box of the ellipse q <= level (q: the rasterizer's
+            // quadratic form, from the conic as it is stored) when the reference's
+            // square box is not truncated.  Outside it alpha < 1/255 is skipped:
+            // q > 9 gives exp(-q/2) < exp(-4.5); and alpha >= 1/255 needs
+            // q <= qa = -2 ln(exp(-4.5) + 1/(255 opacity)).  The level takes qa
+            // with 0.2% + 0.01 to spare, which keeps alpha at least 0.5% below
+            // 1/255 outside the box, far above the f32 error of q and exp.
             float cA = conicA, cB = conicB, cC = conicC;
             if (!a.recBC) {
                 cA = __half2float(__float2half_rn(cA));
@@ -370,7 +382,9 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             }
             const float ac = cA * cC, dt = ac - cB * cB;
             if (dt > 0.0f && ac <= 1024.0f * dt) {
-                const float s = 9.5f / dt;
+                const float qa = -2.0f * logf(DL_GAUSS_FLOOR + DL_MIN_ALPHA / alSt);
+                const float level = fmaxf(0.0f, fminf(9.5f, 1.002f * qa + 0.01f));
+                const float s = level / dt;
                 const float ex = fminf(radius, sqrtf(cC * s)), ey = fminf(radius, sqrtf(cA * s));
                 boxX = ex;
                 boxY = ey;
@@ -412,7 +426,6 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         col0 = fmaxf(col0 + 0.5f, 0.0f);
         col1 = fmaxf(col1 + 0.5f, 0.0f);
         col2 = fmaxf(col2 + 0.5f, 0.0f);
-        const float alpha = (sig * radiusFade) * aaFactor;
         // cull mode: the screen record carries the half-extents of the box the
         // rasterizer tests (the ellipse's box, or the radius square) instead of
         // (radius, depth), which it does not read there

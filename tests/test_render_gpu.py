@@ -270,10 +270,14 @@ def test_render_many_groups_and_sh16_match_the_batch(device):
         assert np.array_equal(a, b)
 
 
-def test_offscreen_cull_changes_no_pixel(device, renderer):
-    # splats whose tile box misses the image (or only has phantom tiles) leave
-    # the depth order; every tile list keeps its order, so pixels are unchanged
-    d = synth.cluster_scene(150_000, seed=19, clusters=32, extent=10.0, bands=2)
+@pytest.mark.parametrize("op_mu", [0.0, -3.0])
+def test_offscreen_cull_changes_no_pixel(device, renderer, op_mu):
+    # splats whose tile box misses the image (or only has phantom tiles), or
+    # whose opacity keeps alpha below 1/255 everywhere, leave the depth order;
+    # the others are binned by the box of the ellipse outside which their alpha
+    # is below 1/255 (smaller for lower opacity).  Every tile list keeps its
+    # order, so pixels are unchanged.  op_mu -3: most opacities below 0.1.
+    d = synth.cluster_scene(150_000, seed=19, clusters=32, extent=10.0, bands=2, op_mu=op_mu)
     cams = synth.ring_cameras(5, resolutions=[(320, 180), (500, 280)]) + [synth.pinhole(256, 256, (0.0, 0.0, 0.5))]
     r2 = dl.Renderer(device)
     sc = r2.upload(d)
