@@ -481,9 +481,11 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     if (f.sched && d.totalTiles) {
         const uint32_t g = std::min<uint32_t>((d.totalTiles + dlr::kSchedThreads - 1) / dlr::kSchedThreads, 2048);
         DL_CK(cudaMemsetAsync(f.shist, 0, 4ull * 256 * d.V, st));
+        // the views that end a rasterizer launch are reordered
+        const uint32_t tailEvery = f.rbGroups > 1 ? (d.V + (uint32_t)f.rbGroups - 1) / (uint32_t)f.rbGroups : d.V;
         dlr::sched_pred_k<<<g, dlr::kSchedThreads, 0, st>>>(f.views, d.V, f.tileBase, f.tileOff, d.TS, d.totalTiles,
                                                             (const __nv_bfloat16*)dl_mlp_weights(f.sched), f.svals1,
-                                                            f.shist);
+                                                            f.shist, tailEvery, f.svals0);
         dlr::sched_scan_k<<<d.V, 32, 0, st>>>(f.tileBase, f.shist);
         dlr::sched_scatter_k<<<std::min<uint32_t>((d.totalTiles + 255) / 256, 2048), 256, 0, st>>>(
             f.svals1, d.totalTiles, f.shist, f.svals0);

@@ -717,13 +717,23 @@ __global__ void tile_features_k(const DlView* views, uint32_t V, const uint32_t*
 // predicted cost, counted per view; sched_scan_k: per view, bucket offsets
 // after the view's first tile; sched_scatter_k: tiles into the work list by
 // bucket.  Views keep their launch order (their tiles share splat records in
-// L2); inside a view tiles go most expensive bucket first, and inside a bucket
-// in whatever order the atomics give — any order yields the same pixels.
+// L2).  Only the view that ends a rasterizer launch (every `tail_every`-th
+// view, and the last) is reordered: its tiles end the launch's queue, where
+// the most expensive ones go first so that no long tile is left for the end;
+// inside a bucket they go in whatever order the atomics give.  Every other
+// view keeps its natural order (identity entries), which keeps neighbouring
+// tiles, and the splat records they share, together in L2.  Any order yields
+// the same pixels.
 constexpr int kSchedThreads = 128;
+constexpr uint32_t kSchedKeep = 0xffffffffu;     // bucket word of a tile in natural order
+__device__ __forceinline__ bool sched_reordered(uint32_t v, uint32_t V, uint32_t tail_every) {
+    return v + 1 == V || (v + 1) % tail_every == 0;
+}
 __global__ void __launch_bounds__(kSchedThreads) sched_pred_k(const DlView* views, uint32_t V, const uint32_t* tile_base,
                                                               const uint32_t* tile_off, uint32_t tile_stride,
                                                               uint32_t total, const __nv_bfloat16* w,
-                                                              uint32_t* __restrict__ bucket, uint32_t* __restrict__ vhist) {
+                                                              uint32_t* __restrict__ bucket, uint32_t* __restrict__ vhist,
+                                                              uint32_t tail_every, uint32_t* __restrict__ work) {
     __shared__ float P[dlmlp::kParams];
     dlmlp::load_params(w, P);
     for (uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x; gt < total; gt += gridDim.x * blockDim.x) {
@@ -731,6 +741,11 @@ __global__ void __launch_bounds__(kSchedThreads) sched_pred_k(const DlView* view
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
             if (tile_base[mid] <= gt) lo = mid; else hi = mid;
+        }
+        if (!sched_reordered(lo, V, tail_every)) {
+            bucket[gt] = kSchedKeep;
+            work[gt] = gt;
+            continue;
         }
         float x[12];
         tile_features(views[lo], tile_off + (uint64_t)lo * tile_stride, gt - tile_base[lo], x);
@@ -754,6 +769,7 @@ __global__ void sched_scatter_k(const uint32_t* __restrict__ bucket, uint32_t to
                                 uint32_t* __restrict__ work) {
     for (uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x; gt < total; gt += gridDim.x * blockDim.x) {
         const uint32_t vb = bucket[gt];
+        if (vb == kSchedKeep) continue;
         work[atomicAdd(&vhist[(vb >> 8) * 256 + (vb & 255u)], 1u)] = gt;
     }
 }

@@ -49,17 +49,23 @@ def training_cameras(seed: int, count: int = 40):
     return cams
 
 
-def collect(renderer: Renderer, seeds=TRAIN_SEEDS, splats: int = 3_000_000, views: int = 40, log=print):
-    """Render every training view alone (plain path) and log its tiles."""
+HEADLINE_FLAGS = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP | _lib.DL_BATCH_CULL_OFFSCREEN
+
+
+def collect(renderer: Renderer, seeds=TRAIN_SEEDS, splats: int = 3_000_000, views: int = 40, log=print,
+            mode: str = "plain"):
+    """Render every training view alone and log its tiles: the plain path
+    (mode "plain") or the batched path's arithmetic and cull mode on an f16
+    scene (mode "headline")."""
     import torch
     X, Y, S = [], [], []
     out = torch.empty(2560 * 1440 * 4, dtype=torch.uint8, device="cuda")
+    flags = (_lib.DL_BATCH_PLAIN if mode == "plain" else HEADLINE_FLAGS) | _lib.DL_BATCH_LOG_TILES
     for seed in seeds:
         t = time.time()
-        scene = renderer.upload(synth.sh3_3m(splats, seed=seed))
+        scene = renderer.upload(synth.sh3_3m(splats, seed=seed), "f32" if mode == "plain" else "f16")
         for cam in training_cameras(seed, views):
-            renderer.render_batch(scene, [cam], flags=_lib.DL_BATCH_PLAIN | _lib.DL_BATCH_LOG_TILES,
-                                  outs=[out.data_ptr()])
+            renderer.render_batch(scene, [cam], flags=flags, outs=[out.data_ptr()])
             f, c = renderer.tile_log()
             X.append(f)
             Y.append(np.log1p(c))
@@ -130,6 +136,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--out", default=None)
     ap.add_argument("--voxel", action="store_true", help="train the voxelizer's block-cost model")
+    ap.add_argument("--mode", choices=("plain", "headline"), default="plain",
+                    help="tile costs logged on the plain path or on the batched path's flags")
     a = ap.parse_args()
     dev = createDevice()
     t = time.time()
@@ -137,7 +145,7 @@ def main():
         X, y, seeds = collect_voxel(dev)
         out = a.out or VOXEL_MODEL_PATH
     else:
-        X, y, seeds = collect(Renderer(dev), splats=a.splats, views=a.views)
+        X, y, seeds = collect(Renderer(dev), splats=a.splats, views=a.views, mode=a.mode)
         out = a.out or MODEL_PATH
     t_collect = time.time() - t
     val = seeds == TRAIN_SEEDS[-1]                  # held-out seed for the prediction error
@@ -147,7 +155,7 @@ def main():
     t_train = time.time() - t
     pred = mlp.predict(X[val]) * sd + mu
     err = pred - y[val]
-    meta = {"samples": int(len(y)), "train_samples": int((~val).sum()), "val_seed": TRAIN_SEEDS[-1],
+    meta = {"mode": "voxel" if a.voxel else a.mode, "samples": int(len(y)), "train_samples": int((~val).sum()), "val_seed": TRAIN_SEEDS[-1],
             "epochs": a.epochs, "final_loss": loss, "y_mean": mu, "y_std": sd,
             "val_rmse_log_cost": float(np.sqrt((err ** 2).mean())),
             "val_spearman": spearman(pred, y[val]),
