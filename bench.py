@@ -411,8 +411,8 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": world * pix * half / (ems / 1e3) / 1e6, "unit": "Mpix/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(pix * 4),
                "call": "dl_render_many (host SplatData -> host RGBA8; SH kept in f16 on the device, "
-                       "upload overlapped with projection in 8 splat ranges, read-back with the "
-                       "rasterizer in 8 view ranges)"}
+                       "geometry upload overlapped with projection in 8 splat ranges, SH upload with the "
+                       "sorts and binning (colours deferred), read-back with the rasterizer in 8 view ranges)"}
         r2.destroy()
 
     if rank != 0:

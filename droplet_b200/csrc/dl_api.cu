@@ -79,7 +79,8 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
                       &r->sortStatus, &r->pairBase, &r->pairCap, &r->pkeys0, &r->pkeys1, &r->pvals0, &r->pvals1,
                       &r->npairs, &r->emitStatus, &r->tileCount, &r->tileOff, &r->pairSegLen, &r->pairSegTileBase,
                       &r->pairGlob, &r->outs, &r->accum, &r->tileEvals, &r->work, &r->rgba, &r->evalCount, &r->own_scene.mem, &r->feat, &r->pred,
-                      &r->skeys0, &r->skeys1, &r->svals0, &r->svals1, &r->sseg, &r->sstatus, &r->shist, &r->tileCycles};
+                      &r->skeys0, &r->skeys1, &r->svals0, &r->svals1, &r->sseg, &r->sstatus, &r->shist, &r->tileCycles,
+                      &r->visMask};
     for (DevBuf* b : bufs) b->release();
     r->tuneOut.release();
     if (r->copy_stream) { cudaStreamSynchronize(r->copy_stream); cudaStreamDestroy(r->copy_stream); }
@@ -208,13 +209,14 @@ extern "C" int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_ca
     // each range starts when it has arrived
     DL_TRY(ensure_copy_stream(r));
     DlUploadChunks up;
-    for (int k = 0; k < kUploadChunks; k++) {
+    for (int k = 0; k <= kUploadChunks; k++)
         if (!r->upload_events[k]) DL_CK(cudaEventCreateWithFlags(&r->upload_events[k], cudaEventDisableTiming));
-        up.events[k] = r->upload_events[k];
-    }
+    for (int k = 0; k < kUploadChunks; k++) up.events[k] = r->upload_events[k];
+    up.sh_event = r->upload_events[kUploadChunks];
     // the previous frame's kernels may still read the scene buffer
     DL_CK(cudaEventRecord(r->copy_event, r->stream));
     DL_CK(cudaStreamWaitEvent(r->copy_stream, r->copy_event, 0));
+    // lays the scene out; the frame issues the copies (up.issue)
     int rc = dl_upload_scene(&r->own_scene, data, prec, r->copy_stream, &up);
     if (rc == DL_OK) rc = render_batch(r, &r->own_scene, cams, n, bg, outs, flags, &up);
     // every return path leaves no copy running
@@ -251,7 +253,11 @@ int render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, cons
     uint64_t launches = 0;
     const bool overlapped = !outDev && n >= 8 && !r->profiling && !(flags & DL_BATCH_PLAIN);
     // an upload still in flight: frames that do not overlap it wait for all of it
-    if (upload && !overlapped) DL_CK(cudaStreamWaitEvent(r->stream, upload->events[upload->count - 1], 0));
+    if (upload && !overlapped) {
+        if (!upload->issued) DL_TRY(upload->issue());
+        DL_CK(cudaStreamWaitEvent(r->stream, upload->events[upload->count - 1], 0));
+        if (upload->sh_separate) DL_CK(cudaStreamWaitEvent(r->stream, upload->sh_event, 0));
+    }
     if (flags & DL_BATCH_PLAIN) {
         for (int i = 0; i < n; i++) {
             if ((uint64_t)views[i].W * views[i].H == 0) continue;

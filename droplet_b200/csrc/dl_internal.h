@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "../../include/droplet_b200.h"
@@ -127,6 +128,7 @@ struct dl_renderer {
 
     // learned schedule and tile-cost logging
     dl_mlp* sched = nullptr;
+    DevBuf visMask;           // deferred-colour record bits [ceil(V/32)][N]
     DevBuf feat, pred, skeys0, skeys1, svals0, svals1, sseg, sstatus, shist, tileCycles;
     uint32_t log_tiles = 0;
 
@@ -136,7 +138,7 @@ struct dl_renderer {
     // read-back of host-output batches, overlapped with rendering
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_event = nullptr;
-    cudaEvent_t upload_events[kUploadChunks] = {};
+    cudaEvent_t upload_events[kUploadChunks + 1] = {};   // geometry chunks, then the SH
 };
 
 struct dl_mlp;
@@ -146,10 +148,19 @@ const void* dl_mlp_weights(const dl_mlp* mlp);   // device BF16 parameters
 // dl_render.cu
 // A scene upload issued in splat ranges on a second stream: chunk c holds
 // splats [bounds[c], bounds[c+1]) and is complete when events[c] has fired.
+// With SH bands, the SH coefficients follow the geometry of all chunks,
+// complete when sh_event has fired (sh_separate = 1), so that frames can defer
+// colours until then.  dl_upload_scene lays the scene out and returns; the
+// frame calls issue() once its own small host-to-device copies are queued, so
+// that they do not wait behind the upload.
 struct DlUploadChunks {
     int count;
     uint32_t bounds[kUploadChunks + 1];
     cudaEvent_t events[kUploadChunks];
+    int sh_separate;
+    cudaEvent_t sh_event;
+    std::function<int()> issue;
+    bool issued = false;
 };
 // Copies that overlap a frame's kernels: projection of each uploaded splat
 // range starts when its chunk has arrived, and the rasterizer runs as `groups`

@@ -136,8 +136,9 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
     const uint64_t total = (precision == DL_PREC_F32 || M == 0) ? oTmp : oTmp + (uint64_t)3 * M * n * 4;
     DL_TRY(s->mem.ensure(total));
     char* b = s->mem.as<char>();
-    // one splat range [g0, g1) of every array
-    auto upload = [&](uint64_t g0, uint64_t g1) -> int {
+    // one splat range [g0, g1) of every array (the SH too when withSh)
+    // (by value: a chunked upload runs from chunks->issue after this returns)
+    auto upload = [=](uint64_t g0, uint64_t g1, bool withSh) -> int {
         const uint64_t c = g1 - g0;
         auto h2d = [&](uint64_t off, const void* src, uint64_t elem) {
             return cudaMemcpyAsync(b + off + elem * g0, (const char*)src + elem * g0, elem * c,
@@ -148,7 +149,7 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
         DL_CK(h2d(oLsc, d->log_scales, 12));
         DL_CK(h2d(oOpl, d->opacity_logits, 4));
         DL_CK(h2d(oDc, d->colors_dc, 12));
-        if (M) {
+        if (M && withSh) {
             if (precision == DL_PREC_F32) {
                 DL_CK(h2d(oSh, d->colors_sh, 12ull * M));
             } else {
@@ -162,15 +163,44 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
         return DL_OK;
     };
     if (chunks) {
-        // equal splat ranges, each followed by its event
+        // the geometry in equal splat ranges, each followed by its event; then
+        // the SH of all splats (the bulk of the bytes), followed by sh_event
         chunks->count = kUploadChunks;
+        chunks->sh_separate = M > 0;
+        chunks->issued = false;
         for (int k = 0; k <= kUploadChunks; k++) chunks->bounds[k] = (uint32_t)(n * (uint64_t)k / kUploadChunks);
-        for (int k = 0; k < kUploadChunks; k++) {
-            if (chunks->bounds[k + 1] > chunks->bounds[k]) DL_TRY(upload(chunks->bounds[k], chunks->bounds[k + 1]));
-            DL_CK(cudaEventRecord(chunks->events[k], st));
-        }
+        chunks->issue = [=]() -> int {
+            for (int k = 0; k < kUploadChunks; k++) {
+                if (chunks->bounds[k + 1] > chunks->bounds[k])
+                    DL_TRY(upload(chunks->bounds[k], chunks->bounds[k + 1], false));
+                DL_CK(cudaEventRecord(chunks->events[k], st));
+            }
+            if (M) {
+                // in the same ranges: copies issued later on other streams (a
+                // frame's view tables) queue behind one copy at most
+                for (int k = 0; k < kUploadChunks; k++) {
+                    const uint64_t g0 = chunks->bounds[k], g1 = chunks->bounds[k + 1];
+                    if (g1 == g0) continue;
+                    const uint64_t e = 12ull * M;
+                    if (precision == DL_PREC_F32) {
+                        DL_CK(cudaMemcpyAsync(b + oSh + e * g0, (const char*)d->colors_sh + e * g0, e * (g1 - g0),
+                                              cudaMemcpyHostToDevice, st));
+                    } else {
+                        DL_CK(cudaMemcpyAsync(b + oTmp + e * g0, (const char*)d->colors_sh + e * g0, e * (g1 - g0),
+                                              cudaMemcpyHostToDevice, st));
+                        sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp) + 3ull * M * g0,
+                                                           (uint16_t*)(b + oSh) + (uint64_t)P16 * g0, g1 - g0, M,
+                                                           (int)P16, precision);
+                        DL_CK(cudaGetLastError());
+                    }
+                }
+                DL_CK(cudaEventRecord(chunks->sh_event, st));
+            }
+            chunks->issued = true;
+            return DL_OK;
+        };
     } else if (n) {
-        DL_TRY(upload(0, n));
+        DL_TRY(upload(0, n, true));
     }
     s->precision = precision;
     s->d.pos = (const float*)(b + oPos);
@@ -219,6 +249,7 @@ struct FramePtrs {
     uint32_t* tileCycles;
     // a scene upload still in flight: projection per splat range after its event
     const DlUploadChunks* upload;
+    uint32_t* visMask;             // colours deferred until the SH has arrived (upload->sh_event)
     // host outputs read back per view range while the next range rasterizes
     int rbGroups;                  // 0: one rasterizer launch, no read-back here
     uint8_t* const* rbHost;        // [V] host destinations
@@ -331,6 +362,7 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
     pa.cull_offscreen = d.cullOff ? 1 : 0;
     pa.g_begin = 0;
     pa.g_end = d.N;
+    pa.vis_mask = f.visMask;
     if (f.upload) {
         for (int k = 0; k < f.upload->count; k++) {
             DL_CK(cudaStreamWaitEvent(st, f.upload->events[k], 0));
@@ -388,8 +420,8 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
 
 // emit -> pair digits -> pair sort -> boundaries -> rasterize.  Expects
 // pairBase / pairCap uploaded.  *finalVals receives the sorted pair values.
-int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEvent_t* ev, uint64_t* launches,
-                uint32_t** finalVals) {
+int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cudaStream_t st, cudaEvent_t* ev,
+                uint64_t* launches, uint32_t** finalVals) {
     DL_CK(cudaMemsetAsync(f.pairHist, 0, 4ull * d.V * 4 * 256, st));
     DL_CK(cudaMemsetAsync(f.emitStatus, 0, 8ull * d.V * d.emitTilesPerView, st));
     DL_CK(cudaMemsetAsync(f.scr + SC_EMIT_CTR, 0, 4ull * 6, st));   // emit + pair counters + work counter
@@ -469,6 +501,22 @@ int launch_back(const FramePtrs& f, const FrameDims& d, cudaStream_t st, cudaEve
     dlr::boundaries_k<<<dim3(bgrid, d.V), 256, 0, st>>>(ba);
     (*launches)++;
     DL_CK(cudaGetLastError());
+
+    // deferred colours, once the SH has arrived
+    if (f.visMask && d.N) {
+        DL_CK(cudaStreamWaitEvent(st, f.upload->sh_event, 0));
+        dlr::ColourArgs ca;
+        ca.sc = sc;
+        ca.views = f.views;
+        ca.num_views = d.V;
+        ca.view_stride = d.stride;
+        ca.vis_mask = f.visMask;
+        ca.recBC = d.f16rec ? nullptr : f.recBC;
+        ca.recH = d.f16rec ? f.recH : nullptr;
+        dlr::colour_k<<<(d.N + 255) / 256, 256, 0, st>>>(ca);
+        (*launches)++;
+        DL_CK(cudaGetLastError());
+    }
 
     // learned schedule: per-tile features, predicted cost, tiles in decreasing order
     const uint32_t* work = f.work;
@@ -704,6 +752,10 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     std::vector<uint32_t> rbTileBase;
     if (overlap) {
         f.upload = overlap->upload;
+        if (f.upload && f.upload->sh_separate) {
+            DL_TRY(r->visMask.ensure(4ull * ((V + 31) / 32) * std::max<uint32_t>(N, 1)));
+            f.visMask = r->visMask.as<uint32_t>();
+        }
         if (overlap->groups > 1 && V > 1) {
             rbTileBase.assign(hTileBase, hTileBase + V + 1);
             f.rbGroups = std::min(overlap->groups, kReadBackGroups);
@@ -734,6 +786,8 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         for (uint32_t v = 0; v < V; v++) { r->h_u64[v] = (uint64_t)v * cap; r->h_u64[V + v] = cap; }
         DL_CK(cudaMemcpyAsync(f.pairBase, r->h_u64, 8ull * V, cudaMemcpyHostToDevice, st));
         DL_CK(cudaMemcpyAsync(f.pairCap, r->h_u64 + V, 8ull * V, cudaMemcpyHostToDevice, st));
+        // a pending scene upload goes behind this frame's small copies
+        if (f.upload && !f.upload->issued) DL_TRY(f.upload->issue());
         uint32_t* finalVals = nullptr;
         // the device sequence of the frame: clears, project, depth sort, pair stages
         auto sequence = [&]() -> int {
@@ -743,7 +797,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             if (f.tileCycles) DL_CK(cudaMemsetAsync(f.tileCycles, 0, 4ull * d.totalTiles, st));
             uint64_t n = 0;
             DL_TRY(launch_front(f, d, sc, st, ev, &n));
-            DL_TRY(launch_back(f, d, st, ev, &n, &finalVals));
+            DL_TRY(launch_back(f, d, sc, st, ev, &n, &finalVals));
             r->launches = n;
             return DL_OK;
         };
@@ -989,7 +1043,7 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     uint64_t launches = 0;
     uint32_t* finalVals = nullptr;
     DL_TRY(launch_front(f, d, sc, st, nullptr, &launches));
-    DL_TRY(launch_back(f, d, st, nullptr, &launches, &finalVals));
+    DL_TRY(launch_back(f, d, sc, st, nullptr, &launches, &finalVals));
 
     uint32_t flagsH[2] = {0, 0};
     DL_CK(cudaMemcpyAsync(&flagsH[0], f.scr + SC_ERR, 4, cudaMemcpyDeviceToHost, st));

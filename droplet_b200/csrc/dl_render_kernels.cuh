@@ -39,6 +39,7 @@ struct ProjectArgs {
     int f64_degenerate;       // recompute det / conic / AA factor in f64 for near-degenerate splats
     int cull_offscreen;       // also cull splats with no tile on the image (no pair can touch a pixel)
     uint32_t g_begin, g_end;  // this launch projects splats [g_begin, g_end)
+    uint32_t* vis_mask;       // non-NULL: colours deferred to colour_k; [ceil(V/32)][N] record bits
 };
 
 // A 2D covariance is near-degenerate when its f32 determinant has lost at
@@ -185,6 +186,30 @@ __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
+// Splat colour for one view (project.ts:236-251): DC plus the SH bands
+// evaluated along the normalised view-space position, + 0.5, clamped at 0.
+// project_k and colour_k both call this, so deferred colours are bit-identical.
+__device__ __forceinline__ void splat_colour(const DlSceneDev& sc, uint32_t g, int M, const float dc[3], float pcx,
+                                             float pcy, float pcz, float& c0, float& c1, float& c2) {
+    float col0 = dc[0], col1 = dc[1], col2 = dc[2];
+    if (sc.bands > 0) {
+        const float len = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
+        float sr, sg, sb;
+        const float dxn = pcx / len, dyn = pcy / len, dzn = pcz / len;
+        if (sc.sh16) {
+            if (sc.bands == 1) eval_sh16<1>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else if (sc.bands == 2) eval_sh16<2>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else eval_sh16<3>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+        } else {
+            eval_sh(sc, (uint64_t)g * 3 * M, M, dxn, dyn, dzn, sr, sg, sb);
+        }
+        col0 = col0 + sr; col1 = col1 + sg; col2 = col2 + sb;
+    }
+    c0 = fmaxf(col0 + 0.5f, 0.0f);
+    c1 = fmaxf(col1 + 0.5f, 0.0f);
+    c2 = fmaxf(col2 + 0.5f, 0.0f);
+}
+
 // One splat, all views.  Thread per splat, index order (coalesced SoA reads).
 constexpr int kProjectMaxViews = 4096;          // views per frame (per-CTA visible counters)
 
@@ -220,9 +245,13 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
     const Cov3 cv = make_cov3(rot, s);
     const float sig = dl_sigmoidf(opl);
     const int M = a.sc.bands == 0 ? 0 : a.sc.bands == 1 ? 3 : a.sc.bands == 2 ? 8 : 15;
-    const uint64_t shBase = (uint64_t)g * 3 * M;
+    uint32_t mword = 0;                           // deferred colour: views of this word with a record
 
     for (uint32_t v = 0; v < a.num_views; v++) {
+        if (a.vis_mask && v && (v & 31u) == 0) {
+            if (inRange) a.vis_mask[(uint64_t)((v >> 5) - 1) * a.sc.n + g] = mword;
+            mword = 0;
+        }
         const DlView& u = vtab[v];
         const float* V = u.view;
         const uint64_t o = (uint64_t)v * a.view_stride + g;
@@ -409,23 +438,10 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             const uint32_t m = __activemask();
             if ((threadIdx.x & 31) == (uint32_t)(__ffs(m) - 1)) atomicAdd(&s_vis[v], (uint32_t)__popc(m));
         }
-        float col0 = dc[0], col1 = dc[1], col2 = dc[2];
-        if (a.sc.bands > 0) {
-            const float len = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
-            float sr, sg, sb;
-            const float dxn = pcx / len, dyn = pcy / len, dzn = pcz / len;
-            if (a.sc.sh16) {
-                if (a.sc.bands == 1) eval_sh16<1>(a.sc, g, dxn, dyn, dzn, sr, sg, sb);
-                else if (a.sc.bands == 2) eval_sh16<2>(a.sc, g, dxn, dyn, dzn, sr, sg, sb);
-                else eval_sh16<3>(a.sc, g, dxn, dyn, dzn, sr, sg, sb);
-            } else {
-                eval_sh(a.sc, shBase, M, dxn, dyn, dzn, sr, sg, sb);
-            }
-            col0 = col0 + sr; col1 = col1 + sg; col2 = col2 + sb;
-        }
-        col0 = fmaxf(col0 + 0.5f, 0.0f);
-        col1 = fmaxf(col1 + 0.5f, 0.0f);
-        col2 = fmaxf(col2 + 0.5f, 0.0f);
+        // deferred: colour_k fills the colour once the SH has arrived
+        float col0 = 0.0f, col1 = 0.0f, col2 = 0.0f;
+        if (a.vis_mask) mword |= 1u << (v & 31u);
+        else splat_colour(a.sc, g, M, dc, pcx, pcy, pcz, col0, col1, col2);
         // cull mode: the screen record carries the half-extents of the box the
         // rasterizer tests (the ellipse's box, or the radius square) instead of
         // (radius, depth), which it does not read there
@@ -443,9 +459,62 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         else
             a.bbox[o] = make_uint2(0xffffu, 0u);
     }
+    if (a.vis_mask && inRange && a.num_views)
+        a.vis_mask[(uint64_t)((a.num_views - 1) >> 5) * a.sc.n + g] = mword;
     __syncthreads();
     for (uint32_t v = threadIdx.x; v < a.num_views; v += blockDim.x)
         if (s_vis[v]) atomicAdd(&a.nvis[v], s_vis[v]);
+}
+
+// Deferred colour: thread per splat, SH read once for all views; writes the
+// colour of every (splat, view) whose record project_k wrote (vis_mask
+// [ceil(V/32)][N], bit v % 32 of word v / 32), with the arithmetic of
+// project_k (splat_colour).  Lets projection, sorting and binning run while
+// the SH coefficients are still being uploaded.
+struct ColourArgs {
+    DlSceneDev sc;
+    const DlView* views;
+    uint32_t num_views;
+    uint64_t view_stride;
+    const uint32_t* vis_mask;
+    float4* recBC;
+    uint4* recH;
+};
+
+__global__ void __launch_bounds__(256) colour_k(ColourArgs a) {
+    __shared__ DlView s_views[kProjectSmemViews];
+    const bool staged = a.num_views <= kProjectSmemViews;
+    if (staged) {
+        const uint32_t words = a.num_views * (uint32_t)(sizeof(DlView) / 4);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.views);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(s_views);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const DlView* vtab = staged ? s_views : a.views;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.sc.n) return;
+    const int M = a.sc.bands == 0 ? 0 : a.sc.bands == 1 ? 3 : a.sc.bands == 2 ? 8 : 15;
+    float pos[3], dc[3];
+    pos[0] = __ldg(a.sc.pos + 3ull * g); pos[1] = __ldg(a.sc.pos + 3ull * g + 1); pos[2] = __ldg(a.sc.pos + 3ull * g + 2);
+    dc[0] = __ldg(a.sc.dc + 3ull * g); dc[1] = __ldg(a.sc.dc + 3ull * g + 1); dc[2] = __ldg(a.sc.dc + 3ull * g + 2);
+    const uint32_t words = (a.num_views + 31) >> 5;
+    for (uint32_t w = 0; w < words; w++) {
+        uint32_t m = __ldg(a.vis_mask + (uint64_t)w * a.sc.n + g);
+        while (m) {
+            const uint32_t v = w * 32 + (uint32_t)(__ffs(m) - 1);
+            m &= m - 1;
+            const float* V = vtab[v].view;
+            const float pcx = ((V[0] * pos[0] + V[4] * pos[1]) + V[8] * pos[2]) + V[12];
+            const float pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
+            const float pcz = ((V[2] * pos[0] + V[6] * pos[1]) + V[10] * pos[2]) + V[14];
+            float c0, c1, c2;
+            splat_colour(a.sc, g, M, dc, pcx, pcy, pcz, c0, c1, c2);
+            const uint64_t o = (uint64_t)v * a.view_stride + g;
+            if (a.recBC) a.recBC[2 * o + 1] = make_float4(c0, c1, c2, 0.0f);
+            else reinterpret_cast<uint2*>(a.recH + o)[1] = make_uint2(pack_h2(c0, c1), pack_h2(c2, 0.0f));
+        }
+    }
 }
 
 // ------------------------------------------------------------------ emit

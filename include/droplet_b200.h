@@ -148,11 +148,13 @@ int dl_render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, c
  * cameras of one host SplatData in one call: the splats are uploaded into the
  * renderer's own grow-only scene buffer, all views are rendered as one batch,
  * and each RGBA8 image is copied to outs[i] (host memory).  With 8 or more
- * views the copies overlap the frame on a second stream: the splats upload in
- * 8 ranges, each projected as soon as it has arrived, and the rasterizer runs
- * over 8 view ranges, each range's images copied back while the next range
- * rasterizes (dl_render_batch with host outputs and 8+ views does the same
- * read-back). */
+ * views the copies overlap the frame on a second stream: the splats' geometry
+ * uploads in 8 ranges, each projected as soon as it has arrived, the SH
+ * coefficients follow while depth sort, binning and pair sort run (colours are
+ * evaluated once they have arrived), and the rasterizer runs over 8 view
+ * ranges, each range's images copied back while the next range rasterizes
+ * (dl_render_batch with host outputs and 8+ views does the same read-back).
+ * The data arrays must stay unchanged until the call returns. */
 int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams, int n, const float bg[4],
                    uint8_t* const* outs, uint32_t flags);
 
