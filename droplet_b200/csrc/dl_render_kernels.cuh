@@ -627,37 +627,48 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
     }
     if (tid == 0) s_excl[kEmitRanks] = total;
 
-    // decoupled look-back over this view's earlier CTAs
-    if (tid == 0) {
+    // decoupled look-back over this view's earlier CTAs, by warp 0: each step
+    // reads the 32 nearest unread predecessors at once.  No fence: a status
+    // word carries its own value, and no other data passes between CTAs.
+    if (warp == 0) {
         unsigned long long* st = a.status + (uint64_t)v * a.tiles_per_view;
         unsigned long long excl = 0;
         if (lt == 0) {
-            dl_st_volatile64(&st[0], kEmitPrefix | (unsigned long long)total);
+            if (lane == 0) dl_st_volatile64(&st[0], kEmitPrefix | (unsigned long long)total);
         } else {
-            __threadfence();
-            dl_st_volatile64(&st[lt], kEmitAgg | (unsigned long long)total);
-            int64_t q = (int64_t)lt - 1;
+            if (lane == 0) dl_st_volatile64(&st[lt], kEmitAgg | (unsigned long long)total);
+            int64_t q = (int64_t)lt - 1;                 // nearest predecessor not yet added
             uint32_t spins = 0;
-            while (q >= 0) {
-                const unsigned long long s = dl_ld_volatile64(&st[q]);
-                const unsigned long long flag = s & ~kEmitMask;
-                if (flag == 0ull) {
-                    if (++spins > DL_SPIN_LIMIT) { atomicOr(a.err, DL_DEVERR_TIMEOUT); break; }
+            while (true) {
+                // tile 0 always publishes an inclusive prefix, so a walk never passes it
+                const unsigned long long w = (q - lane >= 0) ? dl_ld_volatile64(&st[q - lane]) : kEmitPrefix;
+                const unsigned long long flag = w & ~kEmitMask;
+                const uint32_t notReady = __ballot_sync(0xffffffffu, flag == 0ull);
+                const uint32_t prefix = __ballot_sync(0xffffffffu, flag == kEmitPrefix);
+                const int firstNR = notReady ? __ffs(notReady) - 1 : 32;
+                const int firstP = prefix ? __ffs(prefix) - 1 : 32;
+                // lanes before the first unpublished one (through the first prefix) are added
+                const int take = firstP < firstNR ? firstP + 1 : firstNR;
+                unsigned long long add = lane < take ? (w & kEmitMask) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) add += __shfl_xor_sync(0xffffffffu, add, o);
+                excl += add;
+                if (firstP < firstNR) break;
+                q -= take;
+                if (take == 0) {
+                    if (++spins > DL_SPIN_LIMIT) { if (lane == 0) atomicOr(a.err, DL_DEVERR_TIMEOUT); break; }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += s & kEmitMask;
-                if (flag == kEmitPrefix) break;
-                q--;
             }
-            __threadfence();
-            dl_st_volatile64(&st[lt], kEmitPrefix | ((excl + total) & kEmitMask));
+            if (lane == 0) dl_st_volatile64(&st[lt], kEmitPrefix | ((excl + total) & kEmitMask));
         }
-        s_prefix = excl;
-        if (r0 + kEmitRanks >= n) a.npairs[v] = excl + total;    // last CTA of the view
-        const bool over = excl + total > a.pair_cap[v];
-        if (over) atomicOr(a.ovf, DL_DEVERR_OVERFLOW);
-        s_skip = over ? 1u : 0u;
+        if (lane == 0) {
+            s_prefix = excl;
+            if (r0 + kEmitRanks >= n) a.npairs[v] = excl + total;    // last CTA of the view
+            const bool over = excl + total > a.pair_cap[v];
+            if (over) atomicOr(a.ovf, DL_DEVERR_OVERFLOW);
+            s_skip = over ? 1u : 0u;
+        }
     }
     __syncthreads();
     if (s_skip) return;
@@ -673,8 +684,14 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
         const uint32_t w = o - s_excl[lo];
         const uint32_t span = s_span[lo];
         const uint32_t mn = s_min[lo];
-        const uint32_t ty = (mn >> 16) + w / span;
-        const uint32_t tx = (mn & 0xffffu) + w % span;
+        // w / span and w % span: the approximate float quotient is within 1/16
+        // of w / span (which is below 2^16, a tile row), so one step corrects it
+        uint32_t row = __float2uint_rz(__fdividef((float)w, (float)span));
+        int col = (int)w - (int)(row * span);
+        if (col < 0) { row--; col += (int)span; }
+        else if (col >= (int)span) { row++; col -= (int)span; }
+        const uint32_t ty = (mn >> 16) + row;
+        const uint32_t tx = (mn & 0xffffu) + (uint32_t)col;
         const uint32_t tileId = ty * u.tilesX + tx;
         a.pair_keys[outBase + o] = tileId;
         a.pair_vals[outBase + o] = s_g[lo];
