@@ -1080,7 +1080,9 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
                 const float4 sb = s_b[j];
                 if (kCount) evals++;
                 const float p2 = __fmaf_rn(dx, __fmaf_rn(sb.x, dx, sb.y * dy), sb.z * dy * dy);
-                if (p2 > 0.0f || p2 <= -6.4921275f) continue;          // -4.5 * log2(e)
+                // p2 <= -4.5 log2(e) needs no test of its own: there ex2 gives at
+                // most exp(-4.5) (to 2^-22), so alpha < 1/255 skips the splat below
+                if (p2 > 0.0f) continue;
                 float e;
                 asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
                 // e - floor < 0 near the cut gives alpha < 0: skipped like alpha = 0
