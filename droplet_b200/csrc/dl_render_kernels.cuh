@@ -1187,7 +1187,7 @@ __device__ __forceinline__ void raster_subtile2(const RasterArgs& a, uint32_t v,
                             }
                         } else {
                             const float p2 = __fmaf_rn(dx, __fmaf_rn(sb.x, dx, sb.y * dy[k]), sb.z * dy[k] * dy[k]);
-                            if (!(p2 > 0.0f || p2 <= -6.4921275f)) {
+                            if (!(p2 > 0.0f)) {                 // the cut falls to the alpha test
                                 float e;
                                 asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(p2));
                                 alpha[k] = sb.w * (e - DL_GAUSS_FLOOR);
