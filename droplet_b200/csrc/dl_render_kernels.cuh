@@ -498,12 +498,13 @@ __global__ void __launch_bounds__(256) colour_k(ColourArgs a) {
     float pos[3], dc[3];
     pos[0] = __ldg(a.sc.pos + 3ull * g); pos[1] = __ldg(a.sc.pos + 3ull * g + 1); pos[2] = __ldg(a.sc.pos + 3ull * g + 2);
     dc[0] = __ldg(a.sc.dc + 3ull * g); dc[1] = __ldg(a.sc.dc + 3ull * g + 1); dc[2] = __ldg(a.sc.dc + 3ull * g + 2);
-    const uint32_t words = (a.num_views + 31) >> 5;
-    for (uint32_t w = 0; w < words; w++) {
-        uint32_t m = __ldg(a.vis_mask + (uint64_t)w * a.sc.n + g);
-        while (m) {
-            const uint32_t v = w * 32 + (uint32_t)(__ffs(m) - 1);
-            m &= m - 1;
+    // views in the same order in every lane, so that the lanes of a warp
+    // write one view's records together (consecutive splats, coalesced)
+    uint32_t m = 0;
+    for (uint32_t v = 0; v < a.num_views; v++) {
+        if ((v & 31u) == 0) m = __ldg(a.vis_mask + (uint64_t)(v >> 5) * a.sc.n + g);
+        if (!((m >> (v & 31u)) & 1u)) continue;
+        {
             const float* V = vtab[v].view;
             const float pcx = ((V[0] * pos[0] + V[4] * pos[1]) + V[8] * pos[2]) + V[12];
             const float pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
