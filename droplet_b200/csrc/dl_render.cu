@@ -8,6 +8,7 @@
 // Pair buffers are sized from an upper bound; if a frame overflows them the
 // emit kernel flags it, the host grows the buffers and re-runs the pair stages.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -896,7 +897,15 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
 // different streams of one device) race on the array and must be serialised
 // by the caller.  The first call on each device looks up the array's device
 // address (cudaGetSymbolAddress) with that device current; make that first
-// call before any stream capture on the device.
+// call before any stream capture on the device.  The address is kept for the
+// life of the process: a cudaDeviceReset (or a reset of the primary context)
+// unloads the array, and calls after it are not supported.
+//
+// Stream: the calling thread's per-thread default stream (cudaStreamPerThread),
+// so the call does not wait on the other streams of the device; it
+// synchronises that stream before returning.  Its copies from pageable host
+// memory are not allowed while another thread captures a CUDA graph in
+// cudaStreamCaptureModeGlobal.
 // ============================================================================
 namespace {
 
@@ -909,7 +918,9 @@ constexpr size_t kStaticBytes = 16ull << 20;
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
 constexpr int kStaticMaxDevices = 64;
-unsigned char* g_static_addr[kStaticMaxDevices] = {};
+// device address of g_static_scratch per device ordinal; threads that make
+// their first call at once look it up alike and store the same value
+std::atomic<unsigned char*> g_static_addr[kStaticMaxDevices] = {};
 
 // Carves 256-byte-aligned pieces out of the array, in call order.
 struct Carver {
@@ -957,19 +968,21 @@ extern "C" int dl_render_static(const dl_splats* data, const dl_camera* cam, con
     int dev = 0;
     DL_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kStaticMaxDevices) { dl_set_error("dl_render_static: device ordinal too large"); return DL_E_CAPACITY; }
-    if (!g_static_addr[dev]) {
+    unsigned char* base = g_static_addr[dev].load(std::memory_order_acquire);
+    if (!base) {
         void* p = nullptr;
         DL_CK(cudaGetSymbolAddress(&p, g_static_scratch));
-        g_static_addr[dev] = static_cast<unsigned char*>(p);
+        base = static_cast<unsigned char*>(p);
+        g_static_addr[dev].store(base, std::memory_order_release);
     }
-    cudaStream_t st = 0;
+    cudaStream_t st = cudaStreamPerThread;
 
     // ---- carve the array (same layout on every call)
     const int bands = data->colors_sh ? data->sh_bands : 0;
     const int M = bands == 0 ? 0 : bands == 1 ? 3 : bands == 2 ? 8 : 15;
     const uint32_t N = (uint32_t)n;
     const FrameDims d = frame_dims(&v, 1, N, kStaticMaxPairs, 0);
-    Carver c{g_static_addr[dev]};
+    Carver c{base};
     float* dPos = c.take<float>(12ull * kStaticMaxSplats);
     float* dRot = c.take<float>(16ull * kStaticMaxSplats);
     float* dLsc = c.take<float>(12ull * kStaticMaxSplats);

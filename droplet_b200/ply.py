@@ -112,8 +112,12 @@ def loadPlySplats(source: Union[bytes, bytearray, memoryview, str], opts: Option
     opacity = col("opacity").astype(np.float32)
     dc = np.stack([SH_C0 * col("f_dc_0"), SH_C0 * col("f_dc_1"), SH_C0 * col("f_dc_2")], axis=1).astype(np.float32)
     w, qx, qy, qz = col("rot_0"), col("rot_1"), col("rot_2"), col("rot_3")
-    n = np.sqrt(w * w + qx * qx + qy * qy + qz * qz)
-    n = np.where(n == 0.0, 1.0, n)                                  # Math.hypot(...) || 1
+    # Math.hypot(...) || 1: hypot is +Infinity when any argument is infinite
+    # (even beside a NaN), NaN when one is NaN, and `|| 1` maps both NaN and 0 to 1
+    with np.errstate(invalid="ignore", over="ignore"):
+        n = np.sqrt(w * w + qx * qx + qy * qy + qz * qz)
+    n = np.where(np.isinf(w) | np.isinf(qx) | np.isinf(qy) | np.isinf(qz), np.inf, n)
+    n = np.where(np.isnan(n) | (n == 0.0), 1.0, n)
     f = -1.0 if flip else 1.0
     rotations = np.stack([w / n, (f * qx) / n, qy / n, (f * qz) / n], axis=1).astype(np.float32)
     sh = None

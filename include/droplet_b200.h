@@ -162,12 +162,16 @@ int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_camera* cams,
  * memory (an application that owns the whole device through its own
  * allocator, or a real-time loop that may not allocate after start-up): the
  * single-view render of dl_render with no renderer handle, on the current CUDA
- * device and its default stream, with all device scratch taken from one
- * 16 MiB array that the library reserves statically on every GPU that loads
- * it.  Limits: 16384 Gaussians, 921600 pixels (e.g. 1280x720), 4096 16x16
- * tiles, 262144 tile pairs; beyond them it returns DL_E_CAPACITY.  Calls that
- * overlap on one GPU race on the shared array.  The first call on a device
- * looks the array up and should come before any stream capture there.
+ * device, with all device scratch taken from one 16 MiB array that the
+ * library reserves statically on every GPU that loads it.  Limits: 16384
+ * Gaussians, 921600 pixels (e.g. 1280x720), 4096 16x16 tiles, 262144 tile
+ * pairs; beyond them it returns DL_E_CAPACITY.  Calls that overlap on one GPU
+ * race on the shared array.  The first call on a device looks the array up
+ * and should come before any stream capture there; after a cudaDeviceReset
+ * of that device the call is not supported.  It runs on the calling thread's
+ * per-thread default stream (no wait on the device's other streams) and
+ * returns after that stream has finished; its pageable host copies are not
+ * allowed while another thread captures a graph in global capture mode.
  * max_coverage 0 selects the default 16384. */
 int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg[4], uint32_t max_coverage,
                      uint8_t* out_rgba, size_t out_len);

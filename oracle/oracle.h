@@ -32,7 +32,7 @@ int64_t orc_render_get(void* h, const char* name, void* dst, int64_t cap);
 void orc_render_free(void* h);
 
 void* orc_voxelize_run(const orc_splats* data, double voxelRes, double opacityCutoff,
-                       const double* bounds6, int order, float eps);
+                       const double* bounds6, int order, float eps, int64_t zrow_lo, int64_t zrow_hi);
 int64_t orc_voxelize_get(void* h, const char* name, void* dst, int64_t cap);
 void orc_voxelize_free(void* h);
 

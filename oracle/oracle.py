@@ -55,7 +55,8 @@ def lib():
         L.orc_render_free.argtypes = [ctypes.c_void_p]
         L.orc_voxelize_run.restype = ctypes.c_void_p
         L.orc_voxelize_run.argtypes = [ctypes.POINTER(OrcSplats), ctypes.c_double, ctypes.c_double,
-                                       ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_float]
+                                       ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_float,
+                                       ctypes.c_int64, ctypes.c_int64]
         L.orc_voxelize_get.restype = ctypes.c_int64
         L.orc_voxelize_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64]
         L.orc_voxelize_free.argtypes = [ctypes.c_void_p]
@@ -126,12 +127,17 @@ def render(data, camera, background=(0.0, 0.0, 0.0, 1.0), maxCoverage=16384, chu
 
 
 def voxelize(data, voxelResolution=0.05, opacityCutoff=0.1, bounds=None, order=0, eps=1e-5,
-             fields=("block_idx", "mask_lo", "mask_hi", "bounds", "dims")):
+             fields=("block_idx", "mask_lo", "mask_hi", "bounds", "dims"), z_rows=None):
+    """Run the oracle voxelizer.  order 0: canonical summation order (ascending
+    Gaussian index), order 1: the reference's BVH query order.  z_rows=(lo, hi)
+    restricts the run to the 16^3-block batches whose z row is in [lo, hi)."""
     L = lib()
+    zlo, zhi = (0, 0) if z_rows is None else (int(z_rows[0]), int(z_rows[1]))
     b = None
     if bounds is not None:
         b = (ctypes.c_double * 6)(*[float(v) for v in list(bounds[0]) + list(bounds[1])])
-    h = L.orc_voxelize_run(ctypes.byref(splats_struct(data)), voxelResolution, opacityCutoff, b, order, eps)
+    h = L.orc_voxelize_run(ctypes.byref(splats_struct(data)), voxelResolution, opacityCutoff, b, order, eps,
+                           zlo, zhi)
     try:
         out = {f: _fetch(L.orc_voxelize_get, h, f, _VOX_DTYPES[f]) for f in fields}
     finally:

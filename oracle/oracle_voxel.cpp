@@ -216,8 +216,12 @@ struct OrcVoxel {
     uint64_t nearBits = 0, evals = 0, listEntries = 0;
 };
 
+// zrow_lo / zrow_hi: when zrow_hi > zrow_lo, only the batches of 16^3 blocks
+// whose z row (bz / 16) lies in [zrow_lo, zrow_hi) are voxelized (bounds and
+// dims still come from the whole input), so a full-size grid can be checked
+// a few rows at a time; the block list keeps the batch order.
 extern "C" void* orc_voxelize_run(const orc_splats* data, double voxelRes, double opacityCutoff,
-                                  const double* bounds6, int order, float eps) {
+                                  const double* bounds6, int order, float eps, int64_t zrow_lo, int64_t zrow_hi) {
     OrcVoxel* V = new OrcVoxel();
     const double blockSize = 4 * voxelRes;
     computeAabbExtents(*data, V->extents);
@@ -246,8 +250,9 @@ extern "C" void* orc_voxelize_run(const orc_splats* data, double voxelRes, doubl
     const float half = res * 0.5f;
 
     // batch grid, voxelize.ts:185-233
-    struct Batch { int64_t bx, by, bz, cx, cy, cz; double qmn[3], qmx[3]; };
+    struct Batch { int64_t bx, by, bz, cx, cy, cz; double qmn[3], qmx[3]; bool skip; };
     std::vector<Batch> batches;
+    const bool rows = zrow_hi > zrow_lo;
     for (int64_t bz = 0; bz < NZ; bz += 16)
         for (int64_t by = 0; by < NY; by += 16)
             for (int64_t bx = 0; bx < NX; bx += 16) {
@@ -256,6 +261,7 @@ extern "C" void* orc_voxelize_run(const orc_splats* data, double voxelRes, doubl
                 b.cx = std::min<int64_t>(16, NX - bx);
                 b.cy = std::min<int64_t>(16, NY - by);
                 b.cz = std::min<int64_t>(16, NZ - bz);
+                b.skip = rows && (bz / 16 < zrow_lo || bz / 16 >= zrow_hi);
                 b.qmn[0] = V->bounds[0] + (double)bx * blockSize;
                 b.qmn[1] = V->bounds[1] + (double)by * blockSize;
                 b.qmn[2] = V->bounds[2] + (double)bz * blockSize;
@@ -292,6 +298,7 @@ extern "C" void* orc_voxelize_run(const orc_splats* data, double voxelRes, doubl
                     lo[a] = std::min(lo[a], b); hi[a] = std::max(hi[a], b);
                 }
             }
+            if (rows) { lo[2] = std::max<int64_t>(lo[2], zrow_lo); hi[2] = std::min<int64_t>(hi[2], zrow_hi - 1); }
             for (int64_t z = lo[2]; z <= hi[2]; z++)
                 for (int64_t y = lo[1]; y <= hi[1]; y++)
                     for (int64_t x = lo[0]; x <= hi[0]; x++)
@@ -303,6 +310,7 @@ extern "C" void* orc_voxelize_run(const orc_splats* data, double voxelRes, doubl
     #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t bi_ = 0; bi_ < (int64_t)batches.size(); bi_++) {
         const Batch& B = batches[bi_];
+        if (B.skip) continue;
         std::vector<uint32_t> listBuf;
         const std::vector<uint32_t>* list;
         if (order == 1) { bvh->query(B.qmn, B.qmx, listBuf); list = &listBuf; }

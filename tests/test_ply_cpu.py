@@ -61,6 +61,17 @@ def test_zero_quaternion_and_other_elements():
     assert list(d.rotations) == [0.0, -0.0, 0.0, -0.0]           # || 1: divided by 1
 
 
+def test_nan_and_infinite_quaternions_follow_math_hypot():
+    # Math.hypot(w, x, y, z) || 1: a NaN component gives NaN -> 1 (the finite
+    # components pass through); an infinite one gives +Infinity even beside a NaN
+    nan, inf = float("nan"), float("inf")
+    rows = [[0.0] * 10 + [nan, 0.5, 0.25, 2.0], [0.0] * 10 + [inf, nan, 1.0, 2.0]]
+    d = ply.loadPlySplats(_ply(BASE, rows), {"flipY": False})
+    q = d.rotations.reshape(-1, 4)
+    assert np.isnan(q[0, 0]) and list(q[0, 1:]) == [0.5, 0.25, 2.0]
+    assert np.isnan(q[1, 0]) and np.isnan(q[1, 1]) and list(q[1, 2:]) == [0.0, 0.0]
+
+
 @pytest.mark.parametrize("make,msg", [
     (lambda: b"ply\nformat binary_little_endian 1.0\nelement vertex 1\n", "end_header not found"),
     (lambda: b"plx\nend_header\n", "missing magic"),

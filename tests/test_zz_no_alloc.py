@@ -42,6 +42,24 @@ def test_static_render_matches_dl_render_twice():
     r.destroy()
 
 
+def test_static_render_allocates_nothing():
+    # after one warm-up call (driver set-up such as pageable-copy staging), the
+    # device's free memory must not move across further calls
+    import torch
+    data = synth.cluster_scene(12_000, seed=43, clusters=8, extent=1.5, bands=1)
+    cam = synth.pinhole(960, 540, (0.0, 0.3, 4.0))
+    st, first = render_static(data, cam)
+    assert st == _lib.DL_OK, _lib.load().dl_last_error().decode()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        st, again = render_static(data, cam)
+        assert st == _lib.DL_OK and np.array_equal(again, first)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_static_render_rejects_sizes_beyond_its_array():
     data = synth.plain_100k(16_385)
     st, _ = render_static(data, synth.pinhole(320, 180, (0.0, 0.0, 4.0)))
@@ -49,3 +67,21 @@ def test_static_render_rejects_sizes_beyond_its_array():
     assert "16384" in _lib.load().dl_last_error().decode()
     st, _ = render_static(synth.plain_100k(100), synth.pinhole(1920, 1080, (0.0, 0.0, 4.0)))
     assert st == _lib.DL_E_CAPACITY
+    # within the splat and pixel limits, but large splats bin to more tile
+    # pairs than the array holds (2000 splats x ~3600 tiles of a 1280x720 view)
+    n = 2000
+    rng = np.random.default_rng(5)
+    big = dl.SplatData(n, (rng.random((n, 3)) * 0.2 - 0.1).astype(np.float32),
+                       np.tile(np.array([1, 0, 0, 0], np.float32), (n, 1)), np.full((n, 3), np.log(0.6), np.float32),
+                       np.full(n, 2.0, np.float32), np.full((n, 3), 0.3, np.float32))
+    st, _ = render_static(big, synth.pinhole(1280, 720, (0.0, 0.0, 3.0)))
+    assert st == _lib.DL_E_CAPACITY
+    assert "tile pairs" in _lib.load().dl_last_error().decode()
+    # and the next call in range still renders correctly
+    data = synth.plain_100k(3_000)
+    cam = synth.pinhole(640, 360, (0.0, 0.0, 4.0))
+    st, got = render_static(data, cam)
+    assert st == _lib.DL_OK
+    r = dl.Renderer(dl.createDevice())
+    assert np.array_equal(got, r.render(data, cam))
+    r.destroy()
