@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--dry-run", action="store_true",
+                   help="start the ranks and report them, with no GPU work (gloo on the CPU; a check of the launcher)")
     p.add_argument("--workload", default="ring64",
                    choices=["ring64", "plain100k", "sh3-1080p", "sh3-equirect", "zipf10m-16v", "voxel1m", "zipf10m"],
                    help="ring64: the headline render batch; plain100k / sh3-1080p / sh3-equirect / zipf10m-16v: "
@@ -453,11 +455,55 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def launch_ranks(args):
+    """--gpus N outside a torchrun environment: run this script again under
+    torch.distributed.run with N local ranks (one per GPU) and exit with its
+    status.  Rank 0 prints the JSON line."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    sys.stdout.flush()
+    sys.exit(subprocess.call(cmd))
+
+
+def run_dry(args, rank, world):
+    """The ranks come up and report themselves over gloo; rank 0 prints who ran."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        ranks = [rank]
+        if world > 1:
+            got = [None] * world
+            dist.all_gather_object(got, {"rank": rank, "pid": os.getpid()})
+            ranks = [g["rank"] for g in got]
+        if rank == 0:
+            print(json.dumps({"dry_run": True, "n_gpus": len(ranks), "ranks": ranks, "requested": args.gpus,
+                              "backend": "gloo" if world > 1 else None, "torch": torch.__version__}), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        launch_ranks(args)
+    if world != args.gpus and "WORLD_SIZE" in os.environ:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but {world} ranks were started")
+    if args.dry_run:
+        run_dry(args, rank, world)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -468,6 +514,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if dist.get_world_size() != args.gpus:
+            raise SystemExit(f"bench.py: the NCCL group has {dist.get_world_size()} ranks, --gpus is {args.gpus}")
     try:
         if args.workload in VOXEL:
             run_voxel(args, rank, world, local_rank)
