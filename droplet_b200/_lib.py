@@ -40,7 +40,8 @@ EXPORTS = [
     "dl_mlp_predict", "dl_mlp_grad", "dl_mlp_train", "dl_renderer_set_scheduler", "dl_renderer_tile_log",
     "dl_sorter_create", "dl_sorter_destroy", "dl_sorter_set_stream", "dl_sorter_set_digit_bits", "dl_sorter_sort",
     "dl_renderer_set_tuning", "dl_renderer_get_tuning", "dl_renderer_autotune",
-    "dl_device_set_voxel_scheduler", "dl_vox_result_block_log",
+    "dl_device_set_voxel_scheduler", "dl_vox_result_block_log", "dl_test_set_wait_limit",
+    "dl_test_withhold_status", "dl_test_fail_allocation",
 ]
 
 
@@ -131,6 +132,9 @@ def load():
         "dl_device_set_voxel_scheduler": [vp, vp],
         "dl_vox_result_block_log": [vp, vp, vp, ctypes.c_uint64, P(ctypes.c_uint64)],
         "dl_renderer_get_tuning": [vp, P(DlTuning)],
+        "dl_test_set_wait_limit": [ctypes.c_uint32],
+        "dl_test_withhold_status": [i, ctypes.c_uint32],
+        "dl_test_fail_allocation": [i],
         "dl_renderer_autotune": [vp, vp, P(DlCamera), i, P(ctypes.c_float), ctypes.c_uint32, i, P(DlTuning),
                                  P(ctypes.c_double)],
     }

@@ -13,6 +13,31 @@ void dl_set_error(const std::string& msg) { g_last_error = msg; }
 
 extern "C" const char* dl_last_error(void) { return g_last_error.c_str(); }
 
+// ---------------------------------------------------------------- bounded waits (test hooks)
+DlWaitPlan g_dl_wait;
+
+extern "C" int dl_test_set_wait_limit(uint32_t polls) {
+    g_dl_wait.spin_limit = polls ? polls : DL_SPIN_LIMIT;
+    return DL_OK;
+}
+
+int g_dl_alloc_budget = -1;
+
+extern "C" int dl_test_fail_allocation(int after) {
+    g_dl_alloc_budget = after < 0 ? -1 : after;
+    return DL_OK;
+}
+
+extern "C" int dl_test_withhold_status(int stage, uint32_t tile) {
+    if (stage < DL_WAIT_STAGE_NONE || stage > DL_WAIT_STAGE_PAIR_SORT) {
+        dl_set_error("dl_test_withhold_status: stage must be 0..3");
+        return DL_E_INVALID_ARG;
+    }
+    g_dl_wait.withhold_stage = stage;
+    g_dl_wait.withhold_tile = stage == DL_WAIT_STAGE_NONE ? 0xffffffffu : tile;
+    return DL_OK;
+}
+
 // ---------------------------------------------------------------- device
 extern "C" int dl_device_open(int ordinal, dl_device** out) {
     if (!out) { dl_set_error("dl_device_open: out is NULL"); return DL_E_INVALID_ARG; }

@@ -26,6 +26,11 @@ void dl_set_error(const std::string& msg);
         if (s_ != DL_OK) return s_;   \
     } while (0)
 
+// Test hook (dl_test_fail_allocation): the number of device allocations that
+// still succeed before one is refused as if the device were out of memory;
+// negative: none is refused.
+extern int g_dl_alloc_budget;
+
 // Grow-only device buffer.
 struct DevBuf {
     void* p = nullptr;
@@ -36,6 +41,12 @@ struct DevBuf {
         p = nullptr;
         bytes = 0;
         const size_t alloc = need < 256 ? 256 : need;
+        if (g_dl_alloc_budget == 0) {
+            g_dl_alloc_budget = -1;
+            dl_set_error(std::string("cudaMalloc(") + std::to_string(alloc) + "): out of memory (refused by the test hook)");
+            return DL_E_OOM;
+        }
+        if (g_dl_alloc_budget > 0) g_dl_alloc_budget--;
         cudaError_t e = cudaMalloc(&p, alloc);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -48,6 +59,20 @@ struct DevBuf {
     void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
+
+// Bounded device waits (decoupled look-backs): how many polls of an
+// unpublished predecessor a CTA makes before it gives up with
+// DL_DEVERR_TIMEOUT, and a test hook that makes one CTA of one stage withhold
+// its status so that its successors run into that limit (dl_test_* entry
+// points; the defaults leave every stage as it is).
+enum { DL_WAIT_STAGE_NONE = 0, DL_WAIT_STAGE_DEPTH_SORT = 1, DL_WAIT_STAGE_EMIT = 2, DL_WAIT_STAGE_PAIR_SORT = 3 };
+struct DlWaitPlan {
+    uint32_t spin_limit = DL_SPIN_LIMIT;
+    int withhold_stage = DL_WAIT_STAGE_NONE;
+    uint32_t withhold_tile = 0xffffffffu;
+    uint32_t withheld(int stage) const { return withhold_stage == stage ? withhold_tile : 0xffffffffu; }
+};
+extern DlWaitPlan g_dl_wait;
 
 struct dl_mlp;
 struct VoxBufs;

@@ -406,6 +406,8 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
             sp.segs = p == 0 ? ds : ds2; sp.glob_off = f.depthHist;
             sp.status = f.sortStatus; sp.counter = f.scr + SC_DEPTH_CTR + p; sp.err = f.scr + SC_ERR;
             sp.shift = 8 * p; sp.pass = p; sp.passes = 4; sp.drop_max = p == 0 ? 1 : 0;
+            sp.spin_limit = g_dl_wait.spin_limit;
+            if (p == 0) sp.withhold_tile = g_dl_wait.withheld(DL_WAIT_STAGE_DEPTH_SORT);
             launch_pass_bits(8, sp, d.depthGrid, st);
             (*launches)++;
             std::swap(kin, kout);
@@ -447,6 +449,8 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ea.counter = f.scr + SC_EMIT_CTR;
     ea.err = f.scr + SC_ERR;
     ea.ovf = f.scr + SC_OVF;
+    ea.spin_limit = g_dl_wait.spin_limit;
+    ea.withhold_tile = g_dl_wait.withheld(DL_WAIT_STAGE_EMIT);
     dlr::emit_k<<<d.V * d.emitTilesPerView, dlr::kEmitThreads, 0, st>>>(ea);
     (*launches)++;
     DL_CK(cudaGetLastError());
@@ -460,6 +464,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     pd.seg_len = f.pairSegLen;
     pd.bits = d.pbits;
     pd.passes = d.ppasses;
+    pd.err = f.scr + SC_ERR;
     dlr::pair_digits_k<<<d.V, 32, 0, st>>>(pd);
     (*launches)++;
     DL_CK(cudaGetLastError());
@@ -482,6 +487,8 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
             sp.segs = ps; sp.glob_off = f.pairGlob;
             sp.status = f.sortStatus; sp.counter = f.scr + SC_PAIR_CTR + p; sp.err = f.scr + SC_ERR;
             sp.shift = d.pbits * p; sp.pass = p; sp.passes = d.ppasses;
+            sp.spin_limit = g_dl_wait.spin_limit;
+            if (p == 0) sp.withhold_tile = g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT);
             launch_pass_bits(d.pbits, sp, d.pairGrid, st);
             (*launches)++;
             std::swap(kin, kout);
@@ -498,6 +505,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ba.seg_len = f.pairSegLen;
     ba.tile_off = f.tileOff;
     ba.tile_stride = d.TS;
+    ba.err = f.scr + SC_ERR;
     const uint32_t bgrid = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((d.cap + 256) / 256, 1), 2048);
     dlr::boundaries_k<<<dim3(bgrid, d.V), 256, 0, st>>>(ba);
     (*launches)++;
@@ -812,7 +820,9 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             const uint64_t* sp = reinterpret_cast<const uint64_t*>(&sc);
             key.insert(key.end(), sp, sp + sizeof(DlSceneDev) / 8);
             key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid,
-                                   (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2});
+                                   (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2, g_dl_wait.spin_limit,
+                                   g_dl_wait.withheld(DL_WAIT_STAGE_DEPTH_SORT), g_dl_wait.withheld(DL_WAIT_STAGE_EMIT),
+                                   g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT)});
             if (!r->graph_exec || key != r->graph_key) {
                 if (r->graph_exec) { cudaGraphExecDestroy(r->graph_exec); r->graph_exec = nullptr; }
                 cudaGraph_t g = nullptr;

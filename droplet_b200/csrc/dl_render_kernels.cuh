@@ -548,6 +548,8 @@ struct EmitArgs {
     uint32_t* counter;
     uint32_t* err;                 // DL_DEVERR_TIMEOUT
     uint32_t* ovf;                 // DL_DEVERR_OVERFLOW
+    uint32_t spin_limit;           // look-back polls before giving up
+    uint32_t withhold_tile;        // test hook: this CTA tile publishes no status (0xffffffff: none)
 };
 
 // Pair values carry this bit for splats whose box lies entirely left of or
@@ -573,6 +575,8 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
     __shared__ uint32_t s_dh[4 * 256];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // after a timed-out depth sort the sorted indices may hold unwritten slots
+    if (__syncthreads_or(tid == 0 && (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT))) return;
     if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
     for (int i = tid; i < 4 * 256; i += kEmitThreads) s_dh[i] = 0;
     __syncthreads();
@@ -634,10 +638,11 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
     if (warp == 0) {
         unsigned long long* st = a.status + (uint64_t)v * a.tiles_per_view;
         unsigned long long excl = 0;
+        const bool publish = tile != a.withhold_tile;
         if (lt == 0) {
-            if (lane == 0) dl_st_volatile64(&st[0], kEmitPrefix | (unsigned long long)total);
+            if (lane == 0 && publish) dl_st_volatile64(&st[0], kEmitPrefix | (unsigned long long)total);
         } else {
-            if (lane == 0) dl_st_volatile64(&st[lt], kEmitAgg | (unsigned long long)total);
+            if (lane == 0 && publish) dl_st_volatile64(&st[lt], kEmitAgg | (unsigned long long)total);
             int64_t q = (int64_t)lt - 1;                 // nearest predecessor not yet added
             uint32_t spins = 0;
             while (true) {
@@ -657,11 +662,11 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
                 if (firstP < firstNR) break;
                 q -= take;
                 if (take == 0) {
-                    if (++spins > DL_SPIN_LIMIT) { if (lane == 0) atomicOr(a.err, DL_DEVERR_TIMEOUT); break; }
+                    if (++spins > a.spin_limit) { if (lane == 0) atomicOr(a.err, DL_DEVERR_TIMEOUT); break; }
                     __nanosleep(32);
                 }
             }
-            if (lane == 0) dl_st_volatile64(&st[lt], kEmitPrefix | ((excl + total) & kEmitMask));
+            if (lane == 0 && publish) dl_st_volatile64(&st[lt], kEmitPrefix | ((excl + total) & kEmitMask));
         }
         if (lane == 0) {
             s_prefix = excl;
@@ -715,6 +720,7 @@ struct PairDigitArgs {
     const uint64_t* pair_cap;
     uint32_t* seg_len;
     int bits, passes;
+    const uint32_t* err;           // DL_DEVERR_TIMEOUT: the pair lists are not complete
 };
 
 __global__ void pair_digits_k(PairDigitArgs a) {
@@ -728,7 +734,9 @@ __global__ void pair_digits_k(PairDigitArgs a) {
         for (int d = 0; d < radix; d++) { o[d] = acc; acc += h[d]; }
     }
     if (threadIdx.x == 0) {
-        const bool ok = a.npairs[v] <= a.pair_cap[v];
+        // an overflowed view, or any view of a frame with a timed-out wait,
+        // sorts and bins no pairs: nothing downstream reads unwritten slots
+        const bool ok = a.npairs[v] <= a.pair_cap[v] && !(dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT);
         a.seg_len[v] = ok ? (uint32_t)a.npairs[v] : 0u;
     }
 }
@@ -745,11 +753,13 @@ struct BoundArgs {
     const uint32_t* seg_len;       // [V] pairs per view (0 on overflow)
     uint32_t* tile_off;            // [V][tile_stride]
     uint32_t tile_stride;
+    const uint32_t* err;           // DL_DEVERR_TIMEOUT: the sorted keys are not complete
 };
 
 __global__ void boundaries_k(BoundArgs a) {
     const uint32_t v = blockIdx.y;
-    const uint32_t n = a.seg_len[v];
+    // after a timed-out pair sort every view gets empty tiles
+    const uint32_t n = (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT) ? 0u : a.seg_len[v];
     const uint32_t T = a.views[v].numTiles;
     const uint32_t* k = a.keys + a.pair_base[v];
     uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;

@@ -14,9 +14,12 @@
 // every pass sorts each segment separately in the same launch.  Segment
 // lengths live in device memory so a whole frame can run without a host sync.
 //
-// Every look-back wait is bounded (DL_SPIN_LIMIT polls); on expiry the CTA
-// sets DL_DEVERR_TIMEOUT in the error word, assumes a zero prefix and
-// finishes, so the host reports an error instead of the GPU hanging.
+// Every look-back wait is bounded (Pass::spin_limit polls, DL_SPIN_LIMIT by
+// default); on expiry the CTA sets DL_DEVERR_TIMEOUT in the error word, keeps
+// the prefix it has summed so far (so its writes stay inside its segment) and
+// finishes, so the host reports an error instead of the GPU hanging.  A pass
+// that starts with the timeout bit already set does nothing: its input may
+// hold slots that an earlier pass never wrote.
 //
 // Pass kernel choices (measured on B200, 64M random keys, 4 passes, and 256M
 // 14-bit keys in 64 segments, 2 passes; 16 B per key per pass): the warp
@@ -131,6 +134,8 @@ struct Pass {
     // stable pass over the remaining elements, compacted to the segment start.
     // Launch pass_k<BITS, true> for such a pass.
     int drop_max = 0;
+    uint32_t spin_limit = DL_SPIN_LIMIT;   // look-back polls before giving up
+    uint32_t withhold_tile = 0xffffffffu;  // test hook: this global tile publishes no status
 };
 
 constexpr int kLookback = 4;                 // predecessor tiles read per look-back step
@@ -151,11 +156,13 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     __shared__ uint32_t s_nkeep;                 // elements of the tile that are written
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (__syncthreads_or(tid == 0 && (dl_ld_volatile(p.err) & DL_DEVERR_TIMEOUT))) return;
     if (tid == 0) s_tile = atomicAdd(p.counter, 1u);
     for (int i = lane; i < RADIX; i += 32) s_hist[warp][i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     if (tile >= *p.segs.total_tiles) return;
+    const bool publish = tile != p.withhold_tile;
     const uint32_t seg = seg_of_tile(p.segs, tile);
     const uint32_t lt = tile - p.segs.tile_base[seg];
     const uint32_t len = p.segs.len[seg];
@@ -200,7 +207,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     uint32_t cnt = 0;
     if (tid < RADIX) {
         for (int w = 0; w < WARPS; w++) { const uint32_t c = s_hist[w][tid]; s_hist[w][tid] = cnt; cnt += c; }
-        dl_st_volatile(p.status + (size_t)tile * RADIX + tid, (lt == 0 ? kFlagPrefix : kFlagAgg) | cnt);
+        if (publish) dl_st_volatile(p.status + (size_t)tile * RADIX + tid, (lt == 0 ? kFlagPrefix : kFlagAgg) | cnt);
     }
     // exclusive scan of the tile's digit counts -> position of each digit run in the tile
     {
@@ -249,11 +256,11 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
                 if (done) break;
                 q -= used;
                 if (stall) {
-                    if (++spins > DL_SPIN_LIMIT) { atomicOr(p.err, DL_DEVERR_TIMEOUT); break; }
+                    if (++spins > p.spin_limit) { atomicOr(p.err, DL_DEVERR_TIMEOUT); break; }
                     __nanosleep(32);
                 }
             }
-            dl_st_volatile(p.status + (size_t)tile * RADIX + tid, kFlagPrefix | ((excl + cnt) & kValMask));
+            if (publish) dl_st_volatile(p.status + (size_t)tile * RADIX + tid, kFlagPrefix | ((excl + cnt) & kValMask));
         }
         s_glob[tid] = p.glob_off[((size_t)seg * p.passes + p.pass) * RADIX + tid] + excl;
     }

@@ -50,9 +50,11 @@ namespace {
 
 constexpr unsigned long long kAgg = 1ull << 62, kPre = 2ull << 62, kMask = (1ull << 62) - 1;
 
-// Decoupled look-back over CTAs of one chain; called by a single thread.
+// Decoupled look-back over CTAs of one chain; called by a single thread.  At
+// most spin_limit polls of an unpublished predecessor, then DL_DEVERR_TIMEOUT
+// and the prefix summed so far (the CTA's writes stay inside the chain).
 __device__ unsigned long long lookback(unsigned long long* status, uint32_t tile, unsigned long long total,
-                                       uint32_t* err) {
+                                       uint32_t* err, uint32_t spin_limit) {
     if (tile == 0) {
         dl_st_volatile64(&status[0], kPre | total);
         return 0ull;
@@ -66,7 +68,7 @@ __device__ unsigned long long lookback(unsigned long long* status, uint32_t tile
         const unsigned long long s = dl_ld_volatile64(&status[q]);
         const unsigned long long f = s & ~kMask;
         if (f == 0ull) {
-            if (++spins > DL_SPIN_LIMIT) { atomicOr(err, DL_DEVERR_TIMEOUT); break; }
+            if (++spins > spin_limit) { atomicOr(err, DL_DEVERR_TIMEOUT); break; }
             __nanosleep(32);
             continue;
         }
@@ -270,6 +272,7 @@ struct VoxEmitArgs {
     uint32_t* counter;
     uint32_t* err;
     uint32_t* ovf;
+    uint32_t spin_limit;
 };
 
 __global__ void __launch_bounds__(kVT) vox_emit_k(VoxEmitArgs a) {
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(kVT) vox_emit_k(VoxEmitArgs a) {
     for (int j = 0; j < kVI; j++) { s_excl[tid * kVI + j] = run; run += cnt[j]; }
     if (tid == 0) {
         s_excl[kVR] = total;
-        const unsigned long long pre = lookback(a.status, tile, total, a.err);
+        const unsigned long long pre = lookback(a.status, tile, total, a.err, a.spin_limit);
         s_pre = pre;
         if (g0 + kVR >= a.p.n) *a.npairs = pre + total;
         const bool over = pre + total > a.cap;
@@ -371,6 +374,7 @@ struct HeadsArgs {
     unsigned long long* status;
     uint32_t* counter;
     uint32_t* err;
+    uint32_t spin_limit;
 };
 
 __global__ void __launch_bounds__(kVT) vox_heads_k(HeadsArgs a) {
@@ -378,6 +382,11 @@ __global__ void __launch_bounds__(kVT) vox_heads_k(HeadsArgs a) {
     __shared__ uint32_t s_tile;
     __shared__ unsigned long long s_pre;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // after a timed-out sort the keys may hold unwritten slots: no blocks
+    if (__syncthreads_or(tid == 0 && (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT))) {
+        if (blockIdx.x == 0 && tid == 0) { *a.nblocks = 0; a.bstart[0] = 0; }
+        return;
+    }
     if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
@@ -405,7 +414,7 @@ __global__ void __launch_bounds__(kVT) vox_heads_k(HeadsArgs a) {
     uint32_t wpre = 0, total = 0;
     for (int w = 0; w < kVT / 32; w++) { if (w < warp) wpre += s_wsum[w]; total += s_wsum[w]; }
     if (tid == 0) {
-        s_pre = lookback(a.status, tile, total, a.err);
+        s_pre = lookback(a.status, tile, total, a.err, a.spin_limit);
         if (i0 + kVR >= n) { *a.nblocks = (uint32_t)(s_pre + total); a.bstart[s_pre + total] = (uint32_t)n; }
     }
     __syncthreads();
@@ -433,6 +442,7 @@ struct EvalArgs {
     unsigned long long* evals;
     const uint32_t* work;          // optional block order (learned); NULL: block order
     uint32_t* cycles;              // optional [block] SM cycles / 16 spent on the block
+    const uint32_t* err;           // DL_DEVERR_TIMEOUT: the block lists are not complete
 };
 
 __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, const VoxRec& g) {
@@ -459,7 +469,9 @@ __global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
     __shared__ uint32_t s_b;
     __shared__ uint32_t s_mask[2];
     const int tid = threadIdx.x;
-    const uint32_t nb = *a.nblocks;
+    // the heads kernel before this one is complete: a timed-out wait there
+    // (partial block lists) leaves nothing to evaluate
+    const uint32_t nb = (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT) ? 0u : *a.nblocks;
     // linear bit index = z*16 + y*4 + x (shaders/voxelize.ts:137)
     const uint32_t lx = tid & 3, ly = (tid >> 2) & 3, lz = tid >> 4;
     const int64_t NX = a.p.NB[0], NY = a.p.NB[1], NBX = a.p.NBB[0], NBY = a.p.NBB[1];
@@ -537,6 +549,7 @@ struct VoxSchedArgs {
     uint32_t* bucket;              // [block]
     uint32_t* hist;                // [256] (zeroed)
     uint32_t* work;                // [block]
+    const uint32_t* err;           // DL_DEVERR_TIMEOUT: the block lists are not complete
 };
 
 __device__ __forceinline__ void vox_block_features(const VoxSchedArgs& a, uint32_t b, uint32_t nb, float* x) {
@@ -579,7 +592,7 @@ constexpr int kVSchedThreads = 128;
 __global__ void __launch_bounds__(kVSchedThreads) vox_sched_pred_k(VoxSchedArgs a) {
     __shared__ float P[dlmlp::kParams];
     if (a.w) dlmlp::load_params(a.w, P);
-    const uint32_t nb = *a.nblocks;
+    const uint32_t nb = (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT) ? 0u : *a.nblocks;
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
         float x[12];
         vox_block_features(a, b, nb, x);
@@ -603,7 +616,7 @@ __global__ void vox_sched_scan_k(uint32_t* hist) {
 }
 
 __global__ void vox_sched_scatter_k(VoxSchedArgs a) {
-    const uint32_t nb = *a.nblocks;
+    const uint32_t nb = (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT) ? 0u : *a.nblocks;
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
         a.work[atomicAdd(&a.hist[a.bucket[b]], 1u)] = b;
 }
@@ -621,6 +634,7 @@ struct CompactArgs {
     unsigned long long* status;
     uint32_t* counter;
     uint32_t* err;
+    uint32_t spin_limit;
 };
 
 __global__ void __launch_bounds__(kVT) vox_compact_k(CompactArgs a) {
@@ -628,6 +642,10 @@ __global__ void __launch_bounds__(kVT) vox_compact_k(CompactArgs a) {
     __shared__ uint32_t s_tile;
     __shared__ unsigned long long s_pre;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (__syncthreads_or(tid == 0 && (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT))) {
+        if (blockIdx.x == 0 && tid == 0) *a.nout = 0;
+        return;
+    }
     if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
@@ -657,7 +675,7 @@ __global__ void __launch_bounds__(kVT) vox_compact_k(CompactArgs a) {
     uint32_t wpre = 0, total = 0;
     for (int w = 0; w < kVT / 32; w++) { if (w < warp) wpre += s_wsum[w]; total += s_wsum[w]; }
     if (tid == 0) {
-        s_pre = lookback(a.status, tile, total, a.err);
+        s_pre = lookback(a.status, tile, total, a.err, a.spin_limit);
         if (i0 + kVR >= n) *a.nout = (uint32_t)(s_pre + total);
     }
     __syncthreads();
@@ -980,6 +998,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         ea.p = p; ea.ext = B.ext.as<float>(); ea.keys = B.keys0.as<uint32_t>(); ea.vals = B.vals0.as<uint32_t>();
         ea.cap = cap; ea.npairs = (unsigned long long*)(scr + 14); ea.status = B.status.as<unsigned long long>();
         ea.counter = scr + VS_EMIT; ea.err = scr + VS_ERR; ea.ovf = scr + VS_OVF;
+        ea.spin_limit = g_dl_wait.spin_limit;
         vox_emit_k<<<emitTiles, kVT, 0, st>>>(ea);
         unsigned long long npairs = 0;
         {
@@ -1024,6 +1043,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
                 sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout; sp.segs = sg;
                 sp.glob_off = B.hist.as<uint32_t>(); sp.status = B.status.as<uint32_t>(); sp.counter = scr + VS_SORT + ps;
                 sp.err = scr + VS_ERR; sp.shift = 8 * ps; sp.pass = ps; sp.passes = passes;
+                sp.spin_limit = g_dl_wait.spin_limit;
                 dlsort::pass_k<8><<<sortTiles, dlsort::kThreads, 0, st>>>(sp);
                 std::swap(kin, kout);
                 std::swap(vin, vout);
@@ -1041,7 +1061,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         HeadsArgs ha;
         ha.keys = keysF; ha.npairs = (const unsigned long long*)(scr + 14); ha.bkey = B.bkey.as<uint32_t>();
         ha.bstart = B.bstart.as<uint32_t>(); ha.nblocks = scr + VS_NBLK; ha.status = B.status.as<unsigned long long>();
-        ha.counter = scr + VS_HEADS; ha.err = scr + VS_ERR;
+        ha.counter = scr + VS_HEADS; ha.err = scr + VS_ERR; ha.spin_limit = g_dl_wait.spin_limit;
         vox_heads_k<<<headTiles, kVT, 0, st>>>(ha);
 
         // learned block order (and per-block features for cost logging)
@@ -1057,6 +1077,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             sa.w = dev->vox_sched ? (const __nv_bfloat16*)dl_mlp_weights(dev->vox_sched) : nullptr;
             sa.feat = logBlocks ? B.sfeat.as<float>() : nullptr;
             sa.bucket = B.sbucket.as<uint32_t>(); sa.hist = B.shist.as<uint32_t>(); sa.work = B.swork.as<uint32_t>();
+            sa.err = scr + VS_ERR;
             const uint32_t sg = (uint32_t)std::min<uint64_t>((maxBlocks + kVSchedThreads - 1) / kVSchedThreads, 4096);
             if (sa.w) cudaMemsetAsync(B.shist.p, 0, 1024, st);
             vox_sched_pred_k<<<sg, kVSchedThreads, 0, st>>>(sa);
@@ -1070,7 +1091,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         va.p = p; va.rec = B.rec.as<VoxRec>(); va.vals = valsF; va.bkey = B.bkey.as<uint32_t>();
         va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
         va.counter = scr + VS_EVAL; va.evals = nullptr;
-        va.work = work; va.cycles = logBlocks ? B.scycles.as<uint32_t>() : nullptr;
+        va.work = work; va.cycles = logBlocks ? B.scycles.as<uint32_t>() : nullptr; va.err = scr + VS_ERR;
         vox_eval_k<<<dev->sm_count * 32, 64, 0, st>>>(va);
 
         uint32_t hn[2] = {0, 0};
@@ -1102,7 +1123,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         ca.p = p; ca.bkey = B.bkey.as<uint32_t>(); ca.masks = B.masks.as<uint2>(); ca.nblocks = scr + VS_NBLK;
         ca.out_idx = B.oidx.as<uint32_t>(); ca.out_lo = B.olo.as<uint32_t>(); ca.out_hi = B.ohi.as<uint32_t>();
         ca.nout = scr + VS_NOUT; ca.status = B.status.as<unsigned long long>(); ca.counter = scr + VS_COMPACT;
-        ca.err = scr + VS_ERR;
+        ca.err = scr + VS_ERR; ca.spin_limit = g_dl_wait.spin_limit;
         vox_compact_k<<<compTiles, kVT, 0, st>>>(ca);
         uint32_t h2[16];
         if (cudaMemcpyAsync(h2, scr, 64, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {

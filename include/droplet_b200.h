@@ -283,6 +283,25 @@ int dl_renderer_launch_count(dl_renderer* r, uint64_t* count);
 /* Keep the last single-view frame's f32 accumulator (r, g, b, T) for "accum". */
 int dl_renderer_set_debug(dl_renderer* r, int keep_intermediates);
 
+/* ---- bounded device waits (no reference counterpart; the reference throws
+ * on device set-up failure, src/gpu/device.ts:29-35, and has no device-side
+ * waits).  Every decoupled look-back (depth sort, pair emission, pair sort,
+ * the sorter, the voxelizer's binning, block heads and compaction) polls an
+ * unpublished predecessor at most `polls` times, then sets a timeout bit that
+ * the call returns as DL_E_TIMEOUT; the kernels after it skip their work, so
+ * the device stays usable.  polls 0 restores the default (2^21, about 0.2 s).
+ * Process-wide; for tests of the failure path. */
+int dl_test_set_wait_limit(uint32_t polls);
+/* Test hook: CTA `tile` (a global CTA index) of one stage publishes no status,
+ * so that its successors run into the wait limit.  stage: 0 none (default),
+ * 1 the depth sort's first pass, 2 pair emission, 3 the pair sort's first pass. */
+int dl_test_withhold_status(int stage, uint32_t tile);
+/* Test hook: the library's next `after` device allocations succeed and the
+ * one after them fails as cudaMalloc does when the device is out of memory
+ * (the call returns DL_E_OOM); then the hook switches itself off.  Negative:
+ * off.  Process-wide. */
+int dl_test_fail_allocation(int after);
+
 #ifdef __cplusplus
 }
 #endif
