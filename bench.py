@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-tune", action="store_true", help="skip the autotuner (default knobs)")
+    p.add_argument("--raster-shape", default=None,
+                   help="with --no-tune: the rasterizer work item (8x4, 16x2, 4x8, 8x8x2, 8x4-f32x2)")
     p.add_argument("--views", type=int, default=64)
     p.add_argument("--splats", type=int, default=3_000_000)
     p.add_argument("--no-e2e", action="store_true")
@@ -350,6 +352,8 @@ def run_ours(args, rank, world, local_rank):
         return ms
 
     # autotuner (untimed): pair-sort digit width, raster work-item shape, CTAs/SM
+    if args.no_tune and args.raster_shape:
+        r.set_tuning(raster_shape=args.raster_shape)
     tuning = None if args.no_tune else r.autotune(scene, cams, flags=FAST, reps=2)
 
     from droplet_b200 import learned

@@ -66,7 +66,7 @@ class DlRendererOpts(ctypes.Structure):
 
 class DlTuning(ctypes.Structure):
     _fields_ = [("pair_sort_bits", ctypes.c_int32), ("raster_shape", ctypes.c_int32),
-                ("raster_ctas_per_sm", ctypes.c_int32)]
+                ("raster_ctas_per_sm", ctypes.c_int32), ("bin_tile", ctypes.c_int32)]
 
 
 class DlVoxOpts(ctypes.Structure):

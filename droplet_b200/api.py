@@ -190,18 +190,22 @@ class Renderer:
         check(_lib.load().dl_render_batch(self.handle, scene._h, cams, n, _bg(background), ptrs, flags))
         return host
 
-    RASTER_SHAPES = ("8x4", "16x2", "4x8", "8x8x2")
+    RASTER_SHAPES = ("8x4", "16x2", "4x8", "8x8x2", "8x4-f32x2")
 
-    def set_tuning(self, pair_sort_bits: int = 8, raster_shape: str = "8x4", raster_ctas_per_sm: int = 0):
+    BIN_TILES = ("16x16", "8x8", "32x8")
+
+    def set_tuning(self, pair_sort_bits: int = 8, raster_shape: str = "8x4", raster_ctas_per_sm: int = 0,
+                   bin_tile: str = "16x16"):
         """Timing-only knobs of rendered frames (dl_tuning); no knob changes a pixel."""
-        t = _lib.DlTuning(int(pair_sort_bits), self.RASTER_SHAPES.index(raster_shape), int(raster_ctas_per_sm))
+        t = _lib.DlTuning(int(pair_sort_bits), self.RASTER_SHAPES.index(raster_shape), int(raster_ctas_per_sm),
+                          self.BIN_TILES.index(bin_tile))
         check(_lib.load().dl_renderer_set_tuning(self.handle, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
         t = _lib.DlTuning()
         check(_lib.load().dl_renderer_get_tuning(self.handle, ctypes.byref(t)))
         return {"pair_sort_bits": t.pair_sort_bits, "raster_shape": self.RASTER_SHAPES[t.raster_shape],
-                "raster_ctas_per_sm": t.raster_ctas_per_sm}
+                "raster_ctas_per_sm": t.raster_ctas_per_sm, "bin_tile": self.BIN_TILES[t.bin_tile]}
 
     def autotune(self, scene: Scene, cameras: Sequence[RenderCamera], background=None, flags: int = 0,
                  reps: int = 3) -> dict:

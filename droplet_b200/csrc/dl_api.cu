@@ -374,14 +374,15 @@ extern "C" int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst
 
 extern "C" int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t) {
     if (!r || !t) { dl_set_error("dl_renderer_set_tuning: NULL argument"); return DL_E_INVALID_ARG; }
-    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 3 ||
-        t->raster_ctas_per_sm < 0 || t->raster_ctas_per_sm > 5) {
+    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 4 ||
+        t->raster_ctas_per_sm < 0 || t->raster_ctas_per_sm > 5 || t->bin_tile < 0 || t->bin_tile > 2) {
         dl_set_error("dl_renderer_set_tuning: knob out of range");
         return DL_E_INVALID_ARG;
     }
     r->tune.pair_bits = t->pair_sort_bits;
     r->tune.shape = t->raster_shape;
     r->tune.ctas_per_sm = t->raster_ctas_per_sm;
+    r->tune.bin_tile = t->bin_tile;
     return DL_OK;
 }
 
@@ -390,6 +391,7 @@ extern "C" int dl_renderer_get_tuning(dl_renderer* r, dl_tuning* t) {
     t->pair_sort_bits = r->tune.pair_bits;
     t->raster_shape = r->tune.shape;
     t->raster_ctas_per_sm = r->tune.ctas_per_sm;
+    t->bin_tile = r->tune.bin_tile;
     return DL_OK;
 }
 
@@ -429,14 +431,21 @@ extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera
     DlTuning cur = r->tune;
     double curMs = 0.0;
     int rc = timeOne(cur, &curMs);
-    const int bitsC[4] = {8, 7, 6, 8}, shapeC[4] = {0, 1, 2, 3}, ctasC[4] = {0, 4, 3, 0};
-    const int nC[3] = {3, 4, 3};
-    for (int knob = 0; knob < 3 && rc == DL_OK; knob++) {
+    // shape 4 (two splats per step in f32x2) exists for the fast arithmetic only
+    const int bitsC[5] = {8, 7, 6, 8, 8}, shapeC[5] = {4, 0, 1, 2, 3}, ctasC[5] = {0, 4, 3, 0, 0};
+    const int tileC[5] = {0, 1, 2, 0, 0};
+    const bool fast = (flags & DL_BATCH_FAST_EXP) != 0;
+    const int nC[4] = {3, 5, 3, 3};
+    for (int knob = 0; knob < 4 && rc == DL_OK; knob++) {
         for (int c = 0; c < nC[knob] && rc == DL_OK; c++) {
             DlTuning t = cur;
             if (knob == 0) { if (t.pair_bits == bitsC[c]) continue; t.pair_bits = bitsC[c]; }
-            if (knob == 1) { if (t.shape == shapeC[c]) continue; t.shape = shapeC[c]; }
+            if (knob == 1) {
+                if (t.shape == shapeC[c] || (shapeC[c] == 4 && !fast)) continue;
+                t.shape = shapeC[c];
+            }
             if (knob == 2) { if (t.ctas_per_sm == ctasC[c]) continue; t.ctas_per_sm = ctasC[c]; }
+            if (knob == 3) { if (t.bin_tile == tileC[c]) continue; t.bin_tile = tileC[c]; }
             double ms = 0.0;
             rc = timeOne(t, &ms);
             if (rc == DL_OK && ms < curMs) { cur = t; curMs = ms; }
@@ -446,7 +455,12 @@ extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera
     cudaEventDestroy(e1);
     r->tune = cur;
     if (rc != DL_OK) return rc;
-    if (best) { best->pair_sort_bits = cur.pair_bits; best->raster_shape = cur.shape; best->raster_ctas_per_sm = cur.ctas_per_sm; }
+    if (best) {
+        best->pair_sort_bits = cur.pair_bits;
+        best->raster_shape = cur.shape;
+        best->raster_ctas_per_sm = cur.ctas_per_sm;
+        best->bin_tile = cur.bin_tile;
+    }
     if (best_ms) *best_ms = curMs;
     return DL_OK;
 }

@@ -47,10 +47,14 @@ struct DlView {
     float view[16];              // column-major world->camera
     float width, height, focal, cx, cy, near_f, far_f;
     double near_d, far_d;
-    uint32_t W, H, tilesX, tilesY, numTiles;
+    uint32_t W, H;
+    uint32_t tilesX, tilesY, numTiles;   // the binning tile grid (tileW x tileH-pixel tiles)
     int32_t projection;          // 0 pinhole, 1 equirect
-    uint32_t maxCoverage;
+    uint32_t maxCoverage;        // the reference's maxCoveragePerSplat, counted in 16x16 tiles
     float bg[4];
+    uint32_t tileW, tileH;       // binning tile size: 16x16 (the reference's TILE_SIZE) unless tuned
+    uint32_t refTilesX, refTilesY;   // the reference's 16x16 tile grid (coverage count, phantom rule)
+    uint32_t binCap;             // binning tiles one splat may take: maxCoverage at 16x16, else no cap
 };
 
 // Device-resident scene (struct of arrays, as SplatData).

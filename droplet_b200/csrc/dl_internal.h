@@ -100,6 +100,7 @@ struct DlTuning {
     int pair_bits = 8;        // pair-sort digit width 6..8
     int shape = 0;            // rasterizer work item: 0 8x4, 1 16x2, 2 4x8, 3 8x8 (two pixels per lane)
     int ctas_per_sm = 0;      // persistent rasterizer CTAs per SM; 0 = occupancy limit
+    int bin_tile = 0;         // binning tile: 0 16x16 (the reference's), 1 8x8, 2 32x8
 };
 
 constexpr int kUploadChunks = 8;   // splat ranges of an upload that overlaps projection

@@ -108,6 +108,11 @@ int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlVie
     v->numTiles = v->tilesX * v->tilesY;
     v->projection = cam->projection;
     v->maxCoverage = maxCov;
+    v->tileW = DL_TILE;
+    v->tileH = DL_TILE;
+    v->refTilesX = v->tilesX;
+    v->refTilesY = v->tilesY;
+    v->binCap = maxCov;
     const float dflt[4] = {0.0f, 0.0f, 0.0f, 1.0f};
     for (int k = 0; k < 4; k++) v->bg[k] = bg ? bg[k] : dflt[k];
     return DL_OK;
@@ -276,18 +281,62 @@ struct FrameDims {
     bool f16rec = false, fastExp = false, f64deg = false, cullOff = false;
     int subLw = 3;                       // rasterizer work item width log2 (8x4)
     bool ppl2 = false;                   // two pixels per lane (8x8 work items)
+    bool x2 = false;                     // two splats per step in f32x2 arithmetic (fast variant)
+    int iptLg = 3;                       // log2 of the rasterizer work items per binning tile
 };
 
+// Staging margin of the rasterizer (pixels): a splat is staged for a work
+// item when its box widened by this much reaches a pixel centre of the item.
+// 1/64 px is far above the f32 rounding of the box test (under 1e-3 px at
+// the largest image coordinates) and below the 0.1% relative margin between
+// a splat's box and the region where its alpha reaches 1/255.
+// DL_STAGE_PAD overrides it (pixels) for measurements.
+float stage_pad() {
+    static float pad = -1.0f;
+    if (pad < 0.0f) {
+        const char* e = getenv("DL_STAGE_PAD");
+        pad = e ? std::max(0.015625f, (float)atof(e)) : 0.015625f;
+    }
+    return pad;
+}
+
+// Bin a frame's views with tw x th-pixel tiles instead of the reference's
+// 16x16.  Only when no view can truncate a splat's coverage (maxCoverage at
+// least the view's 16x16 tile count), because the truncation keeps a
+// row-major prefix of 16x16 tiles (src/render/shaders/emit-pairs.ts:46-53);
+// without it every pixel is offered the same splats under any tile, so the
+// pixels are the same.  Returns false (views unchanged) when that does not hold
+// or the grid is too large.
+bool dl_retile_views(DlView* v, uint32_t V, uint32_t tw, uint32_t th) {
+    for (uint32_t i = 0; i < V; i++) {
+        const uint64_t ref = (uint64_t)v[i].refTilesX * v[i].refTilesY;
+        const uint64_t tx = (v[i].W + tw - 1) / tw, ty = (v[i].H + th - 1) / th;
+        if (v[i].maxCoverage < ref || tx > 0x7fffu || ty > 0x7fffu || tx * ty >= (1u << 20)) return false;
+    }
+    for (uint32_t i = 0; i < V; i++) {
+        v[i].tileW = tw;
+        v[i].tileH = th;
+        v[i].tilesX = (v[i].W + tw - 1) / tw;
+        v[i].tilesY = (v[i].H + th - 1) / th;
+        v[i].numTiles = v[i].tilesX * v[i].tilesY;
+        v[i].binCap = 0xffffffffu;
+    }
+    return true;
+}
+
 // Persistent rasterizer grid: every SM filled to its occupancy limit.
-uint32_t raster_grid(bool fastExp, bool ppl2) {
-    static int cached[64][4] = {};
+uint32_t raster_grid(bool fastExp, bool ppl2, bool x2) {
+    static int cached[64][5] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    int* c = (dev >= 0 && dev < 64) ? &cached[dev][(fastExp ? 1 : 0) + (ppl2 ? 2 : 0)] : nullptr;
+    const int kind = x2 ? 4 : (fastExp ? 1 : 0) + (ppl2 ? 2 : 0);
+    int* c = (dev >= 0 && dev < 64) ? &cached[dev][kind] : nullptr;
     if (c && *c) return (uint32_t)*c;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (ppl2) {
+    if (x2) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_x2_k<false>, dlr::kRasterThreads, 0);
+    } else if (ppl2) {
         if (fastExp) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize2_k<false>, dlr::kRasterThreads, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize2_k<true>, dlr::kRasterThreads, 0);
     } else if (fastExp) {
@@ -329,7 +378,15 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
     d.f64deg = (flags & DL_BATCH_F64_DEGENERATE) != 0;
     d.cullOff = (flags & DL_BATCH_CULL_OFFSCREEN) != 0;
-    d.rasterGrid = raster_grid(d.fastExp, d.ppl2);
+    d.x2 = t.shape == 4 && d.fastExp;    // the packed variant has the fast arithmetic only
+    // work items must fit the binning tile (every view of a frame has the same tile)
+    const uint32_t tw = V ? hv[0].tileW : DL_TILE, th = V ? hv[0].tileH : DL_TILE;
+    const uint32_t iw = d.ppl2 ? 8u : (1u << d.subLw), ih = d.ppl2 ? 8u : (32u >> d.subLw);
+    if (iw > tw || ih > th) { d.subLw = 3; d.ppl2 = false; }
+    const uint32_t ipt = tw * th / (d.ppl2 ? 64u : 32u);
+    d.iptLg = 0;
+    while ((1u << d.iptLg) < ipt) d.iptLg++;
+    d.rasterGrid = raster_grid(d.fastExp, d.ppl2, d.x2);
     if (t.ctas_per_sm > 0) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -569,16 +626,21 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ra.accum = f.accum;
     ra.work = work;
     ra.item_base = 0;
-    ra.num_items = (d.ppl2 ? 4u : 8u) * d.totalTiles;
+    ra.num_items = (1u << d.iptLg) * d.totalTiles;
+    ra.ipt_lg = d.iptLg;
     ra.work_counter = f.scr + SC_WORK_CTR;
     ra.eval_count = f.evalCount;
     ra.tile_evals = f.tileEvals;
     ra.tile_cycles = f.tileCycles;
     ra.sub_lw = d.subLw;
     ra.rec_box = d.cullOff ? 1 : 0;
+    ra.stage_pad = stage_pad();
     const bool count = ra.eval_count || ra.tile_evals;
     auto raster = [&](const dlr::RasterArgs& x) {
-        if (d.ppl2) {
+        if (d.x2 && !count) {
+            if (x.tile_cycles) dlr::rasterize_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            else dlr::rasterize_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+        } else if (d.ppl2) {
             if (d.fastExp) {
                 if (count) dlr::rasterize2_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
                 else dlr::rasterize2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
@@ -600,7 +662,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
         // orders, so a range of views is a range of items); each range's images
         // go back to the host on the read-back stream while the next rasterizes.
         const uint32_t per = (d.V + (uint32_t)f.rbGroups - 1) / (uint32_t)f.rbGroups;
-        const uint32_t ipt = d.ppl2 ? 4u : 8u;
+        const uint32_t ipt = 1u << d.iptLg;
         static_assert(SC_RASTER_CTR + kReadBackGroups <= kScratchWords, "scratch words");
         DL_CK(cudaMemsetAsync(f.scr + SC_RASTER_CTR, 0, 4ull * kReadBackGroups, st));
         for (uint32_t v0 = 0, g = 0; v0 < d.V; v0 += per, g++) {
@@ -635,6 +697,12 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     if (r->pair_cap_per_view == 0) r->pair_cap_per_view = std::max<uint64_t>(1u << 20, 4ull * N);
     // the plain path keeps the default knobs
     const DlTuning tune = (flags & DL_BATCH_PLAIN) ? DlTuning() : r->tune;
+    std::vector<DlView> retiled;
+    if (tune.bin_tile == 1 || tune.bin_tile == 2) {
+        const uint32_t tw = tune.bin_tile == 1 ? 8u : 32u, th = 8u;
+        retiled.assign(hv, hv + V);
+        if (dl_retile_views(retiled.data(), V, tw, th)) hv = retiled.data();
+    }
     FrameDims d = frame_dims(hv, V, N, r->pair_cap_per_view, flags, tune);
     const bool countEvals = (flags & DL_BATCH_COUNT_EVALS) != 0;
     r->launches = 0;
@@ -820,7 +888,9 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             const uint64_t* sp = reinterpret_cast<const uint64_t*>(&sc);
             key.insert(key.end(), sp, sp + sizeof(DlSceneDev) / 8);
             key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid,
-                                   (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2, g_dl_wait.spin_limit,
+                                   (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2, (uint64_t)d.x2,
+                                   (uint64_t)d.iptLg, (uint64_t)hv[0].tileW, (uint64_t)hv[0].tileH,
+                                   g_dl_wait.spin_limit,
                                    g_dl_wait.withheld(DL_WAIT_STAGE_DEPTH_SORT), g_dl_wait.withheld(DL_WAIT_STAGE_EMIT),
                                    g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT)});
             if (!r->graph_exec || key != r->graph_key) {

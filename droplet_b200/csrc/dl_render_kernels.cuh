@@ -382,8 +382,8 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         uint32_t minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - radius) / 16.0f)));
         uint32_t minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - radius) / 16.0f)));
         float fx1 = floorf((screenX + radius) / 16.0f), fy1 = floorf((screenY + radius) / 16.0f);
-        uint32_t maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
-        uint32_t maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+        uint32_t maxTX = dl_sat_u32(fminf((float)u.refTilesX - 1.0f, fx1));
+        uint32_t maxTY = dl_sat_u32(fminf((float)u.refTilesY - 1.0f, fy1));
         const float alpha = (sig * radiusFade) * aaFactor;
         float boxX = radius, boxY = radius;          // half-extents the rasterizer tests (cull mode)
         // the rasterizer's alpha is opacity * (exp(-q/2) - exp(-4.5)) with the
@@ -421,15 +421,15 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
                 minTY = dl_sat_u32(fmaxf(0.0f, floorf((screenY - ey) / 16.0f)));
                 fx1 = floorf((screenX + ex) / 16.0f);
                 fy1 = floorf((screenY + ey) / 16.0f);
-                maxTX = dl_sat_u32(fminf((float)u.tilesX - 1.0f, fx1));
-                maxTY = dl_sat_u32(fminf((float)u.tilesY - 1.0f, fy1));
+                maxTX = dl_sat_u32(fminf((float)u.refTilesX - 1.0f, fx1));
+                maxTY = dl_sat_u32(fminf((float)u.refTilesY - 1.0f, fy1));
             }
         }
         // A box right edge left of x = 0 (or bottom edge above y = 0) still counts
         // column (row) 0 after the saturation, but no pixel centre can pass its
         // box test there: flag it so the rasterizer skips these pairs unread.
-        const uint32_t phantom = ((fx1 < 0.0f) ? 0x8000u : 0u) | ((fy1 < 0.0f) ? 0x80000000u : 0u);
-        const bool hasTiles = maxTX >= minTX && maxTY >= minTY;
+        uint32_t phantom = ((fx1 < 0.0f) ? 0x8000u : 0u) | ((fy1 < 0.0f) ? 0x80000000u : 0u);
+        bool hasTiles = maxTX >= minTX && maxTY >= minTY;
         if (a.cull_offscreen) {
             // a splat with no tile, or only phantom tiles, touches no pixel:
             // leaving it out of the depth order changes no tile list's order
@@ -437,6 +437,27 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             a.keys[o] = dl_sortable_key(depthKey);
             const uint32_t m = __activemask();
             if ((threadIdx.x & 31) == (uint32_t)(__ffs(m) - 1)) atomicAdd(&s_vis[v], (uint32_t)__popc(m));
+        }
+        if (u.tileW != DL_TILE || u.tileH != DL_TILE) {
+            // A tuned binning tile: the splat goes to the tiles of that grid that
+            // its box (the one the rasterizer tests, or the radius square) meets
+            // on the image.  The host uses another tile only when the reference's
+            // maxCoverage cannot truncate any splat of the view, so every pixel
+            // is offered the same splats as with 16x16 tiles; splats that meet
+            // no tile of the image get none (they touch no pixel).
+            const float bx = a.cull_offscreen ? boxX : radius, by = a.cull_offscreen ? boxY : radius;
+            const float tw = (float)u.tileW, th = (float)u.tileH;
+            const float x0 = floorf((screenX - bx) / tw), x1 = floorf((screenX + bx) / tw);
+            const float y0 = floorf((screenY - by) / th), y1 = floorf((screenY + by) / th);
+            hasTiles = x1 >= 0.0f && y1 >= 0.0f && x0 <= (float)u.tilesX - 1.0f && y0 <= (float)u.tilesY - 1.0f &&
+                       x1 >= x0 && y1 >= y0;
+            if (hasTiles) {
+                minTX = (uint32_t)fmaxf(x0, 0.0f);
+                minTY = (uint32_t)fmaxf(y0, 0.0f);
+                maxTX = (uint32_t)fminf(x1, (float)u.tilesX - 1.0f);
+                maxTY = (uint32_t)fminf(y1, (float)u.tilesY - 1.0f);
+            }
+            phantom = 0u;
         }
         // deferred: colour_k fills the colour once the SH has arrived
         float col0 = 0.0f, col1 = 0.0f, col2 = 0.0f;
@@ -602,7 +623,7 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
             const uint32_t g = a.sorted_vals[vo + r];
             const uint2 bb = a.bbox[vo + g];
             gs[j] = g | ((bb.y & 0x80008000u) ? kPhantomBit : 0u);
-            cnt[j] = bbox_count(bb, u.maxCoverage);
+            cnt[j] = bbox_count(bb, u.binCap);
             mins[j] = bb.x;
             spans[j] = (bb.y & 0x7fffu) - (bb.x & 0xffffu) + 1u;
         }
@@ -792,8 +813,9 @@ __device__ __forceinline__ void tile_features(const DlView& u, const uint32_t* t
     x[8] = tx == 0 ? 1.0f : 0.0f;
     x[9] = logf((float)u.W * (float)u.H) * (1.0f / 16.0f);
     x[10] = log1pf((float)to[u.numTiles] / (float)u.numTiles) * 0.1f;
-    const float wx = fminf(16.0f, (float)u.W - 16.0f * tx), wy = fminf(16.0f, (float)u.H - 16.0f * ty);
-    x[11] = wx * wy * (1.0f / 256.0f);
+    const float tw = (float)u.tileW, th = (float)u.tileH;
+    const float wx = fminf(tw, (float)u.W - tw * tx), wy = fminf(th, (float)u.H - th * ty);
+    x[11] = wx * wy / (tw * th);
 }
 
 // Per global tile features (cost logging).
@@ -907,7 +929,10 @@ struct RasterArgs {
     uint32_t* tile_evals;          // optional [total tiles] evaluated pairs per tile
     uint32_t* tile_cycles;         // optional [total tiles] SM cycles / 16 spent per tile
     int sub_lw;                    // log2 of a work item's width: 3 (8x4), 4 (16x2) or 2 (4x8) pixels
+    int ipt_lg;                    // log2 of the work items per tile
     int rec_box;                   // 1: recA.zw are the half-extents to test (cull mode), else (radius, depth)
+    float stage_pad;               // a splat is staged for a sub-tile when its box, widened by this many
+                                   // pixels, reaches one of the sub-tile's pixel centres
 };
 
 constexpr int kRasterThreads = 256;
@@ -1036,15 +1061,15 @@ __device__ __forceinline__ void raster_subtile(const RasterArgs& a, uint32_t v, 
     const int lane = threadIdx.x & 31;
     const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
     // a work item is sw x sh pixels (sw * sh = 32), 8 items per 16x16 tile
-    const uint32_t lw = (uint32_t)a.sub_lw, sw = 1u << lw, sh = 32u >> lw, perRow = DL_TILE >> lw;
-    const uint32_t sx0 = tx * DL_TILE + (sub % perRow) * sw, sy0 = ty * DL_TILE + (sub / perRow) * sh;
+    const uint32_t lw = (uint32_t)a.sub_lw, sw = 1u << lw, sh = 32u >> lw, perRow = u.tileW >> lw;
+    const uint32_t sx0 = tx * u.tileW + (sub % perRow) * sw, sy0 = ty * u.tileH + (sub / perRow) * sh;
     const uint32_t x = sx0 + (lane & (sw - 1)), y = sy0 + (lane >> lw);
     const bool inImage = x < u.W && y < u.H;
     if (__all_sync(0xffffffffu, !inImage)) return;       // sub-tile entirely outside the image
     const long long t0 = a.tile_cycles ? clock64() : 0;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
-    const float rx0 = (float)sx0 + 0.5f - 1.0f, rx1 = (float)(sx0 + sw) - 0.5f + 1.0f;
-    const float ry0 = (float)sy0 + 0.5f - 1.0f, ry1 = (float)(sy0 + sh) - 0.5f + 1.0f;
+    const float rx0 = (float)sx0 + 0.5f - a.stage_pad, rx1 = (float)(sx0 + sw) - 0.5f + a.stage_pad;
+    const float ry0 = (float)sy0 + 0.5f - a.stage_pad, ry1 = (float)(sy0 + sh) - 0.5f + a.stage_pad;
     const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
     const uint32_t start = to[tile], end = to[tile + 1];
     const uint32_t* vals = a.pair_vals + a.pair_base[v];
@@ -1145,14 +1170,15 @@ __device__ __forceinline__ void raster_subtile2(const RasterArgs& a, uint32_t v,
     const DlView& u = a.views[v];
     const int lane = threadIdx.x & 31;
     const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
-    const uint32_t sx0 = tx * DL_TILE + (sub & 1u) * 8u, sy0 = ty * DL_TILE + (sub >> 1) * 8u;
+    const uint32_t perRow = u.tileW >> 3;       // 8x8 work items
+    const uint32_t sx0 = tx * u.tileW + (sub % perRow) * 8u, sy0 = ty * u.tileH + (sub / perRow) * 8u;
     const uint32_t x = sx0 + (lane & 7), y0 = sy0 + (lane >> 3), y1 = y0 + 4u;
     const bool in0 = x < u.W && y0 < u.H, in1 = x < u.W && y1 < u.H;
     if (__all_sync(0xffffffffu, !in0)) return;            // y1 > y0: no pixel of the item is inside
     const long long t0 = a.tile_cycles ? clock64() : 0;
     const float px = (float)x + 0.5f, py0 = (float)y0 + 0.5f, py1 = (float)y1 + 0.5f;
-    const float rx0 = (float)sx0 + 0.5f - 1.0f, rx1 = (float)(sx0 + 8u) - 0.5f + 1.0f;
-    const float ry0 = (float)sy0 + 0.5f - 1.0f, ry1 = (float)(sy0 + 8u) - 0.5f + 1.0f;
+    const float rx0 = (float)sx0 + 0.5f - a.stage_pad, rx1 = (float)(sx0 + 8u) - 0.5f + a.stage_pad;
+    const float ry0 = (float)sy0 + 0.5f - a.stage_pad, ry1 = (float)(sy0 + 8u) - 0.5f + a.stage_pad;
     const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
     const uint32_t start = to[tile], end = to[tile + 1];
     const uint32_t* vals = a.pair_vals + a.pair_base[v];
@@ -1260,7 +1286,185 @@ __device__ __forceinline__ void raster_subtile2(const RasterArgs& a, uint32_t v,
     if (a.tile_cycles && lane == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
 }
 
-// The two-pixels-per-lane rasterizer: 4 work items per tile.
+// ---- two splats per step in packed f32x2 arithmetic (fast variant only)
+// Same work item, staging and per-pixel arithmetic as raster_subtile's fast
+// loop, but the staged splats are taken two at a time: the quadratic form,
+// exponent and alpha of splats j and j+1 at the lane's pixel are evaluated
+// together with sm_100's two-wide FP32 instructions (__fadd2_rn, __fmul2_rn,
+// __ffma2_rn: per component the same IEEE operation as the scalar
+// instruction), then composited one after the other in depth order.  There
+// is no per-pixel box test: a staged splat reaches the sub-tile, and at
+// pixels outside its box the alpha test skips it (alpha < 1/255 there, see
+// tight_extent), so every pixel gets the same splats, values and order as in
+// raster_subtile.  Staged values are stored negated where that saves an
+// instruction: with na = -alpha, T*na*(-colour) = T*alpha*colour and
+// fma(T, na, T) = fma(-T, alpha, T) exactly.
+//
+// Shared memory per warp: 32 pairs of staged splats, 20 floats a pair:
+//   {-x0, -x1, -y0, -y1}, {A0, A1, B0, B1}, {C0, C1, -o0, -o1},
+//   {-r0, -g0, -b0, -r1}, {-g1, -b1, 0, 0}
+// (A, B, C: the conic scaled by -0.5 log2 e as in stage_chunk's fast path.)
+constexpr int kPairFloats = 20;
+
+__device__ __forceinline__ uint32_t stage_chunk_x2(const RasterArgs& a, const uint32_t* vals, uint32_t b,
+                                                   uint32_t end, uint64_t vo, float rx0, float rx1, float ry0,
+                                                   float ry1, uint32_t lmask, float* sp) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t e0 = b + lane, e1 = b + 32 + lane;
+    const uint32_t g0 = e0 < end ? __ldg(vals + e0) : kPhantomBit;
+    const uint32_t g1 = e1 < end ? __ldg(vals + e1) : kPhantomBit;
+    bool hit0 = false, hit1 = false;
+    float4 ra0 = make_float4(0, 0, 0, 0), ra1 = make_float4(0, 0, 0, 0);
+    if (!(g0 & kPhantomBit)) {
+        ra0 = __ldg(a.recA + vo + g0);
+        const float rx = ra0.z, ry = a.rec_box ? ra0.w : ra0.z;
+        hit0 = rx > 0.0f && !(ra0.x - rx > rx1) && !(ra0.x + rx < rx0) && !(ra0.y - ry > ry1) && !(ra0.y + ry < ry0);
+    }
+    if (!(g1 & kPhantomBit)) {
+        ra1 = __ldg(a.recA + vo + g1);
+        const float rx = ra1.z, ry = a.rec_box ? ra1.w : ra1.z;
+        hit1 = rx > 0.0f && !(ra1.x - rx > rx1) && !(ra1.x + rx < rx0) && !(ra1.y - ry > ry1) && !(ra1.y + ry < ry0);
+    }
+    if (__ballot_sync(0xffffffffu, hit0 || hit1) == 0u) return 0u;
+    uint32_t n = 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        bool hit = h ? hit1 : hit0;
+        const uint32_t g = h ? g1 : g0;
+        const float4 ra = h ? ra1 : ra0;
+        float A = 0.0f, B = 0.0f, C = 0.0f, al = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+        if (hit) {
+            if (a.recBC) {
+                const float4 p = __ldg(a.recBC + 2 * (vo + g));
+                const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
+                A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
+            } else {
+                const uint4 hv = __ldg(a.recH + vo + g);
+                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
+                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
+                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
+                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
+                A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+            }
+            if (!a.rec_box) {
+                float ex, ey;
+                tight_extent(A, B, C, ra.z, ex, ey);
+                hit = !(ra.x - ex > rx1) && !(ra.x + ex < rx0) && !(ra.y - ey > ry1) && !(ra.y + ey < ry0);
+            }
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const uint32_t slot = n + __popc(m & lmask);
+            float* P = sp + (slot >> 1) * kPairFloats;
+            const uint32_t c = slot & 1u;
+            P[0 + c] = -ra.x;
+            P[2 + c] = -ra.y;
+            P[4 + c] = -0.72134752044448170f * A;
+            P[6 + c] = -1.4426950408889634f * B;
+            P[8 + c] = -0.72134752044448170f * C;
+            P[10 + c] = -al;
+            P[12 + 3 * c] = -cr;
+            P[13 + 3 * c] = -cg;
+            P[14 + 3 * c] = -cb;
+        }
+        n += __popc(m);
+    }
+    if ((n & 1u) && lane == 0) {
+        // odd count: a splat of opacity 0 fills the pair (alpha 0 is skipped)
+        float* P = sp + (n >> 1) * kPairFloats;
+        P[1] = 0.0f; P[3] = 0.0f; P[5] = 0.0f; P[7] = 0.0f; P[9] = 0.0f; P[11] = -0.0f;
+        P[15] = 0.0f; P[16] = 0.0f; P[17] = 0.0f;
+    }
+    return n;
+}
+
+template <bool kCycles>
+__device__ __forceinline__ void raster_subtile_x2(const RasterArgs& a, uint32_t v, uint32_t tile, uint32_t sub,
+                                                  uint32_t gt, float* sp) {
+    const DlView& u = a.views[v];
+    const int lane = threadIdx.x & 31;
+    const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
+    const uint32_t lw = (uint32_t)a.sub_lw, sw = 1u << lw, sh = 32u >> lw, perRow = u.tileW >> lw;
+    const uint32_t sx0 = tx * u.tileW + (sub % perRow) * sw, sy0 = ty * u.tileH + (sub / perRow) * sh;
+    const uint32_t x = sx0 + (lane & (sw - 1)), y = sy0 + (lane >> lw);
+    const bool inImage = x < u.W && y < u.H;
+    if (__all_sync(0xffffffffu, !inImage)) return;
+    const long long t0 = kCycles ? clock64() : 0;
+    const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+    const float pad = a.stage_pad;
+    const float rx0 = (float)sx0 + 0.5f - pad, rx1 = (float)(sx0 + sw) - 0.5f + pad;
+    const float ry0 = (float)sy0 + 0.5f - pad, ry1 = (float)(sy0 + sh) - 0.5f + pad;
+    const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    const uint32_t start = to[tile], end = to[tile + 1];
+    const uint32_t* vals = a.pair_vals + a.pair_base[v];
+    const uint64_t vo = (uint64_t)v * a.view_stride;
+    const uint32_t lmask = dl_lanemask_lt();
+    const float2 px2 = make_float2(px, px), py2 = make_float2(py, py);
+    const float2 nfloor2 = make_float2(-DL_GAUSS_FLOOR, -DL_GAUSS_FLOOR);
+
+    float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
+    bool done = !inImage;
+    for (uint32_t b = start; b < end; b += 64) {
+        const uint32_t n = stage_chunk_x2(a, vals, b, end, vo, rx0, rx1, ry0, ry1, lmask, sp);
+        if (n == 0u) continue;
+        __syncwarp();
+        if (!done) {
+            for (uint32_t j = 0; j < n; j += 2) {
+                const float4* P = reinterpret_cast<const float4*>(sp + (j >> 1) * kPairFloats);
+                const float4 q0 = P[0], q1 = P[1], q2 = P[2];
+                const float2 dx = __fadd2_rn(px2, make_float2(q0.x, q0.y));
+                const float2 dy = __fadd2_rn(py2, make_float2(q0.z, q0.w));
+                const float2 t = __fmul2_rn(make_float2(q1.z, q1.w), dy);
+                const float2 qq = __ffma2_rn(make_float2(q1.x, q1.y), dx, t);
+                const float2 uu = __fmul2_rn(__fmul2_rn(make_float2(q2.x, q2.y), dy), dy);
+                const float2 pw = __ffma2_rn(dx, qq, uu);
+                float e0, e1;
+                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(pw.x));
+                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(pw.y));
+                const float2 na = __fmul2_rn(make_float2(q2.z, q2.w), __fadd2_rn(make_float2(e0, e1), nfloor2));
+                // the shader's skips: power > 0, alpha < 1/255
+                const bool ok0 = !(pw.x > 0.0f) && !(na.x > -DL_MIN_ALPHA);
+                const bool ok1 = !(pw.y > 0.0f) && !(na.y > -DL_MIN_ALPHA);
+                if (ok0 || ok1) {
+                    const float4 q3 = P[3];
+                    if (ok0) {
+                        const float w = T * na.x;
+                        c0 = __fmaf_rn(w, q3.x, c0);
+                        c1 = __fmaf_rn(w, q3.y, c1);
+                        c2 = __fmaf_rn(w, q3.z, c2);
+                        T = __fmaf_rn(T, na.x, T);
+                        if (T < DL_MIN_T) { done = true; break; }
+                    }
+                    if (ok1) {
+                        const float4 q4 = P[4];
+                        const float w = T * na.y;
+                        c0 = __fmaf_rn(w, q3.w, c0);
+                        c1 = __fmaf_rn(w, q4.x, c1);
+                        c2 = __fmaf_rn(w, q4.y, c2);
+                        T = __fmaf_rn(T, na.y, T);
+                        if (T < DL_MIN_T) { done = true; break; }
+                    }
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+        __syncwarp();                                   // staging area is reused by the next step
+    }
+    if (inImage) {
+        // finalize.ts:30-43
+        const float rr = fminf(fmaxf(c0 + T * u.bg[0], 0.0f), 1.0f);
+        const float gg = fminf(fmaxf(c1 + T * u.bg[1], 0.0f), 1.0f);
+        const float bb = fminf(fmaxf(c2 + T * u.bg[2], 0.0f), 1.0f);
+        const float aa = fminf(fmaxf((1.0f - T) + T * u.bg[3], 0.0f), 1.0f);
+        const uint32_t out = dl_sat_u32(rr * 255.0f + 0.5f) | (dl_sat_u32(gg * 255.0f + 0.5f) << 8) |
+                             (dl_sat_u32(bb * 255.0f + 0.5f) << 16) | (dl_sat_u32(aa * 255.0f + 0.5f) << 24);
+        a.outs[v][(uint64_t)y * u.W + x] = out;
+        if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c0, c1, c2, T);
+    }
+    if (kCycles && lane == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
+}
+
+// The two-pixels-per-lane rasterizer: 8x8-pixel work items (4 per 16x16 tile).
 template <bool kExactExp, bool kCount = false>
 __global__ void __launch_bounds__(kRasterThreads, 5) rasterize2_k(RasterArgs a) {
     __shared__ float4 s_a[kRasterWarps][64];
@@ -1272,9 +1476,10 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize2_k(RasterArgs a) 
         if (lane == 0) item = a.item_base + atomicAdd(a.work_counter, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= a.num_items) return;
-        const uint32_t gt = a.work ? a.work[item >> 2] : (item >> 2);
+        const uint32_t gt = a.work ? a.work[item >> a.ipt_lg] : (item >> a.ipt_lg);
         const uint32_t v = view_of_tile(a, gt);
-        raster_subtile2<kExactExp, kCount>(a, v, gt - a.tile_base[v], item & 3u, gt, s_a[warp], s_b[warp], s_c[warp]);
+        raster_subtile2<kExactExp, kCount>(a, v, gt - a.tile_base[v], item & ((1u << a.ipt_lg) - 1u), gt, s_a[warp],
+                                           s_b[warp], s_c[warp]);
         __syncwarp();
     }
 }
@@ -1290,9 +1495,27 @@ __global__ void __launch_bounds__(kRasterThreads, 6) rasterize_k(RasterArgs a) {
         if (lane == 0) item = a.item_base + atomicAdd(a.work_counter, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= a.num_items) return;
-        const uint32_t gt = a.work ? a.work[item >> 3] : (item >> 3);
+        const uint32_t gt = a.work ? a.work[item >> a.ipt_lg] : (item >> a.ipt_lg);
         const uint32_t v = view_of_tile(a, gt);
-        raster_subtile<kExactExp, kCount>(a, v, gt - a.tile_base[v], item & 7u, gt, s_a[warp], s_b[warp], s_c[warp]);
+        raster_subtile<kExactExp, kCount>(a, v, gt - a.tile_base[v], item & ((1u << a.ipt_lg) - 1u), gt, s_a[warp],
+                                          s_b[warp], s_c[warp]);
+        __syncwarp();
+    }
+}
+
+// The packed two-splat rasterizer (fast variant): 32-pixel work items (8 per 16x16 tile).
+template <bool kCycles = false>
+__global__ void __launch_bounds__(kRasterThreads, 6) rasterize_x2_k(RasterArgs a) {
+    __shared__ __align__(16) float s_p[kRasterWarps][32 * kPairFloats];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    while (true) {
+        uint32_t item = 0;
+        if (lane == 0) item = a.item_base + atomicAdd(a.work_counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.num_items) return;
+        const uint32_t gt = a.work ? a.work[item >> a.ipt_lg] : (item >> a.ipt_lg);
+        const uint32_t v = view_of_tile(a, gt);
+        raster_subtile_x2<kCycles>(a, v, gt - a.tile_base[v], item & ((1u << a.ipt_lg) - 1u), gt, s_p[warp]);
         __syncwarp();
     }
 }

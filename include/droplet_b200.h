@@ -178,19 +178,23 @@ int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg
 
 /* ---- tuning (no reference counterpart) -----------------------------------
  * Knobs of rendered frames that change timing only, never a pixel.  The
- * binning tile stays 16x16 (the reference's TILE_SIZE): another tile shape
- * changes which tiles the maxCoverage truncation keeps (it is row-major in
- * tile space), and so changes pixels. */
+ * binning tile may be 8x8 or 32x8 instead of the reference's 16x16 TILE_SIZE
+ * only for frames where no splat's coverage can be truncated (every view's
+ * 16x16 tile count at most maxCoveragePerSplat); the truncation keeps a
+ * row-major prefix of 16x16 tiles, so other frames bin with 16x16 tiles. */
 typedef struct dl_tuning {
     int32_t pair_sort_bits;       /* digit width of the tile-pair sort: 6, 7 or 8 (default 8) */
     int32_t raster_shape;         /* pixels of one rasterizer work item (one warp): 0 = 8x4, 1 = 16x2, 2 = 4x8,
-                                     3 = 8x8 with two pixels per lane */
+                                     3 = 8x8 with two pixels per lane, 4 = 8x4 taking two splats per step
+                                     in packed f32x2 arithmetic (DL_BATCH_FAST_EXP frames; others use 0) */
     int32_t raster_ctas_per_sm;   /* persistent rasterizer CTAs per SM, 1..5; 0 = the occupancy limit */
+    int32_t bin_tile;             /* binning tile: 0 = 16x16 (default), 1 = 8x8, 2 = 32x8; work items that do
+                                     not fit the tile fall back to 8x4 */
 } dl_tuning;
 int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t);
 int dl_renderer_get_tuning(dl_renderer* r, dl_tuning* t);
 /* Autotuner: renders the n views of s (flags as dl_render_batch, outputs kept
- * on the device) under candidate tunings — coordinate descent over the three
+ * on the device) under candidate tunings — coordinate descent over the four
  * knobs from the current tuning — timing each as the median of `reps` frames
  * (CUDA events on the renderer's stream, after one warm-up frame), keeps the
  * fastest on the renderer and returns it with its frame time in ms. */

@@ -209,9 +209,12 @@ def test_tuning_knobs_change_no_pixel_and_autotune_keeps_one(device):
     flags = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
     base = r2.render_batch(sc, cams, flags=flags)
     for kw in ({"pair_sort_bits": 7}, {"pair_sort_bits": 6}, {"raster_shape": "16x2"}, {"raster_shape": "4x8"},
-               {"raster_shape": "8x8x2"},
+               {"raster_shape": "8x8x2"}, {"raster_shape": "8x4-f32x2"},
                {"raster_ctas_per_sm": 3}, {"raster_ctas_per_sm": 1},
-               {"pair_sort_bits": 6, "raster_shape": "4x8", "raster_ctas_per_sm": 2}):
+               {"pair_sort_bits": 6, "raster_shape": "4x8", "raster_ctas_per_sm": 2},
+               {"bin_tile": "8x8"}, {"bin_tile": "32x8"}, {"bin_tile": "8x8", "raster_shape": "8x8x2"},
+               {"bin_tile": "8x8", "raster_shape": "16x2"}, {"bin_tile": "32x8", "raster_shape": "8x4-f32x2"},
+               {"bin_tile": "32x8", "raster_shape": "4x8", "pair_sort_bits": 6}):
         r2.set_tuning(**kw)
         for a, b in zip(base, r2.render_batch(sc, cams, flags=flags)):
             assert np.array_equal(a, b), kw
@@ -224,10 +227,15 @@ def test_tuning_knobs_change_no_pixel_and_autotune_keeps_one(device):
     exact = r2.render_batch(sc32, cams)
     for a, c in zip(exact, cams):
         assert np.array_equal(a, renderer_single(device, d, c))
+    for tile in ("8x8", "32x8"):           # exact path binned with other tiles, bit-exact too
+        r2.set_tuning(bin_tile=tile)
+        for a, c in zip(r2.render_batch(sc32, cams), cams):
+            assert np.array_equal(a, renderer_single(device, d, c)), tile
     r2.set_tuning()
     t = r2.autotune(sc, cams, flags=flags, reps=2)
-    assert t["pair_sort_bits"] in (6, 7, 8) and t["raster_shape"] in ("8x4", "16x2", "4x8", "8x8x2") and t["frame_ms"] > 0
-    assert r2.get_tuning() == {k: t[k] for k in ("pair_sort_bits", "raster_shape", "raster_ctas_per_sm")}
+    assert t["pair_sort_bits"] in (6, 7, 8) and t["raster_shape"] in dl.Renderer.RASTER_SHAPES and t["frame_ms"] > 0
+    assert t["bin_tile"] in dl.Renderer.BIN_TILES
+    assert r2.get_tuning() == {k: t[k] for k in ("pair_sort_bits", "raster_shape", "raster_ctas_per_sm", "bin_tile")}
     for a, b in zip(base, r2.render_batch(sc, cams, flags=flags)):
         assert np.array_equal(a, b)
     with pytest.raises(dl.DropletError):
@@ -239,6 +247,27 @@ def renderer_single(device, d, cam):
     try:
         return r.render(d, cam)
     finally:
+        r.destroy()
+
+
+def test_other_binning_tiles_keep_the_coverage_truncation(device):
+    # with a maxCoveragePerSplat below the view's 16x16 tile count a large splat
+    # keeps only a row-major prefix of its 16x16 tiles; a tuned binning tile must
+    # not change that, so such frames bin with 16x16 tiles
+    n = 400
+    rng = np.random.default_rng(9)
+    d = dl.SplatData(n, (rng.random((n, 3)) * 0.4 - 0.2).astype(np.float32),
+                     np.tile(np.array([1, 0, 0, 0], np.float32), (n, 1)), np.full((n, 3), np.log(0.4), np.float32),
+                     rng.normal(0.0, 1.0, n).astype(np.float32), rng.normal(0.0, 0.5, (n, 3)).astype(np.float32))
+    cam = synth.pinhole(320, 240, (0.0, 0.0, 3.0))
+    want = O.render(d, cam, maxCoverage=40)["rgba"]
+    for tile in ("8x8", "32x8"):
+        r = dl.Renderer(device, {"maxCoveragePerSplat": 40})
+        r.set_tuning(bin_tile=tile)
+        sc = r.upload(d)
+        assert np.array_equal(r.render_batch(sc, [cam, cam])[1], want), tile
+        assert np.array_equal(r.render(d, cam), want), tile
+        sc.destroy()
         r.destroy()
 
 
