@@ -4,10 +4,10 @@ from .types import (BackgroundRGBA, Bounds, RenderCamera, SplatData, mat4Identit
                     numSHCoeffsPerChannel, quatRotate, splatInputStride, vec3)
 from ._lib import DropletError
 from .ply import loadPlySplats, splatBounds
-from .api import (BlockMaskBuffer, Device, GpuRadixSorter, Mlp, Renderer, Scene, VoxelBlock, VoxelizeResult,
-                  createDevice, mortonDecode3, mortonEncode3, voxelize)
+from .api import (BlockMaskBuffer, Device, GpuRadixSorter, Mlp, PlySplats, Renderer, Scene, VoxelBlock,
+                  VoxelizeResult, createDevice, mortonDecode3, mortonEncode3, voxelize)
 
 __all__ = ["BackgroundRGBA", "Bounds", "RenderCamera", "SplatData", "mat4Identity", "mat4LookAt",
            "numSHCoeffsPerChannel", "quatRotate", "splatInputStride", "vec3", "DropletError",
            "BlockMaskBuffer", "Device", "GpuRadixSorter", "Mlp", "Renderer", "Scene", "VoxelBlock", "VoxelizeResult", "createDevice",
-           "mortonDecode3", "mortonEncode3", "voxelize", "loadPlySplats", "splatBounds"]
+           "mortonDecode3", "mortonEncode3", "voxelize", "loadPlySplats", "splatBounds", "PlySplats"]

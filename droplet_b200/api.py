@@ -15,13 +15,13 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass
-from typing import List, Optional, Sequence
+from typing import List, Optional, Sequence, Union
 
 import numpy as np
 
 from . import _lib
 from ._lib import DropletError, check
-from .types import BackgroundRGBA, Bounds, RenderCamera, SplatData
+from .types import BackgroundRGBA, Bounds, RenderCamera, SplatData, numSHCoeffsPerChannel
 
 
 def _splats(d: SplatData) -> _lib.DlSplats:
@@ -273,6 +273,57 @@ class Renderer:
         if self._h:
             _lib.load().dl_renderer_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- PLY through the C ABI
+class PlySplats:
+    """A PLY file parsed by the library (dl_ply_load, src/io/ply.ts:120-239)
+    into arrays it owns — page-locked with pinned=True, so rendering or
+    uploading them needs no staging copy.  .data is a SplatData whose arrays
+    view that memory (valid until destroy())."""
+
+    def __init__(self, source: Union[bytes, bytearray, memoryview, str], opts: Optional[dict] = None,
+                 pinned: bool = False):
+        if isinstance(source, str):
+            with open(source, "rb") as f:
+                source = f.read()
+        buf = bytes(source)
+        flip = True if not opts or opts.get("flipY") is None else bool(opts["flipY"])
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        st = L.dl_ply_load(buf, len(buf), 1 if flip else 0, _lib.DL_PLY_PINNED if pinned else 0, ctypes.byref(h))
+        if st != _lib.DL_OK:
+            msg = L.dl_last_error().decode(errors="replace")
+            if st == _lib.DL_E_INVALID_ARG:
+                raise ValueError(msg)            # the reference throws Error with the same message
+            raise DropletError(st, msg)
+        self._h = h.value
+        s = _lib.DlSplats()
+        check(L.dl_ply_splats(self._h, ctypes.byref(s)))
+        n = int(s.count)
+
+        def view(ptr, k):
+            if not ptr or k == 0:
+                return None
+            buf = (ctypes.c_float * k).from_address(ptr)
+            buf._owner = self                    # the arrays keep the parsed memory alive
+            return np.frombuffer(buf, dtype=np.float32)
+        self.data = SplatData(n, view(s.positions, 3 * n), view(s.rotations, 4 * n), view(s.log_scales, 3 * n),
+                              view(s.opacity_logits, n), view(s.colors_dc, 3 * n),
+                              view(s.colors_sh, 3 * numSHCoeffsPerChannel(s.sh_bands) * n) if s.sh_bands else None,
+                              int(s.sh_bands))
+
+    def destroy(self):
+        if self._h:
+            _lib.load().dl_ply_free(self._h)
+            self._h = None
+            self.data = None
 
     def __del__(self):
         try:

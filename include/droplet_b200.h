@@ -253,6 +253,21 @@ int dl_device_set_voxel_scheduler(dl_device* dev, dl_mlp* mlp);
  * each slab, its DL_MLP_IN features and measured cost (SM cycles / 16). */
 int dl_vox_result_block_log(const dl_vox_result* res, float* features, float* cost, uint64_t cap, uint64_t* n);
 
+/* ---- src/io/ply.ts:120-239 loadPlySplats --------------------------------
+ * Parses a 3DGS PLY held in memory (bytes, len) into the SoA arrays of a
+ * dl_splats, with the reference loader's header rules, transforms (flipY:
+ * y, and the quaternion's x and z, negated; f_dc times SH_C0; quaternions
+ * normalized) and error messages (DL_E_INVALID_ARG, message in
+ * dl_last_error).  With DL_PLY_PINNED the arrays are page-locked host memory,
+ * so that dl_scene_upload / dl_render move them to the device without a
+ * staging copy (needs a CUDA device); otherwise ordinary host memory.  The
+ * arrays live until dl_ply_free; dl_ply_splats points a dl_splats at them. */
+#define DL_PLY_PINNED 1u
+typedef struct dl_ply dl_ply;
+int dl_ply_load(const uint8_t* bytes, size_t len, int flip_y, uint32_t flags, dl_ply** out);
+int dl_ply_splats(const dl_ply* p, dl_splats* out);
+int dl_ply_free(dl_ply* p);
+
 /* ---- src/gpu/radix-sort.ts:91-216 GpuRadixSorter ----------------------- */
 /* Stable LSD radix sort of n u32 keys with u32 values in device memory (the
  * reference's sorter is not stable; a stable order is one it may return).

@@ -105,3 +105,68 @@ def test_round_trip_and_bounds(tmp_path):
     p = d.positions.reshape(-1, 3)
     assert b["min"] == [float(v) for v in p.min(0)] and b["max"] == [float(v) for v in p.max(0)]
     assert dl.loadPlySplats is ply.loadPlySplats
+
+
+# ---- the C-ABI loader (dl_ply_load) against the Python loader, ordinary host memory
+def _native(buf, opts=None):
+    return dl.PlySplats(buf, opts, pinned=False)
+
+
+def _same(a, b):
+    assert a.count == b.count and a.shBands == b.shBands
+    for k in ("positions", "rotations", "logScales", "opacityLogits", "colorsDC", "colorsSH"):
+        x, y = getattr(a, k), getattr(b, k)
+        if x is None or y is None:
+            assert x is None and y is None, k
+        else:
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), k
+
+
+def test_native_loader_matches_the_python_loader():
+    rng = np.random.default_rng(11)
+    for bands, k in ((0, 0), (1, 9), (2, 24), (3, 45)):
+        props = BASE + [f"f_rest_{i}" for i in range(k)]
+        perm = rng.permutation(len(props))
+        rows = rng.normal(size=(257, len(props))).astype(np.float32)
+        rows[3, 10:14] = 0.0                                   # zero quaternion
+        rows[4, 10] = np.nan                                   # NaN component
+        rows[5, 11] = np.inf                                   # infinite component
+        buf = _ply([props[i] for i in perm], rows[:, perm].tolist(),
+                   extra_elements="element face 0\nproperty list uchar int vertex_indices\n")
+        for flip in (True, False):
+            p = _native(buf, {"flipY": flip})
+            _same(p.data, ply.loadPlySplats(buf, {"flipY": flip}))
+            p.destroy()
+
+
+def test_native_loader_reads_unaligned_data_and_files(tmp_path):
+    d = synth.cluster_scene(500, seed=6, clusters=3, extent=2.0, bands=2)
+    path = str(tmp_path / "s.ply")
+    ply.savePlySplats(d, path)
+    raw = open(path, "rb").read()
+    _same(_native(path).data, ply.loadPlySplats(path))
+    head = raw.index(b"end_header\n")
+    shifted = raw[:head] + b" " + raw[head:]                  # one header byte more: data at an odd offset
+    _same(_native(shifted).data, ply.loadPlySplats(shifted))
+
+
+@pytest.mark.parametrize("make,msg", [
+    (lambda: b"ply\nformat binary_little_endian 1.0\nelement vertex 1\n", "end_header not found"),
+    (lambda: b"plx\nend_header\n", "missing magic"),
+    (lambda: _ply(BASE, [[0.0] * 14], fmt="ascii 1.0"), "ASCII PLY not supported"),
+    (lambda: _ply(BASE, [[0.0] * 14], fmt="binary_big_endian 1.0"), "only little-endian"),
+    (lambda: _ply(BASE, []), "no vertices"),
+    (lambda: _ply(BASE, [[0.0] * 14])[:-4], "data section truncated"),
+    (lambda: _ply(BASE[:-1], [[0.0] * 13]), 'missing property "rot_3"'),
+    (lambda: _ply(BASE + [f"f_rest_{k}" for k in range(12)], [[0.0] * 26]), "no SH band layout"),
+    (lambda: _ply(BASE, [[0.0] * 14]).replace(b"property float opacity", b"property uchar opacity"),
+     "mixed property types"),
+    (lambda: _ply(BASE, [[0.0] * 14]).replace(b"property float opacity", b"property double opacity"),
+     'unsupported property type "double"'),
+])
+def test_native_loader_errors_match(make, msg):
+    with pytest.raises(ValueError, match=msg) as e:
+        _native(make())
+    with pytest.raises(ValueError) as f:
+        ply.loadPlySplats(make())
+    assert str(e.value) == str(f.value)

@@ -318,3 +318,21 @@ def test_offscreen_cull_changes_no_pixel(device, renderer, op_mu):
     one = r2.render_batch(sc, cams[:1], flags=_lib.DL_BATCH_CULL_OFFSCREEN)[0]
     assert np.array_equal(one, renderer.render(d, cams[0]))
     assert int(r2.debug_get("nvis", np.uint64)[0]) < d.count
+
+
+def test_ply_parsed_into_pinned_memory_renders_like_its_data(renderer, tmp_path):
+    # dl_ply_load parses the file into page-locked arrays; rendering them is
+    # bit-exact with the same splats loaded by the Python loader, and with the oracle
+    from droplet_b200 import ply
+    d = synth.cluster_scene(20_000, seed=8, clusters=8, extent=1.5, bands=3)
+    path = str(tmp_path / "scene.ply")
+    ply.savePlySplats(d, path)
+    p = dl.PlySplats(path, pinned=True)
+    cam = synth.pinhole(640, 360, (0.0, 0.3, 4.0))
+    got = renderer.render(p.data, cam)
+    assert np.array_equal(got, renderer.render(ply.loadPlySplats(path), cam))
+    assert np.array_equal(got, O.render(p.data, cam)["rgba"])
+    sc = renderer.upload(p.data, "f32")
+    assert np.array_equal(renderer.render_batch(sc, [cam])[0], got)
+    sc.destroy()
+    p.destroy()
