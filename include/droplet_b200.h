@@ -133,11 +133,13 @@ enum {
                                      (det < 2^-10 c00 c11); culling and tile ranges unchanged */
     DL_BATCH_SH16 = 512,          /* dl_render_many: keep the uploaded SH coefficients in f16 */
     DL_BATCH_CULL_OFFSCREEN = 1024 /* work that cannot change a pixel is left out: splats with no tile on
-                                      the image leave the depth order, untruncated splats are binned by
-                                      the box of their ellipse q <= 9.5, and the screen record ("recA")
-                                      holds (x, y, half-width, half-height) of the box the rasterizer
-                                      tests.  Pixels are unchanged; tile lists and depth ranks then
-                                      differ from the reference's. */
+                                      the image, and splats whose alpha reaches 1/255 nowhere, leave the
+                                      depth order; untruncated splats are binned by the box of their
+                                      ellipse q <= min(9.5, 1.002 qa + 0.01), qa = -2 ln(exp(-4.5) +
+                                      1/(255 opacity)) being the q where alpha falls to 1/255; and the
+                                      screen record ("recA") holds (x, y, half-width, half-height) of the
+                                      box the rasterizer tests.  Pixels are unchanged; tile lists and
+                                      depth ranks then differ from the reference's. */
 };
 /* Render n views of one resident scene; outs[i] receives cams[i].width *
  * cams[i].height RGBA8 pixels (host or device memory, per flags). */
