@@ -432,8 +432,10 @@ def run_ours(args, rank, world, local_rank):
     sm_mhz = clocks["sm_mhz"] or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     flops = evals * 20
-    roof = {"kernel": "rasterize_k (fused finalize)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+    roof = {"kernel": "rasterizer (fused finalize)", "bound": "hbm", "achieved": achieved, "peak": hbm,
             "unit": "GB/s", "frac": achieved / hbm, "traffic": profile_traffic(),
+            "traffic_source": "ncu dram bytes of a 4-view capture of the same kernel, scaled by tile pairs",
+            "limiter": "instruction issue (FP32 / ALU pipes), not HBM: see compute",
             "peak_source": "measured" if pk else "fallback",
             "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": rast_ms,
             "compute": {"evaluated_pairs": evals, "flops_per_eval": 20,
@@ -442,13 +444,16 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "storage_dtype": "f16 scene SH and projected records (f32 accumulation of colour and transmittance); "
+                             "ex2.approx for the Gaussian",
             "config": config(args, cams, {"mode": "batched: one launch sequence for all views (a CUDA-graph "
                                                   "replay when there are several), splats without on-image tiles "
                                                   "left out of the depth sort, f16 scene SH and records, "
                                                   "hardware exp2 (+-1 LSB), tiles rasterized in decreasing cost "
                                                   "predicted by the learned model",
                                           "parallelism": f"views sharded: {world} rank(s) x {len(cams)} distinct "
-                                                         f"views, scene replicated"}, data),
+                                                         f"views, scene replicated",
+                                          "tile": (tuning or r.get_tuning())["bin_tile"]}, data),
             "plain_value": plain_value, "exact_value": exact_value, "static_value": static_value,
             "learned": (model.meta if model is not None else None), "tuning": tuning,
             "vs_plain": (value / plain_value) if plain_value else None,
