@@ -224,6 +224,18 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
         if (tid < RADIX) s_toff[tid] = wpre + inc - v;
         if (DROP && tid == RADIX - 1) s_nkeep = wpre + inc;
     }
+    __syncthreads();
+    // scatter into shared memory in sorted-within-tile order (needs only the
+    // tile's own offsets, so it runs before the look-back: predecessors have
+    // more time to publish, and fewer waits spin)
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+        if (dig[j] < RADIX) {
+            const uint32_t pos = s_toff[dig[j]] + s_hist[warp][dig[j]] + rank[j];
+            s_keys[pos] = key[j];
+            s_vals[pos] = val[j];
+        }
+    }
     // decoupled look-back for this digit's prefix over earlier tiles of the segment
     if (tid < RADIX) {
         uint32_t excl = 0;
@@ -263,17 +275,6 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
             if (publish) dl_st_volatile(p.status + (size_t)tile * RADIX + tid, kFlagPrefix | ((excl + cnt) & kValMask));
         }
         s_glob[tid] = p.glob_off[((size_t)seg * p.passes + p.pass) * RADIX + tid] + excl;
-    }
-    __syncthreads();
-
-    // scatter into shared memory in sorted-within-tile order
-#pragma unroll
-    for (int j = 0; j < kItems; j++) {
-        if (dig[j] < RADIX) {
-            const uint32_t pos = s_toff[dig[j]] + s_hist[warp][dig[j]] + rank[j];
-            s_keys[pos] = key[j];
-            s_vals[pos] = val[j];
-        }
     }
     __syncthreads();
     // coalesced write-out: consecutive threads write consecutive slots of a digit run
