@@ -27,6 +27,7 @@ DL_BATCH_F64_DEGENERATE = 256
 DL_BATCH_SH16 = 512
 DL_BATCH_CULL_OFFSCREEN = 1024
 DL_PLY_PINNED = 1
+DL_VOX_FAST_EXP = 1
 DL_MLP_IN, DL_MLP_HIDDEN = 12, 64
 DL_MLP_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 
@@ -74,7 +75,8 @@ class DlVoxOpts(ctypes.Structure):
     _fields_ = [("voxel_resolution", ctypes.c_double), ("opacity_cutoff", ctypes.c_double),
                 ("use_defaults", ctypes.c_int32), ("has_bounds", ctypes.c_int32),
                 ("bounds_min", ctypes.c_double * 3), ("bounds_max", ctypes.c_double * 3),
-                ("shard_index", ctypes.c_int32), ("shard_count", ctypes.c_int32), ("log_blocks", ctypes.c_int32)]
+                ("shard_index", ctypes.c_int32), ("shard_count", ctypes.c_int32), ("log_blocks", ctypes.c_int32),
+                ("flags", ctypes.c_uint32)]
 
 
 _lib = None

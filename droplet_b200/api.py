@@ -414,7 +414,8 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
 
     opts["shard"] = (index, count) voxelizes only that shard of the grid's z rows
     of 16^3-block batches (see droplet_b200.shard); bounds and numBlocks stay
-    those of the whole grid."""
+    those of the whole grid.  opts["fastExp"] evaluates the densities with the
+    hardware ex2 (bits within about 1e-5 of the cutoff may change)."""
     opts = opts or {}
     o = _lib.DlVoxOpts()
     res = opts.get("voxelResolution")
@@ -433,6 +434,7 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
     if sh is not None:
         o.shard_index, o.shard_count = int(sh[0]), int(sh[1])
     o.log_blocks = 1 if opts.get("logBlocks") else 0
+    o.flags = _lib.DL_VOX_FAST_EXP if opts.get("fastExp") else 0
     L = _lib.load()
     h = ctypes.c_void_p()
     check(L.dl_voxelize(device.handle, ctypes.byref(_splats(data)), ctypes.byref(o), ctypes.byref(h)))

@@ -445,6 +445,15 @@ struct EvalArgs {
     const uint32_t* err;           // DL_DEVERR_TIMEOUT: the block lists are not complete
 };
 
+template <bool kFast>
+__device__ __forceinline__ float vox_exp(float x) {
+    if (!kFast) return dl_expf(x);
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x * 1.4426950408889634f));
+    return y;
+}
+
+template <bool kFast>
 __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, const VoxRec& g) {
     // shaders/voxelize.ts:62-84, same f32 operation order
     const float d0 = vc[0] - g.px, d1 = vc[1] - g.py, d2 = vc[2] - g.pz;
@@ -461,9 +470,11 @@ __device__ __forceinline__ float eval_gaussian(const float vc[3], float half, co
     const float l2 = (cd2 + g.qw * t2) + (qx * t1 - qy * t0);
     const float s0 = l0 * g.isx, s1 = l1 * g.isy, s2 = l2 * g.isz;
     const float d2s = (s0 * s0 + s1 * s1) + s2 * s2;
-    return g.opacity * dl_expf(-0.5f * d2s);
+    return g.opacity * vox_exp<kFast>(-0.5f * d2s);
 }
 
+// kFast: hardware ex2 for the density exponentials (DL_VOX_FAST_EXP)
+template <bool kFast>
 __global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
     __shared__ VoxRec s_g[64];
     __shared__ uint32_t s_b;
@@ -507,14 +518,14 @@ __global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
             const uint32_t m = min(64u, end - c);
             if (sigma < 7.0f) {
                 for (uint32_t j = 0; j < m; j++) {
-                    sigma = sigma + eval_gaussian(vc, a.p.half, s_g[j]);
+                    sigma = sigma + eval_gaussian<kFast>(vc, a.p.half, s_g[j]);
                     evals++;
                     if (sigma >= 7.0f) break;
                 }
             }
             if (__syncthreads_count(sigma < 7.0f) == 0) break;
         }
-        const float opacity = 1.0f - dl_expf(-sigma);
+        const float opacity = 1.0f - vox_exp<kFast>(-sigma);
         const bool solid = opacity >= a.p.cutoff;
         const uint32_t bal = __ballot_sync(0xffffffffu, solid);
         if ((tid & 31) == 0) s_mask[tid >> 5] = bal;
@@ -749,6 +760,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     if (!dev->vox) dev->vox = new VoxBufs();
     VoxBufs& B = *dev->vox;
     const bool logBlocks = opts && opts->log_blocks;
+    const bool fastExp = opts && (opts->flags & DL_VOX_FAST_EXP);
     const double blockSize = 4 * voxelRes;
     VoxParams p;
     std::memset(&p, 0, sizeof(p));
@@ -1092,7 +1104,8 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
         va.counter = scr + VS_EVAL; va.evals = nullptr;
         va.work = work; va.cycles = logBlocks ? B.scycles.as<uint32_t>() : nullptr; va.err = scr + VS_ERR;
-        vox_eval_k<<<dev->sm_count * 32, 64, 0, st>>>(va);
+        if (fastExp) vox_eval_k<true><<<dev->sm_count * 32, 64, 0, st>>>(va);
+        else vox_eval_k<false><<<dev->sm_count * 32, 64, 0, st>>>(va);
 
         uint32_t hn[2] = {0, 0};
         if (cudaMemcpyAsync(hn, scr + VS_NBLK, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

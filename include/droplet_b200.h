@@ -92,7 +92,12 @@ typedef struct dl_vox_opts {
     int32_t shard_count;
     /* 1: keep per-block features and measured cost (dl_vox_result_block_log) */
     int32_t log_blocks;
+    /* DL_VOX_FAST_EXP: the density exponentials use the hardware ex2 instead
+     * of the library's exact-rounding exp; voxels whose opacity lies within
+     * about 1e-5 of the cutoff may then change (no reference counterpart). */
+    uint32_t flags;
 } dl_vox_opts;
+#define DL_VOX_FAST_EXP 1u
 
 /* ---- errors ------------------------------------------------------------ */
 /* Message of the last failure on this thread ("" if none). */

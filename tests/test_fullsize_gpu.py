@@ -121,9 +121,14 @@ def test_voxel1m_full_size(device):
     assert np.array_equal([g.numBlocksX, g.numBlocksY, g.numBlocksZ], o["dims"])
     ref = O.voxelize(d, 0.05, 0.1, order=1, eps=EPS, fields=REF_FIELDS)
     diff = _eps_band_count(g.buffer.blockIdx, g.buffer.maskLo, g.buffer.maskHi, ref)
+    # the hardware-exp variant against the canonical order, band 1e-4
+    fast = dl.voxelize(device, d, dict(opts, fastExp=True))
+    canon = O.voxelize(d, 0.05, 0.1, eps=1e-4, fields=REF_FIELDS)
+    fdiff = _eps_band_count(fast.buffer.blockIdx, fast.buffer.maskLo, fast.buffer.maskHi, canon)
     print(f"\nvoxel1m: {g.buffer.count} blocks, {g.buffer.popcount()} solid voxels; bit-exact vs canonical order; "
           f"vs reference order {diff} bits differ, all within the {ref['near_bits']} bits with "
-          f"|alpha - cutoff| < {EPS}")
+          f"|alpha - cutoff| < {EPS}; hardware-exp variant: {fdiff} bits differ from the canonical order, all "
+          f"within the {canon['near_bits']} bits with |alpha - cutoff| < 1e-4")
 
 
 def test_zipf10m_grid_by_z_rows(device):

@@ -126,3 +126,24 @@ def test_z_row_shards_concatenate_to_the_whole_grid(device, count):
         assert np.array_equal(np.concatenate([p.buffer.blockIdx for p in p2]), w2.buffer.blockIdx)
     with pytest.raises(dl.DropletError):
         dl.voxelize(device, d, dict(opts, shard=(count, count)))
+
+
+def test_fast_exp_differs_only_near_the_cutoff(device):
+    # DL_VOX_FAST_EXP: the hardware ex2 moves a voxel's opacity by ~1e-6 at most;
+    # bits may change only where the canonical opacity is within eps of the cutoff
+    d = synth.voxel_1m(100_000)
+    opts = {"voxelResolution": 0.05, "opacityCutoff": 0.1}
+    g = dl.voxelize(device, d, dict(opts, fastExp=True))
+    eps = 1e-4
+    f = ("block_idx", "mask_lo", "mask_hi", "near_idx", "near_lo", "near_hi", "near_bits")
+    o = O.voxelize(d, 0.05, 0.1, eps=eps, fields=f)
+    mg = {int(i): (int(l), int(h)) for i, l, h in zip(g.buffer.blockIdx, g.buffer.maskLo, g.buffer.maskHi)}
+    mo = {int(i): (int(l), int(h)) for i, l, h in zip(o["block_idx"], o["mask_lo"], o["mask_hi"])}
+    near = {int(i): (int(l), int(h)) for i, l, h in zip(o["near_idx"], o["near_lo"], o["near_hi"])}
+    differing = 0
+    for k in set(mg) | set(mo):
+        a, b, n = mg.get(k, (0, 0)), mo.get(k, (0, 0)), near.get(k, (0, 0))
+        assert ((a[0] ^ b[0]) & ~n[0]) == 0 and ((a[1] ^ b[1]) & ~n[1]) == 0
+        differing += bin(a[0] ^ b[0]).count("1") + bin(a[1] ^ b[1]).count("1")
+    print(f"fast exp: {differing} bits differ from the canonical order, all within the {o['near_bits']} bits "
+          f"with |alpha - cutoff| < {eps}")
