@@ -282,6 +282,7 @@ struct FrameDims {
     int subLw = 3;                       // rasterizer work item width log2 (8x4)
     bool ppl2 = false;                   // two pixels per lane (8x8 work items)
     bool x2 = false;                     // two splats per step in f32x2 arithmetic (fast variant)
+    bool tileCta = false;                // one CTA per 256-pixel tile, the slice read once (fast variant)
     int iptLg = 3;                       // log2 of the rasterizer work items per binning tile
 };
 
@@ -325,16 +326,18 @@ bool dl_retile_views(DlView* v, uint32_t V, uint32_t tw, uint32_t th) {
 }
 
 // Persistent rasterizer grid: every SM filled to its occupancy limit.
-uint32_t raster_grid(bool fastExp, bool ppl2, bool x2) {
-    static int cached[64][5] = {};
+uint32_t raster_grid(bool fastExp, bool ppl2, bool x2, bool tileCta) {
+    static int cached[64][6] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int kind = x2 ? 4 : (fastExp ? 1 : 0) + (ppl2 ? 2 : 0);
+    const int kind = tileCta ? 5 : x2 ? 4 : (fastExp ? 1 : 0) + (ppl2 ? 2 : 0);
     int* c = (dev >= 0 && dev < 64) ? &cached[dev][kind] : nullptr;
     if (c && *c) return (uint32_t)*c;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (x2) {
+    if (tileCta) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_tile_x2_k<false>, dlr::kRasterThreads, 0);
+    } else if (x2) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_x2_k<false>, dlr::kRasterThreads, 0);
     } else if (ppl2) {
         if (fastExp) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize2_k<false>, dlr::kRasterThreads, 0);
@@ -378,15 +381,16 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     d.fastExp = (flags & DL_BATCH_FAST_EXP) != 0;
     d.f64deg = (flags & DL_BATCH_F64_DEGENERATE) != 0;
     d.cullOff = (flags & DL_BATCH_CULL_OFFSCREEN) != 0;
-    d.x2 = t.shape == 4 && d.fastExp;    // the packed variant has the fast arithmetic only
+    d.x2 = (t.shape == 4 || t.shape == 5) && d.fastExp;    // the packed variants have the fast arithmetic only
     // work items must fit the binning tile (every view of a frame has the same tile)
     const uint32_t tw = V ? hv[0].tileW : DL_TILE, th = V ? hv[0].tileH : DL_TILE;
+    d.tileCta = t.shape == 5 && d.fastExp && tw * th == 256u;   // 8 warps of 8x4 items per tile
     const uint32_t iw = d.ppl2 ? 8u : (1u << d.subLw), ih = d.ppl2 ? 8u : (32u >> d.subLw);
     if (iw > tw || ih > th) { d.subLw = 3; d.ppl2 = false; }
-    const uint32_t ipt = tw * th / (d.ppl2 ? 64u : 32u);
+    const uint32_t ipt = d.tileCta ? 1u : tw * th / (d.ppl2 ? 64u : 32u);
     d.iptLg = 0;
     while ((1u << d.iptLg) < ipt) d.iptLg++;
-    d.rasterGrid = raster_grid(d.fastExp, d.ppl2, d.x2);
+    d.rasterGrid = raster_grid(d.fastExp, d.ppl2, d.x2, d.tileCta);
     if (t.ctas_per_sm > 0) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -625,9 +629,12 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ra.outs = f.outs;
     ra.accum = f.accum;
     ra.work = work;
+    const bool count = f.evalCount || f.tileEvals;
+    // counting frames run the 8x4 warp-item kernel: 8 items per 256-pixel tile
+    const int iptLg = (d.tileCta && count) ? 3 : d.iptLg;
     ra.item_base = 0;
-    ra.num_items = (1u << d.iptLg) * d.totalTiles;
-    ra.ipt_lg = d.iptLg;
+    ra.num_items = (1u << iptLg) * d.totalTiles;
+    ra.ipt_lg = iptLg;
     ra.work_counter = f.scr + SC_WORK_CTR;
     ra.eval_count = f.evalCount;
     ra.tile_evals = f.tileEvals;
@@ -635,9 +642,11 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ra.sub_lw = d.subLw;
     ra.rec_box = d.cullOff ? 1 : 0;
     ra.stage_pad = stage_pad();
-    const bool count = ra.eval_count || ra.tile_evals;
     auto raster = [&](const dlr::RasterArgs& x) {
-        if (d.x2 && !count) {
+        if (d.tileCta && !count) {
+            if (x.tile_cycles) dlr::rasterize_tile_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            else dlr::rasterize_tile_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+        } else if (d.x2 && !count) {
             if (x.tile_cycles) dlr::rasterize_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
             else dlr::rasterize_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
         } else if (d.ppl2) {
@@ -662,7 +671,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
         // orders, so a range of views is a range of items); each range's images
         // go back to the host on the read-back stream while the next rasterizes.
         const uint32_t per = (d.V + (uint32_t)f.rbGroups - 1) / (uint32_t)f.rbGroups;
-        const uint32_t ipt = 1u << d.iptLg;
+        const uint32_t ipt = 1u << iptLg;
         static_assert(SC_RASTER_CTR + kReadBackGroups <= kScratchWords, "scratch words");
         DL_CK(cudaMemsetAsync(f.scr + SC_RASTER_CTR, 0, 4ull * kReadBackGroups, st));
         for (uint32_t v0 = 0, g = 0; v0 < d.V; v0 += per, g++) {
@@ -890,6 +899,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid,
                                    (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2, (uint64_t)d.x2,
                                    (uint64_t)d.iptLg, (uint64_t)hv[0].tileW, (uint64_t)hv[0].tileH,
+                                   (uint64_t)d.tileCta,
                                    g_dl_wait.spin_limit,
                                    g_dl_wait.withheld(DL_WAIT_STAGE_DEPTH_SORT), g_dl_wait.withheld(DL_WAIT_STAGE_EMIT),
                                    g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT)});

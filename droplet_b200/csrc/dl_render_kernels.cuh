@@ -1306,6 +1306,74 @@ __device__ __forceinline__ void raster_subtile2(const RasterArgs& a, uint32_t v,
 // (A, B, C: the conic scaled by -0.5 log2 e as in stage_chunk's fast path.)
 constexpr int kPairFloats = 20;
 
+// Composites the n staged splats of a warp's packed pair buffer sp (layout
+// above) at the lane's pixel, two splats per step, in staging order; sets done
+// once T < 1e-4 (the shader's early out) and stops there.
+__device__ __forceinline__ void composite_x2(const float* sp, uint32_t n, float2 px2, float2 py2, float& c0,
+                                             float& c1, float& c2, float& T, bool& done) {
+    const float2 nfloor2 = make_float2(-DL_GAUSS_FLOOR, -DL_GAUSS_FLOOR);
+    for (uint32_t j = 0; j < n; j += 2) {
+        const float4* P = reinterpret_cast<const float4*>(sp + (j >> 1) * kPairFloats);
+        const float4 q0 = P[0], q1 = P[1], q2 = P[2];
+        const float2 dx = __fadd2_rn(px2, make_float2(q0.x, q0.y));
+        const float2 dy = __fadd2_rn(py2, make_float2(q0.z, q0.w));
+        const float2 t = __fmul2_rn(make_float2(q1.z, q1.w), dy);
+        const float2 qq = __ffma2_rn(make_float2(q1.x, q1.y), dx, t);
+        const float2 uu = __fmul2_rn(__fmul2_rn(make_float2(q2.x, q2.y), dy), dy);
+        const float2 pw = __ffma2_rn(dx, qq, uu);
+        float e0, e1;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(pw.x));
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(pw.y));
+        const float2 na = __fmul2_rn(make_float2(q2.z, q2.w), __fadd2_rn(make_float2(e0, e1), nfloor2));
+        // the shader's skips: power > 0, alpha < 1/255
+        const bool ok0 = !(pw.x > 0.0f) && !(na.x > -DL_MIN_ALPHA);
+        const bool ok1 = !(pw.y > 0.0f) && !(na.y > -DL_MIN_ALPHA);
+        if (ok0 || ok1) {
+            const float4 q3 = P[3];
+            if (ok0) {
+                const float w = T * na.x;
+                c0 = __fmaf_rn(w, q3.x, c0);
+                c1 = __fmaf_rn(w, q3.y, c1);
+                c2 = __fmaf_rn(w, q3.z, c2);
+                T = __fmaf_rn(T, na.x, T);
+                if (T < DL_MIN_T) { done = true; return; }
+            }
+            if (ok1) {
+                const float4 q4 = P[4];
+                const float w = T * na.y;
+                c0 = __fmaf_rn(w, q3.w, c0);
+                c1 = __fmaf_rn(w, q4.x, c1);
+                c2 = __fmaf_rn(w, q4.y, c2);
+                T = __fmaf_rn(T, na.y, T);
+                if (T < DL_MIN_T) { done = true; return; }
+            }
+        }
+    }
+}
+
+// Writes a staged splat into slot `slot` of a packed pair buffer.
+__device__ __forceinline__ void put_pair_slot(float* sp, uint32_t slot, float x, float y, float A, float B, float C,
+                                              float al, float cr, float cg, float cb) {
+    float* P = sp + (slot >> 1) * kPairFloats;
+    const uint32_t c = slot & 1u;
+    P[0 + c] = -x;
+    P[2 + c] = -y;
+    P[4 + c] = -0.72134752044448170f * A;
+    P[6 + c] = -1.4426950408889634f * B;
+    P[8 + c] = -0.72134752044448170f * C;
+    P[10 + c] = -al;
+    P[12 + 3 * c] = -cr;
+    P[13 + 3 * c] = -cg;
+    P[14 + 3 * c] = -cb;
+}
+
+// An odd count: a splat of opacity 0 fills the last pair (alpha 0 is skipped).
+__device__ __forceinline__ void pad_pair_slot(float* sp, uint32_t n) {
+    float* P = sp + (n >> 1) * kPairFloats;
+    P[1] = 0.0f; P[3] = 0.0f; P[5] = 0.0f; P[7] = 0.0f; P[9] = 0.0f; P[11] = -0.0f;
+    P[15] = 0.0f; P[16] = 0.0f; P[17] = 0.0f;
+}
+
 __device__ __forceinline__ uint32_t stage_chunk_x2(const RasterArgs& a, const uint32_t* vals, uint32_t b,
                                                    uint32_t end, uint64_t vo, float rx0, float rx1, float ry0,
                                                    float ry1, uint32_t lmask, float* sp) {
@@ -1353,28 +1421,10 @@ __device__ __forceinline__ uint32_t stage_chunk_x2(const RasterArgs& a, const ui
             }
         }
         const uint32_t m = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-            const uint32_t slot = n + __popc(m & lmask);
-            float* P = sp + (slot >> 1) * kPairFloats;
-            const uint32_t c = slot & 1u;
-            P[0 + c] = -ra.x;
-            P[2 + c] = -ra.y;
-            P[4 + c] = -0.72134752044448170f * A;
-            P[6 + c] = -1.4426950408889634f * B;
-            P[8 + c] = -0.72134752044448170f * C;
-            P[10 + c] = -al;
-            P[12 + 3 * c] = -cr;
-            P[13 + 3 * c] = -cg;
-            P[14 + 3 * c] = -cb;
-        }
+        if (hit) put_pair_slot(sp, n + __popc(m & lmask), ra.x, ra.y, A, B, C, al, cr, cg, cb);
         n += __popc(m);
     }
-    if ((n & 1u) && lane == 0) {
-        // odd count: a splat of opacity 0 fills the pair (alpha 0 is skipped)
-        float* P = sp + (n >> 1) * kPairFloats;
-        P[1] = 0.0f; P[3] = 0.0f; P[5] = 0.0f; P[7] = 0.0f; P[9] = 0.0f; P[11] = -0.0f;
-        P[15] = 0.0f; P[16] = 0.0f; P[17] = 0.0f;
-    }
+    if ((n & 1u) && lane == 0) pad_pair_slot(sp, n);
     return n;
 }
 
@@ -1400,7 +1450,6 @@ __device__ __forceinline__ void raster_subtile_x2(const RasterArgs& a, uint32_t 
     const uint64_t vo = (uint64_t)v * a.view_stride;
     const uint32_t lmask = dl_lanemask_lt();
     const float2 px2 = make_float2(px, px), py2 = make_float2(py, py);
-    const float2 nfloor2 = make_float2(-DL_GAUSS_FLOOR, -DL_GAUSS_FLOOR);
 
     float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
     bool done = !inImage;
@@ -1408,45 +1457,7 @@ __device__ __forceinline__ void raster_subtile_x2(const RasterArgs& a, uint32_t 
         const uint32_t n = stage_chunk_x2(a, vals, b, end, vo, rx0, rx1, ry0, ry1, lmask, sp);
         if (n == 0u) continue;
         __syncwarp();
-        if (!done) {
-            for (uint32_t j = 0; j < n; j += 2) {
-                const float4* P = reinterpret_cast<const float4*>(sp + (j >> 1) * kPairFloats);
-                const float4 q0 = P[0], q1 = P[1], q2 = P[2];
-                const float2 dx = __fadd2_rn(px2, make_float2(q0.x, q0.y));
-                const float2 dy = __fadd2_rn(py2, make_float2(q0.z, q0.w));
-                const float2 t = __fmul2_rn(make_float2(q1.z, q1.w), dy);
-                const float2 qq = __ffma2_rn(make_float2(q1.x, q1.y), dx, t);
-                const float2 uu = __fmul2_rn(__fmul2_rn(make_float2(q2.x, q2.y), dy), dy);
-                const float2 pw = __ffma2_rn(dx, qq, uu);
-                float e0, e1;
-                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(pw.x));
-                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(pw.y));
-                const float2 na = __fmul2_rn(make_float2(q2.z, q2.w), __fadd2_rn(make_float2(e0, e1), nfloor2));
-                // the shader's skips: power > 0, alpha < 1/255
-                const bool ok0 = !(pw.x > 0.0f) && !(na.x > -DL_MIN_ALPHA);
-                const bool ok1 = !(pw.y > 0.0f) && !(na.y > -DL_MIN_ALPHA);
-                if (ok0 || ok1) {
-                    const float4 q3 = P[3];
-                    if (ok0) {
-                        const float w = T * na.x;
-                        c0 = __fmaf_rn(w, q3.x, c0);
-                        c1 = __fmaf_rn(w, q3.y, c1);
-                        c2 = __fmaf_rn(w, q3.z, c2);
-                        T = __fmaf_rn(T, na.x, T);
-                        if (T < DL_MIN_T) { done = true; break; }
-                    }
-                    if (ok1) {
-                        const float4 q4 = P[4];
-                        const float w = T * na.y;
-                        c0 = __fmaf_rn(w, q3.w, c0);
-                        c1 = __fmaf_rn(w, q4.x, c1);
-                        c2 = __fmaf_rn(w, q4.y, c2);
-                        T = __fmaf_rn(T, na.y, T);
-                        if (T < DL_MIN_T) { done = true; break; }
-                    }
-                }
-            }
-        }
+        if (!done) composite_x2(sp, n, px2, py2, c0, c1, c2, T, done);
         if (__all_sync(0xffffffffu, done)) break;
         __syncwarp();                                   // staging area is reused by the next step
     }
@@ -1517,6 +1528,146 @@ __global__ void __launch_bounds__(kRasterThreads, 6) rasterize_x2_k(RasterArgs a
         const uint32_t v = view_of_tile(a, gt);
         raster_subtile_x2<kCycles>(a, v, gt - a.tile_base[v], item & ((1u << a.ipt_lg) - 1u), gt, s_p[warp]);
         __syncwarp();
+    }
+}
+
+// ---- one CTA per tile: the tile's slice is read once (fast variant)
+// A persistent CTA of 8 warps takes whole 256-pixel tiles (16x16, or 32x8 when
+// tuned); warp w owns the 8x4 work item w of the tile.  The slice is read in
+// batches of 256 pairs, one pair per thread: the thread loads the pair value
+// and screen record, tests the splat's box (staging margin as in stage_chunk)
+// against the 8 items' pixel-centre rectangles, and for a splat that reaches
+// any of them loads its record and stages it in shared memory with an 8-bit
+// mask of the items it reaches.  Each warp then takes, in slice order, the
+// staged splats of its own item (ballots over the masks), packs them into its
+// pair buffer 64 at a time and composites them with composite_x2 — the same
+// splats, values and order as raster_subtile_x2.  The CTA stops reading the
+// slice once all 8 warps' pixels are done.  Reads per pair: one pair value and
+// one screen record per tile (not per work item), and one record per splat
+// that reaches the tile.
+constexpr int kTileStage = kRasterThreads;     // pairs staged per batch
+
+template <bool kCycles>
+__global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterArgs a) {
+    __shared__ float s_f[9][kTileStage];       // x, y, A, B, C, alpha, r, g, b of each staged pair
+    __shared__ uint8_t s_m[kTileStage];        // items the staged splat reaches (bit w: item w)
+    __shared__ __align__(16) float s_p[kRasterWarps][32 * kPairFloats];
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t lmask = dl_lanemask_lt();
+    float* sp = s_p[warp];
+    while (true) {
+        if (tid == 0) s_tile = a.item_base + atomicAdd(a.work_counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_tile;
+        if (item >= a.num_items) return;
+        const uint32_t gt = a.work ? a.work[item] : item;
+        const uint32_t v = view_of_tile(a, gt);
+        const uint32_t tile = gt - a.tile_base[v];
+        const DlView& u = a.views[v];
+        const long long t0 = kCycles ? clock64() : 0;
+        const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
+        const uint32_t perRow = u.tileW >> 3;              // 8x4 items per tile row
+        const uint32_t ox = tx * u.tileW, oy = ty * u.tileH;
+        const uint32_t sx0 = ox + (warp % perRow) * 8u, sy0 = oy + (warp / perRow) * 4u;
+        const uint32_t x = sx0 + (lane & 7), y = sy0 + (lane >> 3);
+        const bool inImage = x < u.W && y < u.H;
+        const float2 px2 = make_float2((float)x + 0.5f, (float)x + 0.5f);
+        const float2 py2 = make_float2((float)y + 0.5f, (float)y + 0.5f);
+        const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+        const uint32_t start = to[tile], end = to[tile + 1];
+        const uint32_t* vals = a.pair_vals + a.pair_base[v];
+        const uint64_t vo = (uint64_t)v * a.view_stride;
+        const float pad = a.stage_pad;
+        float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
+        bool done = !inImage;
+        for (uint32_t b = start; b < end; b += kTileStage) {
+            // ---- stage one pair per thread
+            uint32_t mask = 0;
+            const uint32_t e = b + (uint32_t)tid;
+            if (e < end) {
+                const uint32_t g = __ldg(vals + e);
+                if (!(g & kPhantomBit)) {
+                    const float4 ra = __ldg(a.recA + vo + g);
+                    float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
+                    float A = 0.0f, B = 0.0f, C = 0.0f, al = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+                    if (ex > 0.0f) {
+                        // the box against the tile's pixel-centre rectangle first
+                        const float tx0 = (float)ox + 0.5f - pad, tx1 = (float)(ox + u.tileW) - 0.5f + pad;
+                        const float ty0 = (float)oy + 0.5f - pad, ty1 = (float)(oy + u.tileH) - 0.5f + pad;
+                        if (!(ra.x - ex > tx1) && !(ra.x + ex < tx0) && !(ra.y - ey > ty1) && !(ra.y + ey < ty0)) {
+                            if (a.recBC) {
+                                const float4 p = __ldg(a.recBC + 2 * (vo + g));
+                                const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
+                                A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
+                            } else {
+                                const uint4 hv = __ldg(a.recH + vo + g);
+                                const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
+                                const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
+                                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
+                                const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
+                                A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+                            }
+                            if (!a.rec_box) tight_extent(A, B, C, ra.z, ex, ey);
+                            // items: 8x4 pixels, perRow per tile row
+                            for (uint32_t w = 0; w < (uint32_t)kRasterWarps; w++) {
+                                const float ix0 = (float)(ox + (w % perRow) * 8u) + 0.5f - pad;
+                                const float iy0 = (float)(oy + (w / perRow) * 4u) + 0.5f - pad;
+                                const float ix1 = ix0 + 7.0f + 2.0f * pad, iy1 = iy0 + 3.0f + 2.0f * pad;
+                                if (!(ra.x - ex > ix1) && !(ra.x + ex < ix0) && !(ra.y - ey > iy1) &&
+                                    !(ra.y + ey < iy0))
+                                    mask |= 1u << w;
+                            }
+                            if (mask) {
+                                s_f[0][tid] = ra.x; s_f[1][tid] = ra.y;
+                                s_f[2][tid] = A; s_f[3][tid] = B; s_f[4][tid] = C; s_f[5][tid] = al;
+                                s_f[6][tid] = cr; s_f[7][tid] = cg; s_f[8][tid] = cb;
+                            }
+                        }
+                    }
+                }
+            }
+            s_m[tid] = (uint8_t)mask;
+            __syncthreads();
+            // ---- this warp's splats, 64 at a time, in slice order
+            const uint32_t nb = min((uint32_t)kTileStage, end - b);
+            if (!__all_sync(0xffffffffu, done)) {
+                for (uint32_t c = 0; c < nb; c += 64) {
+                    uint32_t n = 0;
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const uint32_t i = c + (uint32_t)h * 32u + (uint32_t)lane;
+                        const bool hit = i < nb && ((s_m[i] >> warp) & 1u);
+                        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+                        if (hit)
+                            put_pair_slot(sp, n + __popc(m & lmask), s_f[0][i], s_f[1][i], s_f[2][i], s_f[3][i],
+                                          s_f[4][i], s_f[5][i], s_f[6][i], s_f[7][i], s_f[8][i]);
+                        n += __popc(m);
+                    }
+                    if (n == 0u) continue;
+                    if ((n & 1u) && lane == 0) pad_pair_slot(sp, n);
+                    __syncwarp();
+                    if (!done) composite_x2(sp, n, px2, py2, c0, c1, c2, T, done);
+                    __syncwarp();                           // the pair buffer is refilled next
+                    if (__all_sync(0xffffffffu, done)) break;
+                }
+            }
+            // every warp is past this batch's staging area; stop once all pixels are done
+            if (__syncthreads_and(done)) break;
+        }
+        if (inImage) {
+            // finalize.ts:30-43
+            const float rr = fminf(fmaxf(c0 + T * u.bg[0], 0.0f), 1.0f);
+            const float gg = fminf(fmaxf(c1 + T * u.bg[1], 0.0f), 1.0f);
+            const float bb = fminf(fmaxf(c2 + T * u.bg[2], 0.0f), 1.0f);
+            const float aa = fminf(fmaxf((1.0f - T) + T * u.bg[3], 0.0f), 1.0f);
+            const uint32_t out = dl_sat_u32(rr * 255.0f + 0.5f) | (dl_sat_u32(gg * 255.0f + 0.5f) << 8) |
+                                 (dl_sat_u32(bb * 255.0f + 0.5f) << 16) | (dl_sat_u32(aa * 255.0f + 0.5f) << 24);
+            a.outs[v][(uint64_t)y * u.W + x] = out;
+            if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c0, c1, c2, T);
+        }
+        if (kCycles && tid == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
+        __syncthreads();                                    // s_tile is rewritten next
     }
 }
 

@@ -209,7 +209,8 @@ def test_tuning_knobs_change_no_pixel_and_autotune_keeps_one(device):
     flags = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
     base = r2.render_batch(sc, cams, flags=flags)
     for kw in ({"pair_sort_bits": 7}, {"pair_sort_bits": 6}, {"raster_shape": "16x2"}, {"raster_shape": "4x8"},
-               {"raster_shape": "8x8x2"}, {"raster_shape": "8x4-f32x2"},
+               {"raster_shape": "8x8x2"}, {"raster_shape": "8x4-f32x2"}, {"raster_shape": "tile-f32x2"},
+               {"raster_shape": "tile-f32x2", "bin_tile": "32x8"}, {"raster_shape": "tile-f32x2", "bin_tile": "8x8"},
                {"raster_ctas_per_sm": 3}, {"raster_ctas_per_sm": 1},
                {"pair_sort_bits": 6, "raster_shape": "4x8", "raster_ctas_per_sm": 2},
                {"bin_tile": "8x8"}, {"bin_tile": "32x8"}, {"bin_tile": "8x8", "raster_shape": "8x8x2"},
