@@ -431,13 +431,15 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
             pa.g_begin = f.upload->bounds[k];
             pa.g_end = f.upload->bounds[k + 1];
             if (pa.g_end > pa.g_begin) {
-                dlr::project_k<<<(pa.g_end - pa.g_begin + 255) / 256, 256, 0, st>>>(pa);
+                if (d.fastExp) dlr::project_k<true><<<(pa.g_end - pa.g_begin + 255) / 256, 256, 0, st>>>(pa);
+                else dlr::project_k<false><<<(pa.g_end - pa.g_begin + 255) / 256, 256, 0, st>>>(pa);
                 (*launches)++;
                 DL_CK(cudaGetLastError());
             }
         }
     } else if (d.N) {
-        dlr::project_k<<<(d.N + 255) / 256, 256, 0, st>>>(pa);
+        if (d.fastExp) dlr::project_k<true><<<(d.N + 255) / 256, 256, 0, st>>>(pa);
+        else dlr::project_k<false><<<(d.N + 255) / 256, 256, 0, st>>>(pa);
         (*launches)++;
     }
     DL_CK(cudaGetLastError());
@@ -583,7 +585,8 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
         ca.vis_mask = f.visMask;
         ca.recBC = d.f16rec ? nullptr : f.recBC;
         ca.recH = d.f16rec ? f.recH : nullptr;
-        dlr::colour_k<<<(d.N + 255) / 256, 256, 0, st>>>(ca);
+        if (d.fastExp) dlr::colour_k<true><<<(d.N + 255) / 256, 256, 0, st>>>(ca);
+        else dlr::colour_k<false><<<(d.N + 255) / 256, 256, 0, st>>>(ca);
         (*launches)++;
         DL_CK(cudaGetLastError());
     }

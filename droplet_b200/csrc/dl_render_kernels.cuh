@@ -80,7 +80,15 @@ __device__ __forceinline__ float sh_coef(const DlSceneDev& sc, uint64_t i) {
     return __ldg(sc.sh + i);
 }
 
+// acc + b * c: the shader's separate multiply and add, or (kFma, the +-1 LSB
+// arithmetic of DL_BATCH_FAST_EXP frames) one fused multiply-add
+template <bool kFma>
+__device__ __forceinline__ float sh_acc(float acc, float b, float c) {
+    return kFma ? __fmaf_rn(b, c, acc) : acc + b * c;
+}
+
 // project.ts:264-331 evalSH (channel-major coefficients, camera-space direction)
+template <bool kFma>
 __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int M, float x, float y, float z,
                                         float& r, float& g, float& b) {
     const float SH1 = 0.4886025119029199f, nSH1 = -0.4886025119029199f;
@@ -88,9 +96,9 @@ __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int
     r = 0.0f; g = 0.0f; b = 0.0f;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        r = r + b1[k] * sh_coef(sc, base + k);
-        g = g + b1[k] * sh_coef(sc, base + M + k);
-        b = b + b1[k] * sh_coef(sc, base + 2 * M + k);
+        r = sh_acc<kFma>(r, b1[k], sh_coef(sc, base + k));
+        g = sh_acc<kFma>(g, b1[k], sh_coef(sc, base + M + k));
+        b = sh_acc<kFma>(b, b1[k], sh_coef(sc, base + 2 * M + k));
     }
     if (sc.bands >= 2) {
         const float xx = x * x, yy = y * y, zz = z * z;
@@ -100,9 +108,9 @@ __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int
                              0.5462742152960396f * (xx - yy)};
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            r = r + b2[k] * sh_coef(sc, base + 3 + k);
-            g = g + b2[k] * sh_coef(sc, base + M + 3 + k);
-            b = b + b2[k] * sh_coef(sc, base + 2 * M + 3 + k);
+            r = sh_acc<kFma>(r, b2[k], sh_coef(sc, base + 3 + k));
+            g = sh_acc<kFma>(g, b2[k], sh_coef(sc, base + M + 3 + k));
+            b = sh_acc<kFma>(b, b2[k], sh_coef(sc, base + 2 * M + 3 + k));
         }
         if (sc.bands >= 3) {
             const float b3[7] = {(-0.5900435899266435f * y) * ((3.0f * xx) - yy),
@@ -114,9 +122,9 @@ __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int
                                  (-0.5900435899266435f * x) * (xx - (3.0f * yy))};
 #pragma unroll
             for (int k = 0; k < 7; k++) {
-                r = r + b3[k] * sh_coef(sc, base + 8 + k);
-                g = g + b3[k] * sh_coef(sc, base + M + 8 + k);
-                b = b + b3[k] * sh_coef(sc, base + 2 * M + 8 + k);
+                r = sh_acc<kFma>(r, b3[k], sh_coef(sc, base + 8 + k));
+                g = sh_acc<kFma>(g, b3[k], sh_coef(sc, base + M + 8 + k));
+                b = sh_acc<kFma>(b, b3[k], sh_coef(sc, base + 2 * M + 8 + k));
             }
         }
     }
@@ -124,7 +132,7 @@ __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int
 
 // evalSH on the 16-bit SH block of one Gaussian (same basis, same summation
 // order as eval_sh): the block is read with 128-bit loads.
-template <int BANDS>
+template <int BANDS, bool kFma>
 __device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, float x, float y, float z,
                                           float& r, float& gr, float& b) {
     constexpr int M = BANDS == 1 ? 3 : BANDS == 2 ? 8 : 15;
@@ -147,9 +155,9 @@ __device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, floa
     r = 0.0f; gr = 0.0f; b = 0.0f;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        r = r + b1[k] * coef(k, 0);
-        gr = gr + b1[k] * coef(k, 1);
-        b = b + b1[k] * coef(k, 2);
+        r = sh_acc<kFma>(r, b1[k], coef(k, 0));
+        gr = sh_acc<kFma>(gr, b1[k], coef(k, 1));
+        b = sh_acc<kFma>(b, b1[k], coef(k, 2));
     }
     if (BANDS >= 2) {
         const float xx = x * x, yy = y * y, zz = z * z;
@@ -159,9 +167,9 @@ __device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, floa
                              0.5462742152960396f * (xx - yy)};
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            r = r + b2[k] * coef(3 + k, 0);
-            gr = gr + b2[k] * coef(3 + k, 1);
-            b = b + b2[k] * coef(3 + k, 2);
+            r = sh_acc<kFma>(r, b2[k], coef(3 + k, 0));
+            gr = sh_acc<kFma>(gr, b2[k], coef(3 + k, 1));
+            b = sh_acc<kFma>(b, b2[k], coef(3 + k, 2));
         }
         if (BANDS >= 3) {
             const float b3[7] = {(-0.5900435899266435f * y) * ((3.0f * xx) - yy),
@@ -173,9 +181,9 @@ __device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, floa
                                  (-0.5900435899266435f * x) * (xx - (3.0f * yy))};
 #pragma unroll
             for (int k = 0; k < 7; k++) {
-                r = r + b3[k] * coef(8 + k, 0);
-                gr = gr + b3[k] * coef(8 + k, 1);
-                b = b + b3[k] * coef(8 + k, 2);
+                r = sh_acc<kFma>(r, b3[k], coef(8 + k, 0));
+                gr = sh_acc<kFma>(gr, b3[k], coef(8 + k, 1));
+                b = sh_acc<kFma>(b, b3[k], coef(8 + k, 2));
             }
         }
     }
@@ -189,6 +197,7 @@ __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
 // Splat colour for one view (project.ts:236-251): DC plus the SH bands
 // evaluated along the normalised view-space position, + 0.5, clamped at 0.
 // project_k and colour_k both call this, so deferred colours are bit-identical.
+template <bool kFma>
 __device__ __forceinline__ void splat_colour(const DlSceneDev& sc, uint32_t g, int M, const float dc[3], float pcx,
                                              float pcy, float pcz, float& c0, float& c1, float& c2) {
     float col0 = dc[0], col1 = dc[1], col2 = dc[2];
@@ -197,11 +206,11 @@ __device__ __forceinline__ void splat_colour(const DlSceneDev& sc, uint32_t g, i
         float sr, sg, sb;
         const float dxn = pcx / len, dyn = pcy / len, dzn = pcz / len;
         if (sc.sh16) {
-            if (sc.bands == 1) eval_sh16<1>(sc, g, dxn, dyn, dzn, sr, sg, sb);
-            else if (sc.bands == 2) eval_sh16<2>(sc, g, dxn, dyn, dzn, sr, sg, sb);
-            else eval_sh16<3>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            if (sc.bands == 1) eval_sh16<1, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else if (sc.bands == 2) eval_sh16<2, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else eval_sh16<3, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
         } else {
-            eval_sh(sc, (uint64_t)g * 3 * M, M, dxn, dyn, dzn, sr, sg, sb);
+            eval_sh<kFma>(sc, (uint64_t)g * 3 * M, M, dxn, dyn, dzn, sr, sg, sb);
         }
         col0 = col0 + sr; col1 = col1 + sg; col2 = col2 + sb;
     }
@@ -216,6 +225,8 @@ constexpr int kProjectMaxViews = 4096;          // views per frame (per-CTA visi
 constexpr uint32_t kProjectSmemViews = 64;      // view tables staged in shared memory up to this count
 static_assert(sizeof(DlView) % 4 == 0, "DlView is copied as 32-bit words");
 
+// kFma: DL_BATCH_FAST_EXP frames evaluate the SH colour with fused multiply-adds
+template <bool kFma>
 __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
     __shared__ uint32_t s_vis[kProjectMaxViews];
     __shared__ DlView s_views[kProjectSmemViews];
@@ -462,7 +473,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         // deferred: colour_k fills the colour once the SH has arrived
         float col0 = 0.0f, col1 = 0.0f, col2 = 0.0f;
         if (a.vis_mask) mword |= 1u << (v & 31u);
-        else splat_colour(a.sc, g, M, dc, pcx, pcy, pcz, col0, col1, col2);
+        else splat_colour<kFma>(a.sc, g, M, dc, pcx, pcy, pcz, col0, col1, col2);
         // cull mode: the screen record carries the half-extents of the box the
         // rasterizer tests (the ellipse's box, or the radius square) instead of
         // (radius, depth), which it does not read there
@@ -502,6 +513,7 @@ struct ColourArgs {
     uint4* recH;
 };
 
+template <bool kFma>
 __global__ void __launch_bounds__(256) colour_k(ColourArgs a) {
     __shared__ DlView s_views[kProjectSmemViews];
     const bool staged = a.num_views <= kProjectSmemViews;
@@ -531,7 +543,7 @@ __global__ void __launch_bounds__(256) colour_k(ColourArgs a) {
             const float pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
             const float pcz = ((V[2] * pos[0] + V[6] * pos[1]) + V[10] * pos[2]) + V[14];
             float c0, c1, c2;
-            splat_colour(a.sc, g, M, dc, pcx, pcy, pcz, c0, c1, c2);
+            splat_colour<kFma>(a.sc, g, M, dc, pcx, pcy, pcz, c0, c1, c2);
             const uint64_t o = (uint64_t)v * a.view_stride + g;
             if (a.recBC) a.recBC[2 * o + 1] = make_float4(c0, c1, c2, 0.0f);
             else reinterpret_cast<uint2*>(a.recH + o)[1] = make_uint2(pack_h2(c0, c1), pack_h2(c2, 0.0f));
