@@ -190,7 +190,7 @@ class Renderer:
         check(_lib.load().dl_render_batch(self.handle, scene._h, cams, n, _bg(background), ptrs, flags))
         return host
 
-    RASTER_SHAPES = ("8x4", "16x2", "4x8", "8x8x2", "8x4-f32x2", "tile-f32x2")
+    RASTER_SHAPES = ("8x4", "16x2", "4x8", "8x8x2", "8x4-f32x2", "tile-f32x2", "tile")
 
     BIN_TILES = ("16x16", "8x8", "32x8")
 

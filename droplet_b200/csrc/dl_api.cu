@@ -374,7 +374,7 @@ extern "C" int dl_renderer_debug_get(dl_renderer* r, const char* name, void* dst
 
 extern "C" int dl_renderer_set_tuning(dl_renderer* r, const dl_tuning* t) {
     if (!r || !t) { dl_set_error("dl_renderer_set_tuning: NULL argument"); return DL_E_INVALID_ARG; }
-    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 5 ||
+    if (t->pair_sort_bits < 6 || t->pair_sort_bits > 8 || t->raster_shape < 0 || t->raster_shape > 6 ||
         t->raster_ctas_per_sm < 0 || t->raster_ctas_per_sm > 5 || t->bin_tile < 0 || t->bin_tile > 2) {
         dl_set_error("dl_renderer_set_tuning: knob out of range");
         return DL_E_INVALID_ARG;
@@ -432,16 +432,16 @@ extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera
     double curMs = 0.0;
     int rc = timeOne(cur, &curMs);
     // shapes 4 and 5 (two splats per step in f32x2) exist for the fast arithmetic only
-    const int bitsC[6] = {8, 7, 6, 8, 8, 8}, shapeC[6] = {5, 4, 0, 1, 2, 3}, ctasC[6] = {0, 4, 3, 0, 0, 0};
-    const int tileC[6] = {0, 1, 2, 0, 0, 0};
+    const int bitsC[7] = {8, 7, 6, 8, 8, 8, 8}, shapeC[7] = {6, 5, 4, 0, 1, 2, 3}, ctasC[7] = {0, 4, 3, 0, 0, 0, 0};
+    const int tileC[7] = {0, 1, 2, 0, 0, 0, 0};
     const bool fast = (flags & DL_BATCH_FAST_EXP) != 0;
-    const int nC[4] = {3, 6, 3, 3};
+    const int nC[4] = {3, 7, 3, 3};
     for (int knob = 0; knob < 4 && rc == DL_OK; knob++) {
         for (int c = 0; c < nC[knob] && rc == DL_OK; c++) {
             DlTuning t = cur;
             if (knob == 0) { if (t.pair_bits == bitsC[c]) continue; t.pair_bits = bitsC[c]; }
             if (knob == 1) {
-                if (t.shape == shapeC[c] || (shapeC[c] >= 4 && !fast)) continue;
+                if (t.shape == shapeC[c] || ((shapeC[c] == 4 || shapeC[c] == 5) && !fast)) continue;
                 t.shape = shapeC[c];
             }
             if (knob == 2) { if (t.ctas_per_sm == ctasC[c]) continue; t.ctas_per_sm = ctasC[c]; }

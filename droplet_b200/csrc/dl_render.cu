@@ -283,6 +283,7 @@ struct FrameDims {
     bool ppl2 = false;                   // two pixels per lane (8x8 work items)
     bool x2 = false;                     // two splats per step in f32x2 arithmetic (fast variant)
     bool tileCta = false;                // one CTA per 256-pixel tile, the slice read once (fast variant)
+    bool tileK = false;                  // one CTA per 256-pixel tile, records read in place (both variants)
     int iptLg = 3;                       // log2 of the rasterizer work items per binning tile
 };
 
@@ -326,16 +327,21 @@ bool dl_retile_views(DlView* v, uint32_t V, uint32_t tw, uint32_t th) {
 }
 
 // Persistent rasterizer grid: every SM filled to its occupancy limit.
-uint32_t raster_grid(bool fastExp, bool ppl2, bool x2, bool tileCta) {
-    static int cached[64][6] = {};
+uint32_t raster_grid(bool fastExp, bool ppl2, bool x2, bool tileCta, bool tileK) {
+    static int cached[64][8] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int kind = tileCta ? 5 : x2 ? 4 : (fastExp ? 1 : 0) + (ppl2 ? 2 : 0);
+    const int kind = tileK ? (fastExp ? 7 : 6) : tileCta ? 5 : x2 ? 4 : (fastExp ? 1 : 0) + (ppl2 ? 2 : 0);
     int* c = (dev >= 0 && dev < 64) ? &cached[dev][kind] : nullptr;
     if (c && *c) return (uint32_t)*c;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (tileCta) {
+    if (tileK) {
+        if (fastExp) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_tile_k<false, false>,
+                                                                   dlr::kRasterThreads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_tile_k<true, false>,
+                                                           dlr::kRasterThreads, 0);
+    } else if (tileCta) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_tile_x2_k<false>, dlr::kRasterThreads, 0);
     } else if (x2) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dlr::rasterize_x2_k<false>, dlr::kRasterThreads, 0);
@@ -385,12 +391,13 @@ FrameDims frame_dims(const DlView* hv, uint32_t V, uint32_t N, uint64_t cap, uin
     // work items must fit the binning tile (every view of a frame has the same tile)
     const uint32_t tw = V ? hv[0].tileW : DL_TILE, th = V ? hv[0].tileH : DL_TILE;
     d.tileCta = t.shape == 5 && d.fastExp && tw * th == 256u;   // 8 warps of 8x4 items per tile
+    d.tileK = t.shape == 6 && tw * th == 256u;
     const uint32_t iw = d.ppl2 ? 8u : (1u << d.subLw), ih = d.ppl2 ? 8u : (32u >> d.subLw);
     if (iw > tw || ih > th) { d.subLw = 3; d.ppl2 = false; }
-    const uint32_t ipt = d.tileCta ? 1u : tw * th / (d.ppl2 ? 64u : 32u);
+    const uint32_t ipt = (d.tileCta || d.tileK) ? 1u : tw * th / (d.ppl2 ? 64u : 32u);
     d.iptLg = 0;
     while ((1u << d.iptLg) < ipt) d.iptLg++;
-    d.rasterGrid = raster_grid(d.fastExp, d.ppl2, d.x2, d.tileCta);
+    d.rasterGrid = raster_grid(d.fastExp, d.ppl2, d.x2, d.tileCta, d.tileK);
     if (t.ctas_per_sm > 0) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -634,7 +641,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ra.work = work;
     const bool count = f.evalCount || f.tileEvals;
     // counting frames run the 8x4 warp-item kernel: 8 items per 256-pixel tile
-    const int iptLg = (d.tileCta && count) ? 3 : d.iptLg;
+    const int iptLg = ((d.tileCta || d.tileK) && count) ? 3 : d.iptLg;
     ra.item_base = 0;
     ra.num_items = (1u << iptLg) * d.totalTiles;
     ra.ipt_lg = iptLg;
@@ -646,7 +653,15 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ra.rec_box = d.cullOff ? 1 : 0;
     ra.stage_pad = stage_pad();
     auto raster = [&](const dlr::RasterArgs& x) {
-        if (d.tileCta && !count) {
+        if (d.tileK && !count) {
+            if (d.fastExp) {
+                if (x.tile_cycles) dlr::rasterize_tile_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                else dlr::rasterize_tile_k<false, false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            } else {
+                if (x.tile_cycles) dlr::rasterize_tile_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                else dlr::rasterize_tile_k<true, false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            }
+        } else if (d.tileCta && !count) {
             if (x.tile_cycles) dlr::rasterize_tile_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
             else dlr::rasterize_tile_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
         } else if (d.x2 && !count) {
@@ -902,7 +917,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             key.insert(key.end(), {V, N, d.maxT, d.TS, d.totalTiles, d.stride, d.cap, (uint64_t)flags, d.rasterGrid,
                                    (uint64_t)d.pbits, (uint64_t)d.subLw, (uint64_t)d.ppl2, (uint64_t)d.x2,
                                    (uint64_t)d.iptLg, (uint64_t)hv[0].tileW, (uint64_t)hv[0].tileH,
-                                   (uint64_t)d.tileCta,
+                                   (uint64_t)d.tileCta, (uint64_t)d.tileK,
                                    g_dl_wait.spin_limit,
                                    g_dl_wait.withheld(DL_WAIT_STAGE_DEPTH_SORT), g_dl_wait.withheld(DL_WAIT_STAGE_EMIT),
                                    g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT)});

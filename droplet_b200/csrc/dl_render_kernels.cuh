@@ -1683,4 +1683,166 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterA
     }
 }
 
+// ---- one CTA per tile, staged records read in place (both arithmetic variants)
+// As rasterize_tile_x2_k, a persistent CTA of 8 warps takes whole 256-pixel
+// tiles and reads the slice once, 256 pairs per batch, one pair per thread.
+// The staging thread computes the 8x4 work items its splat's box reaches from
+// the box's column and row ranges (pixel-centre rectangles widened by the
+// staging margin) and stores the record once, in the form the compositing
+// loop reads it (3 x float4: x, y and the conic, opacity, colour).  A warp
+// then lists the batch slots of its own item in slice order (ballots, one
+// byte per listed slot) and composites straight from the staged records — no
+// per-warp copy — with rasterize.ts:62-79 per pixel in slice order: the exact
+// arithmetic of raster_subtile (kExactExp) or its fast loop.  There is no
+// per-pixel box test: at pixels outside the box alpha < 1/255 is skipped.
+template <bool kExactExp, bool kCycles>
+__global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs a) {
+    __shared__ float4 s_r[3][kTileStage];      // staged records
+    __shared__ uint8_t s_m[kTileStage];        // items the staged splat reaches (bit w: item w)
+    __shared__ uint8_t s_l[kRasterWarps][kTileStage];   // per warp: its batch slots in order
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t lmask = dl_lanemask_lt();
+    while (true) {
+        if (tid == 0) s_tile = a.item_base + atomicAdd(a.work_counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_tile;
+        if (item >= a.num_items) return;
+        const uint32_t gt = a.work ? a.work[item] : item;
+        const uint32_t v = view_of_tile(a, gt);
+        const uint32_t tile = gt - a.tile_base[v];
+        const DlView& u = a.views[v];
+        const long long t0 = kCycles ? clock64() : 0;
+        const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
+        const uint32_t perRow = u.tileW >> 3;              // 8x4 items per tile row
+        const uint32_t rows = u.tileH >> 2;
+        const uint32_t ox = tx * u.tileW, oy = ty * u.tileH;
+        const uint32_t x = ox + (warp % perRow) * 8u + (lane & 7), y = oy + (warp / perRow) * 4u + (lane >> 3);
+        const bool inImage = x < u.W && y < u.H;
+        const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+        const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+        const uint32_t start = to[tile], end = to[tile + 1];
+        const uint32_t* vals = a.pair_vals + a.pair_base[v];
+        const uint64_t vo = (uint64_t)v * a.view_stride;
+        const float pad = a.stage_pad;
+        float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
+        bool done = !inImage;
+        for (uint32_t b = start; b < end; b += kTileStage) {
+            // ---- stage one pair per thread
+            uint32_t mask = 0;
+            const uint32_t e = b + (uint32_t)tid;
+            if (e < end) {
+                const uint32_t g = __ldg(vals + e);
+                if (!(g & kPhantomBit)) {
+                    const float4 ra = __ldg(a.recA + vo + g);
+                    float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
+                    if (ex > 0.0f) {
+                        float A, B, C, al, cr, cg, cb;
+                        if (a.recBC) {
+                            const float4 p = __ldg(a.recBC + 2 * (vo + g));
+                            const float4 q = __ldg(a.recBC + 2 * (vo + g) + 1);
+                            A = p.x; B = p.y; C = p.z; al = p.w; cr = q.x; cg = q.y; cb = q.z;
+                        } else {
+                            const uint4 hv = __ldg(a.recH + vo + g);
+                            const float2 ab = __half22float2(*reinterpret_cast<const __half2*>(&hv.x));
+                            const float2 ca = __half22float2(*reinterpret_cast<const __half2*>(&hv.y));
+                            const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&hv.z));
+                            const float2 bz = __half22float2(*reinterpret_cast<const __half2*>(&hv.w));
+                            A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
+                        }
+                        if (!a.rec_box) tight_extent(A, B, C, ra.z, ex, ey);
+                        // item column c covers pixel centres ox + 8c + 0.5 .. ox + 8c + 7.5,
+                        // item row r covers oy + 4r + 0.5 .. oy + 4r + 3.5
+                        const float lx = ra.x - ex - pad - (float)ox, hx = ra.x + ex + pad - (float)ox;
+                        const float ly = ra.y - ey - pad - (float)oy, hy = ra.y + ey + pad - (float)oy;
+                        const int cA = max(0, (int)ceilf((lx - 7.5f) * 0.125f));
+                        const int cB = min((int)perRow - 1, (int)floorf((hx - 0.5f) * 0.125f));
+                        const int rA = max(0, (int)ceilf((ly - 3.5f) * 0.25f));
+                        const int rB = min((int)rows - 1, (int)floorf((hy - 0.5f) * 0.25f));
+                        if (cA <= cB && rA <= rB && hx >= 0.5f && hy >= 0.5f &&
+                            lx <= (float)u.tileW - 0.5f && ly <= (float)u.tileH - 0.5f) {
+                            const uint32_t cm = ((1u << (cB + 1)) - 1u) & ~((1u << cA) - 1u);
+                            for (int r = rA; r <= rB; r++) mask |= cm << (r * (int)perRow);
+                            if (kExactExp) {
+                                s_r[0][tid] = make_float4(ra.x, ra.y, A, 2.0f * B);
+                            } else {
+                                // conic pre-scaled by -0.5*log2(e): the quadratic form is ex2's argument
+                                s_r[0][tid] = make_float4(ra.x, ra.y, -0.72134752044448170f * A,
+                                                          -1.4426950408889634f * B);
+                                C = -0.72134752044448170f * C;
+                            }
+                            s_r[1][tid] = make_float4(C, al, cr, cg);
+                            s_r[2][tid] = make_float4(cb, 0.0f, 0.0f, 0.0f);
+                        }
+                    }
+                }
+            }
+            s_m[tid] = (uint8_t)mask;
+            __syncthreads();
+            const uint32_t nb = min((uint32_t)kTileStage, end - b);
+            if (!__all_sync(0xffffffffu, done)) {
+                // ---- this warp's slots, in slice order
+                uint32_t n = 0;
+                for (uint32_t c = 0; c < nb; c += 32) {
+                    const uint32_t i = c + (uint32_t)lane;
+                    const bool hit = i < nb && ((s_m[i] >> warp) & 1u);
+                    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) s_l[warp][n + __popc(m & lmask)] = (uint8_t)i;
+                    n += __popc(m);
+                }
+                __syncwarp();
+                if (!done) {
+                    for (uint32_t j = 0; j < n; j++) {
+                        const uint32_t i = s_l[warp][j];
+                        const float4 r0 = s_r[0][i], r1 = s_r[1][i];
+                        const float dx = px - r0.x, dy = py - r0.y;
+                        float alpha;
+                        if (kExactExp) {
+                            const float power = -0.5f * ((((r0.z * dx) * dx) + ((r0.w * dx) * dy)) + ((r1.x * dy) * dy));
+                            if (power > 0.0f || power <= DL_POWER_CUT) continue;
+                            alpha = r1.y * fmaxf(0.0f, dl_expf(power) - DL_GAUSS_FLOOR);
+                        } else {
+                            const float p2 = __fmaf_rn(dx, __fmaf_rn(r0.z, dx, r0.w * dy), r1.x * dy * dy);
+                            if (p2 > 0.0f) continue;
+                            float ev;
+                            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ev) : "f"(p2));
+                            alpha = r1.y * (ev - DL_GAUSS_FLOOR);
+                        }
+                        if (alpha < DL_MIN_ALPHA) continue;
+                        const float w = T * alpha;
+                        const float cbl = s_r[2][i].x;
+                        if (kExactExp) {
+                            c0 = c0 + w * r1.z;
+                            c1 = c1 + w * r1.w;
+                            c2 = c2 + w * cbl;
+                            T = T * (1.0f - alpha);
+                        } else {
+                            c0 = __fmaf_rn(w, r1.z, c0);
+                            c1 = __fmaf_rn(w, r1.w, c1);
+                            c2 = __fmaf_rn(w, cbl, c2);
+                            T = __fmaf_rn(-T, alpha, T);
+                        }
+                        if (T < DL_MIN_T) { done = true; break; }
+                    }
+                }
+            }
+            // every warp is past this batch's staging area; stop once all pixels are done
+            if (__syncthreads_and(done)) break;
+        }
+        if (inImage) {
+            // finalize.ts:30-43
+            const float rr = fminf(fmaxf(c0 + T * u.bg[0], 0.0f), 1.0f);
+            const float gg = fminf(fmaxf(c1 + T * u.bg[1], 0.0f), 1.0f);
+            const float bb = fminf(fmaxf(c2 + T * u.bg[2], 0.0f), 1.0f);
+            const float aa = fminf(fmaxf((1.0f - T) + T * u.bg[3], 0.0f), 1.0f);
+            const uint32_t out = dl_sat_u32(rr * 255.0f + 0.5f) | (dl_sat_u32(gg * 255.0f + 0.5f) << 8) |
+                                 (dl_sat_u32(bb * 255.0f + 0.5f) << 16) | (dl_sat_u32(aa * 255.0f + 0.5f) << 24);
+            a.outs[v][(uint64_t)y * u.W + x] = out;
+            if (a.accum) a.accum[(uint64_t)y * u.W + x] = make_float4(c0, c1, c2, T);
+        }
+        if (kCycles && tid == 0) atomicAdd(&a.tile_cycles[gt], (uint32_t)((clock64() - t0) >> 4));
+        __syncthreads();                                    // s_tile is rewritten next
+    }
+}
+
 }  // namespace dlr

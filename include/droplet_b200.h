@@ -195,7 +195,9 @@ typedef struct dl_tuning {
                                      3 = 8x8 with two pixels per lane, 4 = 8x4 taking two splats per step
                                      in packed f32x2 arithmetic, 5 = the same with one CTA per 256-pixel
                                      tile reading the tile's pairs once (4 and 5: DL_BATCH_FAST_EXP frames,
-                                     others use 0; 5 with 8x8 tiles uses 4) */
+                                     others use 0; 5 with 8x8 tiles uses 4), 6 = one CTA per 256-pixel tile
+                                     compositing the staged records in place, either arithmetic (with 8x8
+                                     tiles it uses 0) */
     int32_t raster_ctas_per_sm;   /* persistent rasterizer CTAs per SM, 1..5; 0 = the occupancy limit */
     int32_t bin_tile;             /* binning tile: 0 = 16x16 (default), 1 = 8x8, 2 = 32x8; work items that do
                                      not fit the tile fall back to 8x4 */

@@ -211,6 +211,8 @@ def test_tuning_knobs_change_no_pixel_and_autotune_keeps_one(device):
     for kw in ({"pair_sort_bits": 7}, {"pair_sort_bits": 6}, {"raster_shape": "16x2"}, {"raster_shape": "4x8"},
                {"raster_shape": "8x8x2"}, {"raster_shape": "8x4-f32x2"}, {"raster_shape": "tile-f32x2"},
                {"raster_shape": "tile-f32x2", "bin_tile": "32x8"}, {"raster_shape": "tile-f32x2", "bin_tile": "8x8"},
+               {"raster_shape": "tile"}, {"raster_shape": "tile", "bin_tile": "32x8"},
+               {"raster_shape": "tile", "bin_tile": "8x8"},
                {"raster_ctas_per_sm": 3}, {"raster_ctas_per_sm": 1},
                {"pair_sort_bits": 6, "raster_shape": "4x8", "raster_ctas_per_sm": 2},
                {"bin_tile": "8x8"}, {"bin_tile": "32x8"}, {"bin_tile": "8x8", "raster_shape": "8x8x2"},
@@ -230,6 +232,10 @@ def test_tuning_knobs_change_no_pixel_and_autotune_keeps_one(device):
         assert np.array_equal(a, renderer_single(device, d, c))
     for tile in ("8x8", "32x8"):           # exact path binned with other tiles, bit-exact too
         r2.set_tuning(bin_tile=tile)
+        for a, c in zip(r2.render_batch(sc32, cams), cams):
+            assert np.array_equal(a, renderer_single(device, d, c)), tile
+    for tile in ("16x16", "32x8"):         # exact path, one CTA per tile
+        r2.set_tuning(raster_shape="tile", bin_tile=tile)
         for a, c in zip(r2.render_batch(sc32, cams), cams):
             assert np.array_equal(a, renderer_single(device, d, c)), tile
     r2.set_tuning()
