@@ -1686,22 +1686,26 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterA
 // ---- one CTA per tile, staged records read in place (both arithmetic variants)
 // As rasterize_tile_x2_k, a persistent CTA of 8 warps takes whole 256-pixel
 // tiles and reads the slice once, 256 pairs per batch, one pair per thread.
-// The staging thread computes the 8x4 work items its splat's box reaches from
-// the box's column and row ranges (pixel-centre rectangles widened by the
-// staging margin) and stores the record once, in the form the compositing
-// loop reads it (3 x float4: x, y and the conic, opacity, colour).  A warp
-// then lists the batch slots of its own item in slice order (ballots, one
-// byte per listed slot) and composites straight from the staged records — no
-// per-warp copy — with rasterize.ts:62-79 per pixel in slice order: the exact
-// arithmetic of raster_subtile (kExactExp) or its fast loop.  There is no
-// per-pixel box test: at pixels outside the box alpha < 1/255 is skipped.
+// The work is split into 4x4-pixel cells, 16 per tile: each half-warp owns
+// one cell (lanes 0-15 the left half of warp w's 8x4 block, lanes 16-31 the
+// right half) and composites its own list of splats, so a splat that reaches
+// only one half of the block costs the other half nothing.  The staging
+// thread computes the cells its splat's box reaches from the box's column and
+// row ranges (pixel-centre rectangles widened by the staging margin) and
+// stores the record once, in the form the compositing loop reads it (x, y and
+// the conic, opacity, colour).  Each half-warp then lists the batch slots of
+// its cell in slice order (ballots, one byte per slot) and composites straight
+// from the staged records with rasterize.ts:62-79 per pixel in slice order:
+// the exact arithmetic of raster_subtile (kExactExp) or its fast loop.  There
+// is no per-pixel box test: at pixels outside the box alpha < 1/255 is skipped.
 template <bool kExactExp, bool kCycles>
 __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs a) {
-    __shared__ float4 s_r[3][kTileStage];      // staged records
-    __shared__ uint8_t s_m[kTileStage];        // items the staged splat reaches (bit w: item w)
-    __shared__ uint8_t s_l[kRasterWarps][kTileStage];   // per warp: its batch slots in order
+    __shared__ float4 s_r[2][kTileStage];      // staged records: (x, y, A, B), (C, alpha, r, g)
+    __shared__ float s_b[kTileStage];          // staged blue
+    __shared__ uint16_t s_m[kTileStage];       // cells the staged splat reaches (bit c: cell c, row-major)
+    __shared__ uint8_t s_l[kRasterWarps][2][kTileStage];   // per half-warp: its batch slots in order
     __shared__ uint32_t s_tile;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, half = lane >> 4;
     const uint32_t lmask = dl_lanemask_lt();
     while (true) {
         if (tid == 0) s_tile = a.item_base + atomicAdd(a.work_counter, 1u);
@@ -1714,10 +1718,12 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs
         const DlView& u = a.views[v];
         const long long t0 = kCycles ? clock64() : 0;
         const uint32_t tx = tile % u.tilesX, ty = tile / u.tilesX;
-        const uint32_t perRow = u.tileW >> 3;              // 8x4 items per tile row
-        const uint32_t rows = u.tileH >> 2;
+        const uint32_t perRow = u.tileW >> 3;               // 8x4 blocks (one per warp) per tile row
+        const uint32_t cols = u.tileW >> 2, rows = u.tileH >> 2;   // 4x4 cells
         const uint32_t ox = tx * u.tileW, oy = ty * u.tileH;
-        const uint32_t x = ox + (warp % perRow) * 8u + (lane & 7), y = oy + (warp / perRow) * 4u + (lane >> 3);
+        const uint32_t cx = (warp % perRow) * 2u + (uint32_t)half, cy = warp / perRow;
+        const uint32_t cell = cy * cols + cx;
+        const uint32_t x = ox + cx * 4u + (lane & 3), y = oy + cy * 4u + ((lane >> 2) & 3);
         const bool inImage = x < u.W && y < u.H;
         const float px = (float)x + 0.5f, py = (float)y + 0.5f;
         const uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
@@ -1751,18 +1757,17 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs
                             A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
                         }
                         if (!a.rec_box) tight_extent(A, B, C, ra.z, ex, ey);
-                        // item column c covers pixel centres ox + 8c + 0.5 .. ox + 8c + 7.5,
-                        // item row r covers oy + 4r + 0.5 .. oy + 4r + 3.5
+                        // cell column c covers pixel centres ox + 4c + 0.5 .. ox + 4c + 3.5,
+                        // cell row r covers oy + 4r + 0.5 .. oy + 4r + 3.5
                         const float lx = ra.x - ex - pad - (float)ox, hx = ra.x + ex + pad - (float)ox;
                         const float ly = ra.y - ey - pad - (float)oy, hy = ra.y + ey + pad - (float)oy;
-                        const int cA = max(0, (int)ceilf((lx - 7.5f) * 0.125f));
-                        const int cB = min((int)perRow - 1, (int)floorf((hx - 0.5f) * 0.125f));
+                        const int cA = max(0, (int)ceilf((lx - 3.5f) * 0.25f));
+                        const int cB = min((int)cols - 1, (int)floorf((hx - 0.5f) * 0.25f));
                         const int rA = max(0, (int)ceilf((ly - 3.5f) * 0.25f));
                         const int rB = min((int)rows - 1, (int)floorf((hy - 0.5f) * 0.25f));
-                        if (cA <= cB && rA <= rB && hx >= 0.5f && hy >= 0.5f &&
-                            lx <= (float)u.tileW - 0.5f && ly <= (float)u.tileH - 0.5f) {
+                        if (cA <= cB && rA <= rB) {
                             const uint32_t cm = ((1u << (cB + 1)) - 1u) & ~((1u << cA) - 1u);
-                            for (int r = rA; r <= rB; r++) mask |= cm << (r * (int)perRow);
+                            for (int r = rA; r <= rB; r++) mask |= cm << (r * (int)cols);
                             if (kExactExp) {
                                 s_r[0][tid] = make_float4(ra.x, ra.y, A, 2.0f * B);
                             } else {
@@ -1772,28 +1777,34 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs
                                 C = -0.72134752044448170f * C;
                             }
                             s_r[1][tid] = make_float4(C, al, cr, cg);
-                            s_r[2][tid] = make_float4(cb, 0.0f, 0.0f, 0.0f);
+                            s_b[tid] = cb;
                         }
                     }
                 }
             }
-            s_m[tid] = (uint8_t)mask;
+            s_m[tid] = (uint16_t)mask;
             __syncthreads();
             const uint32_t nb = min((uint32_t)kTileStage, end - b);
             if (!__all_sync(0xffffffffu, done)) {
-                // ---- this warp's slots, in slice order
-                uint32_t n = 0;
+                // ---- the slots of both cells of this warp, in slice order
+                const uint32_t c0bit = (warp % perRow) * 2u + cy * cols;   // the left cell's bit
+                uint32_t n0 = 0, n1 = 0;
                 for (uint32_t c = 0; c < nb; c += 32) {
                     const uint32_t i = c + (uint32_t)lane;
-                    const bool hit = i < nb && ((s_m[i] >> warp) & 1u);
-                    const uint32_t m = __ballot_sync(0xffffffffu, hit);
-                    if (hit) s_l[warp][n + __popc(m & lmask)] = (uint8_t)i;
-                    n += __popc(m);
+                    const uint32_t mm = i < nb ? (uint32_t)s_m[i] >> c0bit : 0u;
+                    const uint32_t m0 = __ballot_sync(0xffffffffu, mm & 1u);
+                    const uint32_t m1 = __ballot_sync(0xffffffffu, mm & 2u);
+                    if (mm & 1u) s_l[warp][0][n0 + __popc(m0 & lmask)] = (uint8_t)i;
+                    if (mm & 2u) s_l[warp][1][n1 + __popc(m1 & lmask)] = (uint8_t)i;
+                    n0 += __popc(m0);
+                    n1 += __popc(m1);
                 }
                 __syncwarp();
+                const uint32_t n = half ? n1 : n0;
+                const uint8_t* lst = s_l[warp][half];
                 if (!done) {
                     for (uint32_t j = 0; j < n; j++) {
-                        const uint32_t i = s_l[warp][j];
+                        const uint32_t i = lst[j];
                         const float4 r0 = s_r[0][i], r1 = s_r[1][i];
                         const float dx = px - r0.x, dy = py - r0.y;
                         float alpha;
@@ -1810,7 +1821,7 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs
                         }
                         if (alpha < DL_MIN_ALPHA) continue;
                         const float w = T * alpha;
-                        const float cbl = s_r[2][i].x;
+                        const float cbl = s_b[i];
                         if (kExactExp) {
                             c0 = c0 + w * r1.z;
                             c1 = c1 + w * r1.w;
