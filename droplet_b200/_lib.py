@@ -28,6 +28,7 @@ DL_BATCH_SH16 = 512
 DL_BATCH_CULL_OFFSCREEN = 1024
 DL_PLY_PINNED = 1
 DL_VOX_FAST_EXP = 1
+DL_VOX_PROFILE = 2
 DL_MLP_IN, DL_MLP_HIDDEN = 12, 64
 DL_MLP_PARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 
@@ -44,6 +45,7 @@ EXPORTS = [
     "dl_renderer_set_tuning", "dl_renderer_get_tuning", "dl_renderer_autotune",
     "dl_device_set_voxel_scheduler", "dl_vox_result_block_log", "dl_test_set_wait_limit",
     "dl_test_withhold_status", "dl_test_fail_allocation", "dl_ply_load", "dl_ply_splats", "dl_ply_free",
+    "dl_vox_result_stage_times",
 ]
 
 
@@ -141,6 +143,7 @@ def load():
         "dl_ply_load": [vp, ctypes.c_size_t, i, ctypes.c_uint32, P(vp)],
         "dl_ply_splats": [vp, P(DlSplats)],
         "dl_ply_free": [vp],
+        "dl_vox_result_stage_times": [vp, P(ctypes.c_double), i],
         "dl_renderer_autotune": [vp, vp, P(DlCamera), i, P(ctypes.c_float), ctypes.c_uint32, i, P(DlTuning),
                                  P(ctypes.c_double)],
     }

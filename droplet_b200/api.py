@@ -407,6 +407,7 @@ class VoxelizeResult:
     numBlocksY: float
     numBlocksZ: float
     blockLog: Optional[tuple] = None           # (features [n, 12], cost [n]) with opts["logBlocks"]
+    stageTimes: Optional[dict] = None          # device ms per stage with opts["profile"]
 
 
 def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> VoxelizeResult:
@@ -434,7 +435,7 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
     if sh is not None:
         o.shard_index, o.shard_count = int(sh[0]), int(sh[1])
     o.log_blocks = 1 if opts.get("logBlocks") else 0
-    o.flags = _lib.DL_VOX_FAST_EXP if opts.get("fastExp") else 0
+    o.flags = (_lib.DL_VOX_FAST_EXP if opts.get("fastExp") else 0) | (_lib.DL_VOX_PROFILE if opts.get("profile") else 0)
     L = _lib.load()
     h = ctypes.c_void_p()
     check(L.dl_voxelize(device.handle, ctypes.byref(_splats(data)), ctypes.byref(o), ctypes.byref(h)))
@@ -450,6 +451,11 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
         hi = np.empty(n, np.uint32)
         if n:
             check(L.dl_vox_result_copy(h, idx.ctypes.data, lo.ctypes.data, hi.ctypes.data))
+        stages = None
+        if opts.get("profile"):
+            ms = (ctypes.c_double * 6)()
+            check(L.dl_vox_result_stage_times(h, ms, 6))
+            stages = dict(zip(("prep", "binning", "sort", "heads", "eval", "compact"), list(ms)))
         log = None
         if o.log_blocks:
             m = ctypes.c_uint64()
@@ -462,7 +468,7 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
     finally:
         L.dl_vox_result_free(h)
     return VoxelizeResult(BlockMaskBuffer(idx, lo, hi), Bounds(tuple(bmin), tuple(bmax)),
-                          o.voxel_resolution, dims[0], dims[1], dims[2], log)
+                          o.voxel_resolution, dims[0], dims[1], dims[2], log, stages)
 
 
 # ---------------------------------------------------------------- learned tile-cost model

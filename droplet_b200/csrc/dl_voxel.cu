@@ -44,7 +44,37 @@ struct dl_vox_result {
     double bmin[3], bmax[3], dims[3];
     std::vector<uint32_t> idx, lo, hi;
     std::vector<float> log_feat, log_cost;         // per evaluated block, with log_blocks
+    double stage_ms[6] = {0, 0, 0, 0, 0, 0};       // with DL_VOX_PROFILE: prep, binning, sort, heads, eval, compact
 };
+
+namespace {
+// Device-time marks of a profiled voxelize call: each interval between two
+// marks is charged to the stage of the mark that ends it.
+struct VoxMarks {
+    bool on = false;
+    cudaStream_t st = nullptr;
+    std::vector<std::pair<int, cudaEvent_t>> ev;
+    void mark(int stage) {
+        if (!on) return;
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        cudaEventRecord(e, st);
+        ev.emplace_back(stage, e);
+    }
+    void finish(double* ms) {
+        if (on && !ev.empty()) {
+            cudaEventSynchronize(ev.back().second);
+            for (size_t i = 1; i < ev.size(); i++) {
+                float t = 0.0f;
+                if (cudaEventElapsedTime(&t, ev[i - 1].second, ev[i].second) == cudaSuccess) ms[ev[i].first] += t;
+            }
+        }
+        for (auto& e : ev) cudaEventDestroy(e.second);
+        ev.clear();
+    }
+    ~VoxMarks() { for (auto& e : ev) cudaEventDestroy(e.second); }
+};
+}  // namespace
 
 namespace {
 
@@ -761,6 +791,10 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     VoxBufs& B = *dev->vox;
     const bool logBlocks = opts && opts->log_blocks;
     const bool fastExp = opts && (opts->flags & DL_VOX_FAST_EXP);
+    VoxMarks marks;
+    marks.on = opts && (opts->flags & DL_VOX_PROFILE);
+    marks.st = st;
+    marks.mark(0);
     const double blockSize = 4 * voxelRes;
     VoxParams p;
     std::memset(&p, 0, sizeof(p));
@@ -915,6 +949,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             return fail(DL_E_CUDA);
         }
     }
+    marks.mark(0);
     // A slab is a box of batches contiguous in batch order: whole z rows, or
     // whole y rows of one z row, or a range of batches of one (z, y) row.
     struct Slab { int64_t z0, z1, y0, y1, x0, x1; unsigned long long pairs; };
@@ -1012,6 +1047,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         ea.counter = scr + VS_EMIT; ea.err = scr + VS_ERR; ea.ovf = scr + VS_OVF;
         ea.spin_limit = g_dl_wait.spin_limit;
         vox_emit_k<<<emitTiles, kVT, 0, st>>>(ea);
+        marks.mark(1);
         unsigned long long npairs = 0;
         {
             uint32_t h[16];
@@ -1063,6 +1099,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             keysF = kin;
             valsF = vin;
         }
+        marks.mark(2);
         // ---- blocks, evaluation, compaction
         const uint64_t maxBlocks = std::max<unsigned long long>(npairs, 1);
         if ((s = B.bkey.ensure(4 * maxBlocks)) != DL_OK || (s = B.bstart.ensure(4 * (maxBlocks + 1))) != DL_OK ||
@@ -1099,6 +1136,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
                 work = sa.work;
             }
         }
+        marks.mark(3);
         EvalArgs va;
         va.p = p; va.rec = B.rec.as<VoxRec>(); va.vals = valsF; va.bkey = B.bkey.as<uint32_t>();
         va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
@@ -1107,6 +1145,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         if (fastExp) vox_eval_k<true><<<dev->sm_count * 32, 64, 0, st>>>(va);
         else vox_eval_k<false><<<dev->sm_count * 32, 64, 0, st>>>(va);
 
+        marks.mark(4);
         uint32_t hn[2] = {0, 0};
         if (cudaMemcpyAsync(hn, scr + VS_NBLK, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
@@ -1138,6 +1177,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         ca.nout = scr + VS_NOUT; ca.status = B.status.as<unsigned long long>(); ca.counter = scr + VS_COMPACT;
         ca.err = scr + VS_ERR; ca.spin_limit = g_dl_wait.spin_limit;
         vox_compact_k<<<compTiles, kVT, 0, st>>>(ca);
+        marks.mark(5);
         uint32_t h2[16];
         if (cudaMemcpyAsync(h2, scr, 64, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
             dl_set_error(std::string("voxelize compact: ") + cudaGetErrorString(cudaGetLastError()));
@@ -1156,7 +1196,14 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             }
         }
     }
+    marks.finish(R->stage_ms);
     *out = R;
+    return DL_OK;
+}
+
+extern "C" int dl_vox_result_stage_times(const dl_vox_result* r, double* ms, int n) {
+    if (!r || !ms) { dl_set_error("dl_vox_result_stage_times: NULL argument"); return DL_E_INVALID_ARG; }
+    for (int i = 0; i < n && i < 6; i++) ms[i] = r->stage_ms[i];
     return DL_OK;
 }
 
