@@ -1320,7 +1320,9 @@ constexpr int kPairFloats = 20;
 
 // Composites the n staged splats of a warp's packed pair buffer sp (layout
 // above) at the lane's pixel, two splats per step, in staging order; sets done
-// once T < 1e-4 (the shader's early out) and stops there.
+// once T < 1e-4 (the shader's early out) and stops there.  Skipped splats go
+// through the blend with alpha 0 (no branch): fma(T, 0, T) = T and
+// fma(T * 0, -colour, c) = c for a finite colour.
 __device__ __forceinline__ void composite_x2(const float* sp, uint32_t n, float2 px2, float2 py2, float& c0,
                                              float& c1, float& c2, float& T, bool& done) {
     const float2 nfloor2 = make_float2(-DL_GAUSS_FLOOR, -DL_GAUSS_FLOOR);
@@ -1340,25 +1342,24 @@ __device__ __forceinline__ void composite_x2(const float* sp, uint32_t n, float2
         // the shader's skips: power > 0, alpha < 1/255
         const bool ok0 = !(pw.x > 0.0f) && !(na.x > -DL_MIN_ALPHA);
         const bool ok1 = !(pw.y > 0.0f) && !(na.y > -DL_MIN_ALPHA);
-        if (ok0 || ok1) {
-            const float4 q3 = P[3];
-            if (ok0) {
-                const float w = T * na.x;
-                c0 = __fmaf_rn(w, q3.x, c0);
-                c1 = __fmaf_rn(w, q3.y, c1);
-                c2 = __fmaf_rn(w, q3.z, c2);
-                T = __fmaf_rn(T, na.x, T);
-                if (T < DL_MIN_T) { done = true; return; }
-            }
-            if (ok1) {
-                const float4 q4 = P[4];
-                const float w = T * na.y;
-                c0 = __fmaf_rn(w, q3.w, c0);
-                c1 = __fmaf_rn(w, q4.x, c1);
-                c2 = __fmaf_rn(w, q4.y, c2);
-                T = __fmaf_rn(T, na.y, T);
-                if (T < DL_MIN_T) { done = true; return; }
-            }
+        {
+            // branch-free: a skipped splat composites with alpha 0, which leaves
+            // c and T exactly as they are (the colours are finite: put_pair_slot)
+            const float4 q3 = P[3], q4 = P[4];
+            const float a0 = ok0 ? na.x : 0.0f;
+            float w = T * a0;
+            c0 = __fmaf_rn(w, q3.x, c0);
+            c1 = __fmaf_rn(w, q3.y, c1);
+            c2 = __fmaf_rn(w, q3.z, c2);
+            T = __fmaf_rn(T, a0, T);
+            if (T < DL_MIN_T) { done = true; return; }
+            const float a1 = ok1 ? na.y : 0.0f;
+            w = T * a1;
+            c0 = __fmaf_rn(w, q3.w, c0);
+            c1 = __fmaf_rn(w, q4.x, c1);
+            c2 = __fmaf_rn(w, q4.y, c2);
+            T = __fmaf_rn(T, a1, T);
+            if (T < DL_MIN_T) { done = true; return; }
         }
     }
 }
@@ -1374,9 +1375,12 @@ __device__ __forceinline__ void put_pair_slot(float* sp, uint32_t slot, float x,
     P[6 + c] = -1.4426950408889634f * B;
     P[8 + c] = -0.72134752044448170f * C;
     P[10 + c] = -al;
-    P[12 + 3 * c] = -cr;
-    P[13 + 3 * c] = -cg;
-    P[14 + 3 * c] = -cb;
+    // colours are >= 0 (project.ts clamps at 0, no upper clamp); an infinite
+    // one is held as FLT_MAX, so that alpha 0 times it is 0 and a composited
+    // one still saturates its channel: the final bytes are the same
+    P[12 + 3 * c] = -fminf(cr, 3.402823466e38f);
+    P[13 + 3 * c] = -fminf(cg, 3.402823466e38f);
+    P[14 + 3 * c] = -fminf(cb, 3.402823466e38f);
 }
 
 // An odd count: a splat of opacity 0 fills the last pair (alpha 0 is skipped).
