@@ -453,9 +453,9 @@ def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> Vo
             check(L.dl_vox_result_copy(h, idx.ctypes.data, lo.ctypes.data, hi.ctypes.data))
         stages = None
         if opts.get("profile"):
-            ms = (ctypes.c_double * 6)()
-            check(L.dl_vox_result_stage_times(h, ms, 6))
-            stages = dict(zip(("prep", "binning", "sort", "heads", "eval", "compact"), list(ms)))
+            ms = (ctypes.c_double * 7)()
+            check(L.dl_vox_result_stage_times(h, ms, 7))
+            stages = dict(zip(("prep", "binning", "sort", "heads", "eval", "compact", "host"), list(ms)))
         log = None
         if o.log_blocks:
             m = ctypes.c_uint64()

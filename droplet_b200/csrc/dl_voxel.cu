@@ -44,7 +44,8 @@ struct dl_vox_result {
     double bmin[3], bmax[3], dims[3];
     std::vector<uint32_t> idx, lo, hi;
     std::vector<float> log_feat, log_cost;         // per evaluated block, with log_blocks
-    double stage_ms[6] = {0, 0, 0, 0, 0, 0};       // with DL_VOX_PROFILE: prep, binning, sort, heads, eval, compact
+    // with DL_VOX_PROFILE: prep, binning, sort, heads, eval, compact, host (slab set-up and result copies)
+    double stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -80,34 +81,46 @@ namespace {
 
 constexpr unsigned long long kAgg = 1ull << 62, kPre = 2ull << 62, kMask = (1ull << 62) - 1;
 
-// Decoupled look-back over CTAs of one chain; called by a single thread.  At
-// most spin_limit polls of an unpublished predecessor, then DL_DEVERR_TIMEOUT
-// and the prefix summed so far (the CTA's writes stay inside the chain).
-__device__ unsigned long long lookback(unsigned long long* status, uint32_t tile, unsigned long long total,
-                                       uint32_t* err, uint32_t spin_limit) {
+// Decoupled look-back over the CTAs of one chain, by one whole warp: each step
+// reads the 32 nearest predecessors not yet added (lane l reads tile q - l),
+// adds the aggregates before the first unpublished one, and stops at the
+// first inclusive prefix.  At most spin_limit polls of an unpublished
+// predecessor, then DL_DEVERR_TIMEOUT and the prefix summed so far (the CTA's
+// writes stay inside the chain).  No fence: a status word carries its own
+// value and no other data passes between CTAs.  Returns the exclusive prefix
+// to every lane.
+__device__ unsigned long long lookback_warp(unsigned long long* status, uint32_t tile, unsigned long long total,
+                                            uint32_t* err, uint32_t spin_limit) {
+    const int lane = threadIdx.x & 31;
     if (tile == 0) {
-        dl_st_volatile64(&status[0], kPre | total);
+        if (lane == 0) dl_st_volatile64(&status[0], kPre | total);
         return 0ull;
     }
-    __threadfence();
-    dl_st_volatile64(&status[tile], kAgg | total);
+    if (lane == 0) dl_st_volatile64(&status[tile], kAgg | total);
     unsigned long long excl = 0;
     int64_t q = (int64_t)tile - 1;
     uint32_t spins = 0;
-    while (q >= 0) {
-        const unsigned long long s = dl_ld_volatile64(&status[q]);
-        const unsigned long long f = s & ~kMask;
-        if (f == 0ull) {
-            if (++spins > spin_limit) { atomicOr(err, DL_DEVERR_TIMEOUT); break; }
+    while (true) {
+        // tile 0 always publishes an inclusive prefix, so a walk never passes it
+        const unsigned long long w = (q - lane >= 0) ? dl_ld_volatile64(&status[q - lane]) : kPre;
+        const unsigned long long f = w & ~kMask;
+        const uint32_t notReady = __ballot_sync(0xffffffffu, f == 0ull);
+        const uint32_t prefix = __ballot_sync(0xffffffffu, f == kPre);
+        const int firstNR = notReady ? __ffs(notReady) - 1 : 32;
+        const int firstP = prefix ? __ffs(prefix) - 1 : 32;
+        const int take = firstP < firstNR ? firstP + 1 : firstNR;
+        unsigned long long add = lane < take ? (w & kMask) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) add += __shfl_xor_sync(0xffffffffu, add, o);
+        excl += add;
+        if (firstP < firstNR) break;
+        q -= take;
+        if (take == 0) {
+            if (++spins > spin_limit) { if (lane == 0) atomicOr(err, DL_DEVERR_TIMEOUT); break; }
             __nanosleep(32);
-            continue;
         }
-        excl += s & kMask;
-        if (f == kPre) break;
-        q--;
     }
-    __threadfence();
-    dl_st_volatile64(&status[tile], kPre | ((excl + total) & kMask));
+    if (lane == 0) dl_st_volatile64(&status[tile], kPre | ((excl + total) & kMask));
     return excl;
 }
 
@@ -360,14 +373,16 @@ __global__ void __launch_bounds__(kVT) vox_emit_k(VoxEmitArgs a) {
     uint32_t run = wpre + inc - local;
 #pragma unroll
     for (int j = 0; j < kVI; j++) { s_excl[tid * kVI + j] = run; run += cnt[j]; }
-    if (tid == 0) {
-        s_excl[kVR] = total;
-        const unsigned long long pre = lookback(a.status, tile, total, a.err, a.spin_limit);
-        s_pre = pre;
-        if (g0 + kVR >= a.p.n) *a.npairs = pre + total;
-        const bool over = pre + total > a.cap;
-        if (over) atomicOr(a.ovf, DL_DEVERR_OVERFLOW);
-        s_skip = over;
+    if (warp == 0) {
+        const unsigned long long pre = lookback_warp(a.status, tile, total, a.err, a.spin_limit);
+        if (lane == 0) {
+            s_excl[kVR] = total;
+            s_pre = pre;
+            if (g0 + kVR >= a.p.n) *a.npairs = pre + total;
+            const bool over = pre + total > a.cap;
+            if (over) atomicOr(a.ovf, DL_DEVERR_OVERFLOW);
+            s_skip = over;
+        }
     }
     __syncthreads();
     if (s_skip) return;
@@ -407,6 +422,8 @@ struct HeadsArgs {
     uint32_t spin_limit;
 };
 
+constexpr int kHI = 16, kHR = kVT * kHI;      // sorted keys per thread / per CTA of the heads kernel
+
 __global__ void __launch_bounds__(kVT) vox_heads_k(HeadsArgs a) {
     __shared__ uint32_t s_wsum[kVT / 32];
     __shared__ uint32_t s_tile;
@@ -421,42 +438,44 @@ __global__ void __launch_bounds__(kVT) vox_heads_k(HeadsArgs a) {
     __syncthreads();
     const uint32_t tile = s_tile;
     const unsigned long long n = *a.npairs;
-    const unsigned long long i0 = (unsigned long long)tile * kVR;
+    const unsigned long long i0 = (unsigned long long)tile * kHR;
     if (i0 >= n) {
         if (tile == 0 && tid == 0) { *a.nblocks = 0; a.bstart[0] = 0; }
         return;
     }
-    uint32_t head[kVI], local = 0;
+    // warp-striped: warp w reads keys [i0 + 512 w, i0 + 512 (w + 1)), 32 at a time
+    const uint32_t lmask = dl_lanemask_lt();
+    const unsigned long long wb = i0 + (unsigned long long)warp * 32 * kHI;
+    uint32_t hm[kHI], key[kHI], wcount = 0;
 #pragma unroll
-    for (int j = 0; j < kVI; j++) {
-        const unsigned long long i = i0 + tid * kVI + j;
-        head[j] = (i < n && (i == 0 || a.keys[i] != a.keys[i - 1])) ? 1u : 0u;
-        local += head[j];
+    for (int j = 0; j < kHI; j++) {
+        const unsigned long long i = wb + (unsigned long long)j * 32 + lane;
+        key[j] = i < n ? a.keys[i] : 0u;
+        const bool head = i < n && (i == 0 || key[j] != a.keys[i - 1]);
+        hm[j] = __ballot_sync(0xffffffffu, head);
+        wcount += __popc(hm[j]);
     }
-    uint32_t inc = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
-    }
-    if (lane == 31) s_wsum[warp] = inc;
+    if (lane == 0) s_wsum[warp] = wcount;
     __syncthreads();
     uint32_t wpre = 0, total = 0;
     for (int w = 0; w < kVT / 32; w++) { if (w < warp) wpre += s_wsum[w]; total += s_wsum[w]; }
-    if (tid == 0) {
-        s_pre = lookback(a.status, tile, total, a.err, a.spin_limit);
-        if (i0 + kVR >= n) { *a.nblocks = (uint32_t)(s_pre + total); a.bstart[s_pre + total] = (uint32_t)n; }
+    if (warp == 0) {
+        const unsigned long long pre = lookback_warp(a.status, tile, total, a.err, a.spin_limit);
+        if (lane == 0) {
+            s_pre = pre;
+            if (i0 + kHR >= n) { *a.nblocks = (uint32_t)(pre + total); a.bstart[pre + total] = (uint32_t)n; }
+        }
     }
     __syncthreads();
-    uint32_t run = (uint32_t)s_pre + wpre + inc - local;
+    uint32_t run = (uint32_t)s_pre + wpre;
 #pragma unroll
-    for (int j = 0; j < kVI; j++) {
-        if (head[j]) {
-            const unsigned long long i = i0 + tid * kVI + j;
-            a.bkey[run] = a.keys[i];
-            a.bstart[run] = (uint32_t)i;
-            run++;
+    for (int j = 0; j < kHI; j++) {
+        if ((hm[j] >> lane) & 1u) {
+            const uint32_t pos = run + __popc(hm[j] & lmask);
+            a.bkey[pos] = key[j];
+            a.bstart[pos] = (uint32_t)(wb + (unsigned long long)j * 32 + lane);
         }
+        run += __popc(hm[j]);
     }
 }
 
@@ -715,9 +734,12 @@ __global__ void __launch_bounds__(kVT) vox_compact_k(CompactArgs a) {
     __syncthreads();
     uint32_t wpre = 0, total = 0;
     for (int w = 0; w < kVT / 32; w++) { if (w < warp) wpre += s_wsum[w]; total += s_wsum[w]; }
-    if (tid == 0) {
-        s_pre = lookback(a.status, tile, total, a.err, a.spin_limit);
-        if (i0 + kVR >= n) *a.nout = (uint32_t)(s_pre + total);
+    if (warp == 0) {
+        const unsigned long long pre = lookback_warp(a.status, tile, total, a.err, a.spin_limit);
+        if (lane == 0) {
+            s_pre = pre;
+            if (i0 + kVR >= n) *a.nout = (uint32_t)(pre + total);
+        }
     }
     __syncthreads();
     uint32_t run = (uint32_t)s_pre + wpre + inc - local;
@@ -1029,6 +1051,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     for (const Slab& slab : slabs) {
         const unsigned long long cap = slab.pairs;
         if (cap == 0) continue;
+        marks.mark(6);
         p.zlo = slab.z0 * 16;
         p.zhi = std::min<int64_t>(slab.z1 * 16, p.NB[2]) - 1;
         p.ylo = slab.y0 * 16;
@@ -1105,7 +1128,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         if ((s = B.bkey.ensure(4 * maxBlocks)) != DL_OK || (s = B.bstart.ensure(4 * (maxBlocks + 1))) != DL_OK ||
             (s = B.masks.ensure(8 * maxBlocks)) != DL_OK)
             return fail(s);
-        const uint32_t headTiles = (uint32_t)std::max<unsigned long long>(1, (npairs + kVR - 1) / kVR);
+        const uint32_t headTiles = (uint32_t)std::max<unsigned long long>(1, (npairs + kHR - 1) / kHR);
         cudaMemsetAsync(B.status.p, 0, 8ull * headTiles, st);
         HeadsArgs ha;
         ha.keys = keysF; ha.npairs = (const unsigned long long*)(scr + 14); ha.bkey = B.bkey.as<uint32_t>();
@@ -1196,6 +1219,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
             }
         }
     }
+    marks.mark(6);
     marks.finish(R->stage_ms);
     *out = R;
     return DL_OK;
@@ -1203,7 +1227,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
 
 extern "C" int dl_vox_result_stage_times(const dl_vox_result* r, double* ms, int n) {
     if (!r || !ms) { dl_set_error("dl_vox_result_stage_times: NULL argument"); return DL_E_INVALID_ARG; }
-    for (int i = 0; i < n && i < 6; i++) ms[i] = r->stage_ms[i];
+    for (int i = 0; i < n && i < 7; i++) ms[i] = r->stage_ms[i];
     return DL_OK;
 }
 

@@ -98,8 +98,8 @@ typedef struct dl_vox_opts {
     uint32_t flags;
 } dl_vox_opts;
 #define DL_VOX_FAST_EXP 1u
-/* DL_VOX_PROFILE: record the device time of the call's stages (prep, binning,
- * sort, block heads, evaluation, compaction), read by dl_vox_result_stage_times */
+/* DL_VOX_PROFILE: record the device time of the call's stages, read by
+ * dl_vox_result_stage_times */
 #define DL_VOX_PROFILE 2u
 
 /* ---- errors ------------------------------------------------------------ */
@@ -268,7 +268,8 @@ int dl_device_set_voxel_scheduler(dl_device* dev, dl_mlp* mlp);
 int dl_vox_result_block_log(const dl_vox_result* res, float* features, float* cost, uint64_t cap, uint64_t* n);
 /* Device ms per stage of a call made with DL_VOX_PROFILE (no reference
  * counterpart): prep (upload, extents, bounds, batch counts), binning, sort,
- * block heads (and the learned order), evaluation, compaction with read-back. */
+ * block heads (and the learned order), evaluation, compaction, and the time
+ * the device waits for the host between slabs (set-up, result copies). */
 int dl_vox_result_stage_times(const dl_vox_result* res, double* ms, int n);
 
 /* ---- src/io/ply.ts:120-239 loadPlySplats --------------------------------
