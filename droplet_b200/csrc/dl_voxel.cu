@@ -32,6 +32,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -40,9 +43,45 @@
 #include "dl_mlp.cuh"
 #include "dl_sort.cuh"
 
+// Page-locked host memory for the block lists of a call on their way back
+// from the device.  A result handle keeps the buffer until dl_vox_result_free,
+// which hands it back for the device's next call (or frees it when the pool
+// already holds one); so block lists come back at full PCIe rate without
+// pinning memory on every call.
+struct PinnedPool {
+    std::mutex m;
+    void* p = nullptr;
+    size_t cap = 0;
+    ~PinnedPool() { if (p) cudaFreeHost(p); }
+    void take(void** q, size_t* c) {
+        std::lock_guard<std::mutex> g(m);
+        *q = p; *c = cap; p = nullptr; cap = 0;
+    }
+    void give(void* q, size_t c) {
+        if (!q) return;
+        std::lock_guard<std::mutex> g(m);
+        if (p && cap >= c) { cudaFreeHost(q); return; }
+        if (p) cudaFreeHost(p);
+        p = q; cap = c;
+    }
+};
+
 struct dl_vox_result {
     double bmin[3], bmax[3], dims[3];
-    std::vector<uint32_t> idx, lo, hi;
+    std::vector<uint32_t> idx, lo, hi;             // block lists built on the host (cutoff <= 0)
+    // block lists read back from the device: per slab, count entries of idx, lo
+    // and hi one after the other in the pinned buffer, from word offset off
+    std::shared_ptr<PinnedPool> pool;
+    uint32_t* pinned = nullptr;
+    size_t pinned_cap = 0;                         // bytes
+    uint64_t pinned_used = 0;                      // u32 words
+    uint64_t pinned_count = 0;                     // blocks
+    std::vector<std::pair<uint64_t, uint32_t>> segs;
+    ~dl_vox_result() {
+        if (!pinned) return;
+        if (pool) pool->give(pinned, pinned_cap);
+        else cudaFreeHost(pinned);
+    }
     std::vector<float> log_feat, log_cost;         // per evaluated block, with log_blocks
     // with DL_VOX_PROFILE: prep, binning, sort, heads, eval, compact, host (slab set-up and result copies)
     double stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -770,6 +809,7 @@ double js_round(double x) {
 
 // The voxelizer's grow-only device buffers, kept on the device between calls.
 struct VoxBufs {
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     std::vector<DevBuf*> all;
     DevBuf scene, ext, rec, part, bounds, axes, scratch, keys0, keys1, vals0, vals1, status, hist, segs, bkey, bstart,
         masks, oidx, olo, ohi, used, bcount, sfeat, sbucket, shist, swork, scycles;
@@ -825,7 +865,14 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
     p.half = p.res * 0.5f;
     p.cutoff = (float)cutoffD;
     p.blockSize = blockSize;
-    auto fail = [&](int code) { delete R; return code; };
+    // (a failed call waits for copies still in flight into R's buffer first)
+    auto fail = [&](int code) { cudaStreamSynchronize(st); delete R; return code; };
+    R->pool = B.pinned;
+    {
+        void* q = nullptr;
+        B.pinned->take(&q, &R->pinned_cap);
+        R->pinned = static_cast<uint32_t*>(q);
+    }
 
     // ---- upload + per-Gaussian prep + bounds
     const uint64_t oRot = (12 * n + 255) / 256 * 256, oLsc = oRot + (16 * n + 255) / 256 * 256;
@@ -1208,18 +1255,44 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         }
         if (h2[VS_ERR] & DL_DEVERR_TIMEOUT) { dl_set_error("a bounded device-side wait timed out"); return fail(DL_E_TIMEOUT); }
         const uint32_t nout = h2[VS_NOUT];
-        const size_t o0 = R->idx.size();
-        R->idx.resize(o0 + nout); R->lo.resize(o0 + nout); R->hi.resize(o0 + nout);
         if (nout) {
-            if (cudaMemcpy(R->idx.data() + o0, B.oidx.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                cudaMemcpy(R->lo.data() + o0, B.olo.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                cudaMemcpy(R->hi.data() + o0, B.ohi.p, 4ull * nout, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            // this slab's lists go to the pinned buffer behind the earlier
+            // slabs' (asynchronously: the next slab's kernels queue behind the
+            // copies on the same stream, so B.oidx/olo/ohi are not overwritten early)
+            const uint64_t need = 4ull * (R->pinned_used + 3ull * nout);
+            if (need > R->pinned_cap) {
+                if (cudaStreamSynchronize(st) != cudaSuccess) {
+                    dl_set_error(std::string("voxelize: ") + cudaGetErrorString(cudaGetLastError()));
+                    return fail(DL_E_CUDA);
+                }
+                const size_t nc = std::max<size_t>(need + need / 2, 16u << 20);
+                void* q = nullptr;
+                if (cudaHostAlloc(&q, nc, cudaHostAllocDefault) != cudaSuccess) {
+                    dl_set_error("voxelize: cudaHostAlloc(" + std::to_string(nc) + ") for the block lists failed");
+                    return fail(DL_E_OOM);
+                }
+                if (R->pinned_used) std::memcpy(q, R->pinned, 4ull * R->pinned_used);
+                if (R->pinned) cudaFreeHost(R->pinned);
+                R->pinned = static_cast<uint32_t*>(q);
+                R->pinned_cap = nc;
+            }
+            uint32_t* dst = R->pinned + R->pinned_used;
+            if (cudaMemcpyAsync(dst, B.oidx.p, 4ull * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaMemcpyAsync(dst + nout, B.olo.p, 4ull * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaMemcpyAsync(dst + 2ull * nout, B.ohi.p, 4ull * nout, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
                 dl_set_error("voxelize: result copy failed");
                 return fail(DL_E_CUDA);
             }
+            R->segs.emplace_back(R->pinned_used, nout);
+            R->pinned_used += 3ull * nout;
+            R->pinned_count += nout;
         }
     }
     marks.mark(6);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        dl_set_error(std::string("voxelize: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(DL_E_CUDA);
+    }
     marks.finish(R->stage_ms);
     *out = R;
     return DL_OK;
@@ -1239,7 +1312,7 @@ extern "C" int dl_vox_result_info(const dl_vox_result* r, double bmin[3], double
         if (bmax) bmax[k] = r->bmax[k];
         if (dims) dims[k] = r->dims[k];
     }
-    if (count) *count = r->idx.size();
+    if (count) *count = r->idx.size() + r->pinned_count;
     return DL_OK;
 }
 
@@ -1249,6 +1322,25 @@ extern "C" int dl_vox_result_copy(const dl_vox_result* r, uint32_t* idx, uint32_
     if (n && idx) std::memcpy(idx, r->idx.data(), 4 * n);
     if (n && lo) std::memcpy(lo, r->lo.data(), 4 * n);
     if (n && hi) std::memcpy(hi, r->hi.data(), 4 * n);
+    if (!r->pinned_count) return DL_OK;
+    // the device's lists, slab by slab after the host-built ones; the three
+    // arrays are gathered by three threads when they are large
+    auto gather = [r, n](uint32_t* dst, int which) {
+        if (!dst) return;
+        uint64_t o = n;
+        for (const auto& sg : r->segs) {
+            std::memcpy(dst + o, r->pinned + sg.first + (uint64_t)which * sg.second, 4ull * sg.second);
+            o += sg.second;
+        }
+    };
+    if (r->pinned_count < (1u << 20)) {
+        gather(idx, 0); gather(lo, 1); gather(hi, 2);
+    } else {
+        std::thread t1(gather, lo, 1), t2(gather, hi, 2);
+        gather(idx, 0);
+        t1.join();
+        t2.join();
+    }
     return DL_OK;
 }
 
