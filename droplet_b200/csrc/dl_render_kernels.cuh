@@ -80,6 +80,21 @@ __device__ __forceinline__ float sh_coef(const DlSceneDev& sc, uint64_t i) {
     return __ldg(sc.sh + i);
 }
 
+// Division and square root of the projection: correctly rounded, as the
+// shader's f32 operations (bit-exact with the oracle), or in the +-1 LSB
+// arithmetic of DL_BATCH_FAST_EXP frames (kFast) the hardware approximations
+// (relative error about 2^-22: far inside the margins of every integer
+// decision they feed, which are pixels or 0.2% of a box).
+template <bool kFast>
+__device__ __forceinline__ float pdiv(float a, float b) { return kFast ? __fdividef(a, b) : a / b; }
+template <bool kFast>
+__device__ __forceinline__ float psqrt(float x) {
+    if (!kFast) return sqrtf(x);
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // acc + b * c: the shader's separate multiply and add, or (kFma, the +-1 LSB
 // arithmetic of DL_BATCH_FAST_EXP frames) one fused multiply-add
 template <bool kFma>
@@ -202,9 +217,9 @@ __device__ __forceinline__ void splat_colour(const DlSceneDev& sc, uint32_t g, i
                                              float pcy, float pcz, float& c0, float& c1, float& c2) {
     float col0 = dc[0], col1 = dc[1], col2 = dc[2];
     if (sc.bands > 0) {
-        const float len = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
+        const float len = psqrt<kFma>((pcx * pcx + pcy * pcy) + pcz * pcz);
         float sr, sg, sb;
-        const float dxn = pcx / len, dyn = pcy / len, dzn = pcz / len;
+        const float dxn = pdiv<kFma>(pcx, len), dyn = pdiv<kFma>(pcy, len), dzn = pdiv<kFma>(pcz, len);
         if (sc.sh16) {
             if (sc.bands == 1) eval_sh16<1, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
             else if (sc.bands == 2) eval_sh16<2, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
@@ -301,8 +316,8 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         bool culled = false;
         if (u.projection == 0) {
             culled = depth <= u.near_f || depth >= u.far_f;
-            screenX = (pcx * u.focal) / -pcz + u.cx;
-            screenY = (-pcy * u.focal) / -pcz + u.cy;
+            screenX = pdiv<kFma>(pcx * u.focal, -pcz) + u.cx;
+            screenY = pdiv<kFma>(-pcy * u.focal, -pcz) + u.cy;
         } else {
             const float r = sqrtf((pcx * pcx + pcy * pcy) + pcz * pcz);
             culled = r <= u.near_f;
@@ -332,7 +347,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             const float cc12 = (a10 * v20 + a11 * v21) + a12 * v22;
             const float cc22 = (a20 * v20 + a21 * v21) + a22 * v22;
             // EWA Jacobian as written (project.ts:128-149)
-            const float invZ = 1.0f / pcz;
+            const float invZ = pdiv<kFma>(1.0f, pcz);
             const float j00 = u.focal * invZ;
             const float j02 = ((-u.focal * pcx) * invZ) * invZ;
             const float j11 = u.focal * invZ;
@@ -349,7 +364,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             const float c00 = c00o + DL_AA_DILATION;
             const float c11 = c11o + DL_AA_DILATION;
             const float det = c00 * c11 - c01 * c01;
-            aaFactor = sqrtf(fmaxf(detOrig / det, 0.0f));
+            aaFactor = psqrt<kFma>(fmaxf(pdiv<kFma>(detOrig, det), 0.0f));
             if (det <= 1.0e-6f) {
                 culled = true;
             } else if (a.f64_degenerate && det < kDegenerateRel * (c00 * c11)) {
@@ -363,19 +378,19 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
                 conicC = (float)((double)c00 / d64);
                 aaFactor = (float)sqrt(fmax(o64 / d64, 0.0));
             } else {
-                const float invDet = 1.0f / det;
+                const float invDet = pdiv<kFma>(1.0f, det);
                 conicA = c11 * invDet;
                 conicB = -c01 * invDet;
                 conicC = c00 * invDet;
             }
             if (!culled) {
                 const float mid = 0.5f * (c00 + c11);
-                const float radiusEig = sqrtf(fmaxf(0.1f, mid * mid - det));
+                const float radiusEig = psqrt<kFma>(fmaxf(0.1f, mid * mid - det));
                 const float lambda1 = mid + radiusEig;
-                const float radiusRaw = DL_SIGMA_CUTOFF * sqrtf(lambda1);
+                const float radiusRaw = DL_SIGMA_CUTOFF * psqrt<kFma>(lambda1);
                 const float fadeStart = DL_FADE_START_FRAC * u.height;
                 const float fadeEnd = DL_FADE_END_FRAC * u.height;
-                radiusFade = fminf(fmaxf((fadeEnd - radiusRaw) / (fadeEnd - fadeStart), 0.0f), 1.0f);
+                radiusFade = fminf(fmaxf(pdiv<kFma>(fadeEnd - radiusRaw, fadeEnd - fadeStart), 0.0f), 1.0f);
                 if (radiusFade <= 0.0f) culled = true;
                 else radius = ceilf(fminf(radiusRaw, fadeEnd));
             }
@@ -422,10 +437,11 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             }
             const float ac = cA * cC, dt = ac - cB * cB;
             if (dt > 0.0f && ac <= 1024.0f * dt) {
-                const float qa = -2.0f * logf(DL_GAUSS_FLOOR + DL_MIN_ALPHA / alSt);
+                const float lx = DL_GAUSS_FLOOR + pdiv<kFma>(DL_MIN_ALPHA, alSt);
+                const float qa = -2.0f * (kFma ? __logf(lx) : logf(lx));
                 const float level = fmaxf(0.0f, fminf(9.5f, 1.002f * qa + 0.01f));
-                const float s = level / dt;
-                const float ex = fminf(radius, sqrtf(cC * s)), ey = fminf(radius, sqrtf(cA * s));
+                const float s = pdiv<kFma>(level, dt);
+                const float ex = fminf(radius, psqrt<kFma>(cC * s)), ey = fminf(radius, psqrt<kFma>(cA * s));
                 boxX = ex;
                 boxY = ey;
                 minTX = dl_sat_u32(fmaxf(0.0f, floorf((screenX - ex) / 16.0f)));
