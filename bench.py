@@ -425,6 +425,7 @@ def run_ours(args, rank, world, local_rank):
         hptrs = [h.data_ptr() for h in houts]
         r2 = dl.Renderer(dev)
         r2.set_stream(stream.cuda_stream)
+        r2.set_tuning(**r.get_tuning())            # the knobs the autotuner picked for this batch
         many = lambda: r2.render_many(hdata, cams, flags=FAST | _lib.DL_BATCH_SH16, outs=hptrs)
         many()
         half = max(1, args.steps // 2)

@@ -194,7 +194,7 @@ class Renderer:
 
     BIN_TILES = ("16x16", "8x8", "32x8")
 
-    def set_tuning(self, pair_sort_bits: int = 8, raster_shape: str = "8x4", raster_ctas_per_sm: int = 0,
+    def set_tuning(self, pair_sort_bits: int = 8, raster_shape: str = "tile-f32x2", raster_ctas_per_sm: int = 0,
                    bin_tile: str = "16x16"):
         """Timing-only knobs of rendered frames (dl_tuning); no knob changes a pixel."""
         t = _lib.DlTuning(int(pair_sort_bits), self.RASTER_SHAPES.index(raster_shape), int(raster_ctas_per_sm),

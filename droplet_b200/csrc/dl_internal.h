@@ -98,7 +98,9 @@ struct dl_scene {
 // Knobs of a batched frame that change timing only (dl_tuning in the ABI).
 struct DlTuning {
     int pair_bits = 8;        // pair-sort digit width 6..8
-    int shape = 0;            // rasterizer work item: 0 8x4, 1 16x2, 2 4x8, 3 8x8 (two pixels per lane)
+    int shape = 5;            // rasterizer: 0 8x4, 1 16x2, 2 4x8, 3 8x8 (two pixels per lane) warp items,
+                              // 4 8x4 packed, 5 one CTA per tile packed (fast frames; others use 0), 6 one CTA
+                              // per tile in place
     int ctas_per_sm = 0;      // persistent rasterizer CTAs per SM; 0 = occupancy limit
     int bin_tile = 0;         // binning tile: 0 16x16 (the reference's), 1 8x8, 2 32x8
 };

@@ -194,7 +194,7 @@ int dl_render_static(const dl_splats* data, const dl_camera* cam, const float bg
  * row-major prefix of 16x16 tiles, so other frames bin with 16x16 tiles. */
 typedef struct dl_tuning {
     int32_t pair_sort_bits;       /* digit width of the tile-pair sort: 6, 7 or 8 (default 8) */
-    int32_t raster_shape;         /* pixels of one rasterizer work item (one warp): 0 = 8x4, 1 = 16x2, 2 = 4x8,
+    int32_t raster_shape;         /* rasterizer (default 5): pixels of one work item (one warp): 0 = 8x4, 1 = 16x2, 2 = 4x8,
                                      3 = 8x8 with two pixels per lane, 4 = 8x4 taking two splats per step
                                      in packed f32x2 arithmetic, 5 = the same with one CTA per 256-pixel
                                      tile reading the tile's pairs once (4 and 5: DL_BATCH_FAST_EXP frames,
