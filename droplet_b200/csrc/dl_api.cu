@@ -448,6 +448,9 @@ extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera
             if (knob == 3) { if (t.bin_tile == tileC[c]) continue; t.bin_tile = tileC[c]; }
             double ms = 0.0;
             rc = timeOne(t, &ms);
+            // a candidate that cannot render this batch (e.g. finer binning
+            // tiles pushing a view past the pair capacity) is skipped
+            if (rc == DL_E_CAPACITY) { rc = DL_OK; continue; }
             if (rc == DL_OK && ms < curMs) { cur = t; curMs = ms; }
         }
     }

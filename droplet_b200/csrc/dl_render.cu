@@ -874,9 +874,16 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
     const bool useGraph = !(flags & DL_BATCH_NO_GRAPH) && !(flags & DL_BATCH_PLAIN) && V > 1 && !r->profiling &&
                           !overlap && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
 
+    // a frame that cannot fit leaves the capacity where it found it, so the
+    // renderer keeps serving batches that do fit
+    const uint64_t capOnEntry = r->pair_cap_per_view;
     for (int attempt = 0; attempt < 3; attempt++) {
         const uint64_t cap = r->pair_cap_per_view;
-        if (cap >= (1ull << 30)) { dl_set_error("more than 2^30 tile pairs in one view"); return DL_E_CAPACITY; }
+        if (cap >= (1ull << 30)) {
+            r->pair_cap_per_view = capOnEntry;
+            dl_set_error("more than 2^30 tile pairs in one view");
+            return DL_E_CAPACITY;
+        }
         d = frame_dims(hv, V, N, cap, flags, tune);
         DL_TRY(r->pkeys0.ensure(4ull * V * cap));
         DL_TRY(r->pvals0.ensure(4ull * V * cap));
@@ -977,6 +984,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         r->log_tiles = logTiles ? d.totalTiles : 0;
         return DL_OK;
     }
+    r->pair_cap_per_view = capOnEntry;
     dl_set_error("pair buffers overflowed repeatedly");
     return DL_E_CAPACITY;
 }

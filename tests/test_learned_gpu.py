@@ -1,7 +1,7 @@
 """The learned tile-cost model: its hand-written GPU kernels against a float64
 NumPy restatement, and the guarantee that the schedule it produces changes no
 pixel.  Its gain is measured against the logged tile costs (list-scheduling makespan)
-and timed in bench.py (value vs static_value)."""
+and timed in bench.py (learned_value beside the static-order value)."""
 import numpy as np
 import pytest
 
