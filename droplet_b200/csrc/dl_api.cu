@@ -458,6 +458,13 @@ extern "C" int dl_renderer_autotune(dl_renderer* r, dl_scene* s, const dl_camera
     cudaEventDestroy(e1);
     r->tune = cur;
     if (rc != DL_OK) return rc;
+    // a finer binning candidate may have grown the per-view pair capacity far
+    // past what the chosen knobs need, and views then sit further apart in
+    // the pair buffers than they have to; one more frame with the chosen
+    // knobs sizes the capacity for them.
+    DL_TRY(dl_render_batch(r, s, cams, n, bg, outs.data(), fl));
+    const uint64_t need = r->last_max_pairs + r->last_max_pairs / 4 + 4096;
+    if (need < r->pair_cap_per_view) r->pair_cap_per_view = need;
     if (best) {
         best->pair_sort_bits = cur.pair_bits;
         best->raster_shape = cur.shape;

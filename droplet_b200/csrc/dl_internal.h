@@ -130,6 +130,7 @@ struct dl_renderer {
     uint64_t* h_u64 = nullptr;          // pinned scratch
     size_t h_u64_cap = 0;
     uint64_t pair_cap_per_view = 0;
+    uint64_t last_max_pairs = 0;          // largest view's tile pairs in the last frame that fit
 
     // last frame (single view) for debug copies
     uint32_t last_n = 0, last_stride = 0, last_T = 0, last_W = 0, last_H = 0, last_pairs_final = 0;

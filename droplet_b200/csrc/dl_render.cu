@@ -52,8 +52,8 @@ int ensure_pinned(void** p, size_t* cap, size_t need) {
 
 template <int BITS>
 void launch_pass(const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
-    if (p.drop_max) dlsort::pass_k<BITS, true><<<grid, dlsort::kThreads, 0, st>>>(p);
-    else dlsort::pass_k<BITS><<<grid, dlsort::kThreads, 0, st>>>(p);
+    if (p.drop_max) dlsort::pass_k<BITS, true><<<dlsort::pass_grid(grid), dlsort::kThreads, 0, st>>>(p);
+    else dlsort::pass_k<BITS><<<dlsort::pass_grid(grid), dlsort::kThreads, 0, st>>>(p);
 }
 
 void launch_pass_bits(int bits, const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
@@ -972,6 +972,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             r->pair_cap_per_view = maxPairs + maxPairs / 4 + 4096;
             continue;
         }
+        r->last_max_pairs = maxPairs;
         r->last_n = N;
         r->last_stride = (uint32_t)d.stride;
         r->last_T = hv[0].numTiles;

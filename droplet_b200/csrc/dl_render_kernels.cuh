@@ -1330,15 +1330,18 @@ __device__ __forceinline__ void raster_subtile2(const RasterArgs& a, uint32_t v,
 //
 // Shared memory per warp: 32 pairs of staged splats, 20 floats a pair:
 //   {-x0, -x1, -y0, -y1}, {A0, A1, B0, B1}, {C0, C1, -o0, -o1},
-//   {-r0, -g0, -b0, -r1}, {-g1, -b1, 0, 0}
-// (A, B, C: the conic scaled by -0.5 log2 e as in stage_chunk's fast path.)
+//   {-r0, -g0, -r1, -g1}, {-b0, -b1, unused, unused}
+// (A, B, C: the conic scaled by -0.5 log2 e as in stage_chunk's fast path;
+// red and green of a splat side by side, so one f32x2 FMA blends both.)
 constexpr int kPairFloats = 20;
 
 // Composites the n staged splats of a warp's packed pair buffer sp (layout
 // above) at the lane's pixel, two splats per step, in staging order; sets done
 // once T < 1e-4 (the shader's early out) and stops there.  Skipped splats go
 // through the blend with alpha 0 (no branch): fma(T, 0, T) = T and
-// fma(T * 0, -colour, c) = c for a finite colour.
+// fma(T * 0, -colour, c) = c for a finite colour.  The second splat of a step
+// also blends with alpha 0 when the first one ended the pixel, so one test of
+// T per step serves both.
 __device__ __forceinline__ void composite_x2(const float* sp, uint32_t n, float2 px2, float2 py2, float& c0,
                                              float& c1, float& c2, float& T, bool& done) {
     const float2 nfloor2 = make_float2(-DL_GAUSS_FLOOR, -DL_GAUSS_FLOOR);
@@ -1359,22 +1362,20 @@ __device__ __forceinline__ void composite_x2(const float* sp, uint32_t n, float2
         const bool ok0 = !(pw.x > 0.0f) && !(na.x > -DL_MIN_ALPHA);
         const bool ok1 = !(pw.y > 0.0f) && !(na.y > -DL_MIN_ALPHA);
         {
-            // branch-free: a skipped splat composites with alpha 0, which leaves
-            // c and T exactly as they are (the colours are finite: put_pair_slot)
             const float4 q3 = P[3], q4 = P[4];
             const float a0 = ok0 ? na.x : 0.0f;
             float w = T * a0;
-            c0 = __fmaf_rn(w, q3.x, c0);
-            c1 = __fmaf_rn(w, q3.y, c1);
-            c2 = __fmaf_rn(w, q3.z, c2);
+            float2 rg = make_float2(c0, c1);
+            rg = __ffma2_rn(make_float2(w, w), make_float2(q3.x, q3.y), rg);
+            c2 = __fmaf_rn(w, q4.x, c2);
             T = __fmaf_rn(T, a0, T);
-            if (T < DL_MIN_T) { done = true; return; }
-            const float a1 = ok1 ? na.y : 0.0f;
+            const bool d0 = T < DL_MIN_T;
+            const float a1 = (ok1 && !d0) ? na.y : 0.0f;
             w = T * a1;
-            c0 = __fmaf_rn(w, q3.w, c0);
-            c1 = __fmaf_rn(w, q4.x, c1);
+            rg = __ffma2_rn(make_float2(w, w), make_float2(q3.z, q3.w), rg);
             c2 = __fmaf_rn(w, q4.y, c2);
             T = __fmaf_rn(T, a1, T);
+            c0 = rg.x; c1 = rg.y;
             if (T < DL_MIN_T) { done = true; return; }
         }
     }
@@ -1394,16 +1395,16 @@ __device__ __forceinline__ void put_pair_slot(float* sp, uint32_t slot, float x,
     // colours are >= 0 (project.ts clamps at 0, no upper clamp); an infinite
     // one is held as FLT_MAX, so that alpha 0 times it is 0 and a composited
     // one still saturates its channel: the final bytes are the same
-    P[12 + 3 * c] = -fminf(cr, 3.402823466e38f);
-    P[13 + 3 * c] = -fminf(cg, 3.402823466e38f);
-    P[14 + 3 * c] = -fminf(cb, 3.402823466e38f);
+    P[12 + 2 * c] = -fminf(cr, 3.402823466e38f);
+    P[13 + 2 * c] = -fminf(cg, 3.402823466e38f);
+    P[16 + c] = -fminf(cb, 3.402823466e38f);
 }
 
 // An odd count: a splat of opacity 0 fills the last pair (alpha 0 is skipped).
 __device__ __forceinline__ void pad_pair_slot(float* sp, uint32_t n) {
     float* P = sp + (n >> 1) * kPairFloats;
     P[1] = 0.0f; P[3] = 0.0f; P[5] = 0.0f; P[7] = 0.0f; P[9] = 0.0f; P[11] = -0.0f;
-    P[15] = 0.0f; P[16] = 0.0f; P[17] = 0.0f;
+    P[14] = 0.0f; P[15] = 0.0f; P[17] = 0.0f;
 }
 
 __device__ __forceinline__ uint32_t stage_chunk_x2(const RasterArgs& a, const uint32_t* vals, uint32_t b,
@@ -1641,15 +1642,22 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterA
                                 A = ab.x; B = ab.y; C = ca.x; al = ca.y; cr = rg.x; cg = rg.y; cb = bz.x;
                             }
                             if (!a.rec_box) tight_extent(A, B, C, ra.z, ex, ey);
-                            // items: 8x4 pixels, perRow per tile row
-                            for (uint32_t w = 0; w < (uint32_t)kRasterWarps; w++) {
-                                const float ix0 = (float)(ox + (w % perRow) * 8u) + 0.5f - pad;
-                                const float iy0 = (float)(oy + (w / perRow) * 4u) + 0.5f - pad;
-                                const float ix1 = ix0 + 7.0f + 2.0f * pad, iy1 = iy0 + 3.0f + 2.0f * pad;
-                                if (!(ra.x - ex > ix1) && !(ra.x + ex < ix0) && !(ra.y - ey > iy1) &&
-                                    !(ra.y + ey < iy0))
-                                    mask |= 1u << w;
-                            }
+                            // items: 8x4 pixels, perRow per tile row; item column c covers
+                            // pixel centres ox + 8c + 0.5 .. + 7.5, item row r oy + 4r + 0.5 .. + 3.5
+                            const float lx = ra.x - ex - pad - (float)ox, hx = ra.x + ex + pad - (float)ox;
+                            const float ly = ra.y - ey - pad - (float)oy, hy = ra.y + ey + pad - (float)oy;
+                            if (ex == ex && ey == ey) {
+                                const int cA = max(0, (int)ceilf((lx - 7.5f) * 0.125f));
+                                const int cB = min((int)perRow - 1, (int)floorf((hx - 0.5f) * 0.125f));
+                                const int rA = max(0, (int)ceilf((ly - 3.5f) * 0.25f));
+                                const int rB = min(kRasterWarps / (int)perRow - 1, (int)floorf((hy - 0.5f) * 0.25f));
+                                if (cA <= cB && rA <= rB) {
+                                    const uint32_t cm = ((2u << cB) - 1u) & ~((1u << cA) - 1u);
+                                    for (int r = rA; r <= rB; r++) mask |= cm << (r * (int)perRow);
+                                }
+                            } else {
+                                mask = (1u << kRasterWarps) - 1u;   // a NaN extent reaches every item, as
+                            }                                       // the comparisons it fails would say
                             if (mask) {
                                 s_f[0][tid] = ra.x; s_f[1][tid] = ra.y;
                                 s_f[2][tid] = A; s_f[3][tid] = B; s_f[4][tid] = C; s_f[5][tid] = al;
@@ -1742,7 +1750,6 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs
         const uint32_t cols = u.tileW >> 2, rows = u.tileH >> 2;   // 4x4 cells
         const uint32_t ox = tx * u.tileW, oy = ty * u.tileH;
         const uint32_t cx = (warp % perRow) * 2u + (uint32_t)half, cy = warp / perRow;
-        const uint32_t cell = cy * cols + cx;
         const uint32_t x = ox + cx * 4u + (lane & 3), y = oy + cy * 4u + ((lane >> 2) & 3);
         const bool inImage = x < u.W && y < u.H;
         const float px = (float)x + 0.5f, py = (float)y + 0.5f;

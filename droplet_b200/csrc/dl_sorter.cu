@@ -58,7 +58,7 @@ void sort_bits(dl_sorter* s, uint32_t* keys, uint32_t* vals, uint64_t n, int pas
         sp.status = s->status.as<uint32_t>(); sp.counter = meta + kMetaCtr + p; sp.err = meta + kMetaErr;
         sp.shift = BITS * p; sp.pass = p; sp.passes = passes;
         sp.spin_limit = g_dl_wait.spin_limit;
-        dlsort::pass_k<BITS><<<tiles, dlsort::kThreads, 0, st>>>(sp);
+        dlsort::pass_k<BITS><<<dlsort::pass_grid(tiles), dlsort::kThreads, 0, st>>>(sp);
         std::swap(kin, kout);
         // values: the pass's output becomes the next input; the other buffer of
         // the pair (or, after an implicit-index first pass, the spare) is next

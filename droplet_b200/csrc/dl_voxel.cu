@@ -1162,7 +1162,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
                 sp.glob_off = B.hist.as<uint32_t>(); sp.status = B.status.as<uint32_t>(); sp.counter = scr + VS_SORT + ps;
                 sp.err = scr + VS_ERR; sp.shift = 8 * ps; sp.pass = ps; sp.passes = passes;
                 sp.spin_limit = g_dl_wait.spin_limit;
-                dlsort::pass_k<8><<<sortTiles, dlsort::kThreads, 0, st>>>(sp);
+                dlsort::pass_k<8><<<dlsort::pass_grid(sortTiles), dlsort::kThreads, 0, st>>>(sp);
                 std::swap(kin, kout);
                 std::swap(vin, vout);
             }
