@@ -209,6 +209,22 @@ __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
+// Camera-space position (project.ts:79-84): the shader's order, or in the
+// +-1 LSB arithmetic of DL_BATCH_FAST_EXP frames (kFma) fused multiply-adds.
+// project_k and colour_k both call this, so deferred colours are bit-identical.
+template <bool kFma>
+__device__ __forceinline__ void cam_pos(const float* V, const float pos[3], float& pcx, float& pcy, float& pcz) {
+    if (kFma) {
+        pcx = __fmaf_rn(V[8], pos[2], __fmaf_rn(V[4], pos[1], V[0] * pos[0])) + V[12];
+        pcy = __fmaf_rn(V[9], pos[2], __fmaf_rn(V[5], pos[1], V[1] * pos[0])) + V[13];
+        pcz = __fmaf_rn(V[10], pos[2], __fmaf_rn(V[6], pos[1], V[2] * pos[0])) + V[14];
+    } else {
+        pcx = ((V[0] * pos[0] + V[4] * pos[1]) + V[8] * pos[2]) + V[12];
+        pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
+        pcz = ((V[2] * pos[0] + V[6] * pos[1]) + V[10] * pos[2]) + V[14];
+    }
+}
+
 // Splat colour for one view (project.ts:236-251): DC plus the SH bands
 // evaluated along the normalised view-space position, + 0.5, clamped at 0.
 // project_k and colour_k both call this, so deferred colours are bit-identical.
@@ -217,7 +233,8 @@ __device__ __forceinline__ void splat_colour(const DlSceneDev& sc, uint32_t g, i
                                              float pcy, float pcz, float& c0, float& c1, float& c2) {
     float col0 = dc[0], col1 = dc[1], col2 = dc[2];
     if (sc.bands > 0) {
-        const float len = psqrt<kFma>((pcx * pcx + pcy * pcy) + pcz * pcz);
+        const float len = psqrt<kFma>(kFma ? __fmaf_rn(pcz, pcz, __fmaf_rn(pcy, pcy, pcx * pcx))
+                                           : (pcx * pcx + pcy * pcy) + pcz * pcz);
         float sr, sg, sb;
         const float dxn = pdiv<kFma>(pcx, len), dyn = pdiv<kFma>(pcy, len), dzn = pdiv<kFma>(pcz, len);
         if (sc.sh16) {
@@ -240,9 +257,11 @@ constexpr int kProjectMaxViews = 4096;          // views per frame (per-CTA visi
 constexpr uint32_t kProjectSmemViews = 64;      // view tables staged in shared memory up to this count
 static_assert(sizeof(DlView) % 4 == 0, "DlView is copied as 32-bit words");
 
-// kFma: DL_BATCH_FAST_EXP frames evaluate the SH colour with fused multiply-adds
+// kFma: DL_BATCH_FAST_EXP frames evaluate the camera-space position, the 2D
+// covariance and the SH colour with fused multiply-adds (64 registers, 4 CTAs
+// per SM; the shader's order needs 80 registers, 3 CTAs per SM)
 template <bool kFma>
-__global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
+__global__ void __launch_bounds__(256, kFma ? 4 : 3) project_k(ProjectArgs a) {
     __shared__ uint32_t s_vis[kProjectMaxViews];
     __shared__ DlView s_views[kProjectSmemViews];
     for (uint32_t v = threadIdx.x; v < a.num_views; v += blockDim.x) s_vis[v] = 0;
@@ -308,9 +327,8 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         if (!visible) continue;
 
         // ---- project.ts:79-84
-        const float pcx = ((V[0] * pos[0] + V[4] * pos[1]) + V[8] * pos[2]) + V[12];
-        const float pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
-        const float pcz = ((V[2] * pos[0] + V[6] * pos[1]) + V[10] * pos[2]) + V[14];
+        float pcx, pcy, pcz;
+        cam_pos<kFma>(V, pos, pcx, pcy, pcz);
         const float depth = -pcz;
         float screenX, screenY;
         bool culled = false;
@@ -328,42 +346,67 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
         }
         float conicA = 0, conicB = 0, conicC = 0, radius = 0, radiusFade = 0, aaFactor = 0;
         if (!culled) {
-            // Σ_cam = V Σ Vᵀ (project.ts:103-123)
-            const float v00 = V[0], v01 = V[4], v02 = V[8], v10 = V[1], v11 = V[5], v12 = V[9];
-            const float v20 = V[2], v21 = V[6], v22 = V[10];
-            const float a00 = (v00 * cv.c00 + v01 * cv.c01) + v02 * cv.c02;
-            const float a01 = (v00 * cv.c01 + v01 * cv.c11) + v02 * cv.c12;
-            const float a02 = (v00 * cv.c02 + v01 * cv.c12) + v02 * cv.c22;
-            const float a10 = (v10 * cv.c00 + v11 * cv.c01) + v12 * cv.c02;
-            const float a11 = (v10 * cv.c01 + v11 * cv.c11) + v12 * cv.c12;
-            const float a12 = (v10 * cv.c02 + v11 * cv.c12) + v12 * cv.c22;
-            const float a20 = (v20 * cv.c00 + v21 * cv.c01) + v22 * cv.c02;
-            const float a21 = (v20 * cv.c01 + v21 * cv.c11) + v22 * cv.c12;
-            const float a22 = (v20 * cv.c02 + v21 * cv.c12) + v22 * cv.c22;
-            const float cc00 = (a00 * v00 + a01 * v01) + a02 * v02;
-            const float cc01 = (a00 * v10 + a01 * v11) + a02 * v12;
-            const float cc02 = (a00 * v20 + a01 * v21) + a02 * v22;
-            const float cc11 = (a10 * v10 + a11 * v11) + a12 * v12;
-            const float cc12 = (a10 * v20 + a11 * v21) + a12 * v22;
-            const float cc22 = (a20 * v20 + a21 * v21) + a22 * v22;
-            // EWA Jacobian as written (project.ts:128-149)
-            const float invZ = pdiv<kFma>(1.0f, pcz);
-            const float j00 = u.focal * invZ;
-            const float j02 = ((-u.focal * pcx) * invZ) * invZ;
-            const float j11 = u.focal * invZ;
-            const float j12 = ((-u.focal * pcy) * invZ) * invZ;
-            const float b00 = j00 * cc00 + j02 * cc02;
-            const float b01 = j00 * cc01 + j02 * cc12;
-            const float b02 = j00 * cc02 + j02 * cc22;
-            const float b11 = j11 * cc11 + j12 * cc12;
-            const float b12 = j11 * cc12 + j12 * cc22;
-            const float c00o = b00 * j00 + b02 * j02;
-            const float c01 = b01 * j11 + b02 * j12;
-            const float c11o = b11 * j11 + b12 * j12;
-            const float detOrig = c00o * c11o - c01 * c01;
+            float c00o, c01, c11o;
+            if (kFma) {
+                // +-1 LSB frames: the same 2D covariance J W Σ Wᵀ Jᵀ (W: the view
+                // rotation) associated as (J W) Σ (J W)ᵀ, in fused multiply-adds:
+                // 45 operations where the shader's order takes 99
+                const float invZ = pdiv<true>(1.0f, pcz);
+                const float j00 = u.focal * invZ;
+                const float j02 = ((-u.focal * pcx) * invZ) * invZ;
+                const float j12 = ((-u.focal * pcy) * invZ) * invZ;
+                const float t00 = __fmaf_rn(j02, V[2], j00 * V[0]), t01 = __fmaf_rn(j02, V[6], j00 * V[4]);
+                const float t02 = __fmaf_rn(j02, V[10], j00 * V[8]);
+                const float t10 = __fmaf_rn(j12, V[2], j00 * V[1]), t11 = __fmaf_rn(j12, V[6], j00 * V[5]);
+                const float t12 = __fmaf_rn(j12, V[10], j00 * V[9]);
+                const float s0 = __fmaf_rn(cv.c02, t02, __fmaf_rn(cv.c01, t01, cv.c00 * t00));
+                const float s1 = __fmaf_rn(cv.c12, t02, __fmaf_rn(cv.c11, t01, cv.c01 * t00));
+                const float s2 = __fmaf_rn(cv.c22, t02, __fmaf_rn(cv.c12, t01, cv.c02 * t00));
+                const float q0 = __fmaf_rn(cv.c02, t12, __fmaf_rn(cv.c01, t11, cv.c00 * t10));
+                const float q1 = __fmaf_rn(cv.c12, t12, __fmaf_rn(cv.c11, t11, cv.c01 * t10));
+                const float q2 = __fmaf_rn(cv.c22, t12, __fmaf_rn(cv.c12, t11, cv.c02 * t10));
+                c00o = __fmaf_rn(t02, s2, __fmaf_rn(t01, s1, t00 * s0));
+                c01 = __fmaf_rn(t12, s2, __fmaf_rn(t11, s1, t10 * s0));
+                c11o = __fmaf_rn(t12, q2, __fmaf_rn(t11, q1, t10 * q0));
+            } else {
+                // Σ_cam = V Σ Vᵀ (project.ts:103-123)
+                const float v00 = V[0], v01 = V[4], v02 = V[8], v10 = V[1], v11 = V[5], v12 = V[9];
+                const float v20 = V[2], v21 = V[6], v22 = V[10];
+                const float a00 = (v00 * cv.c00 + v01 * cv.c01) + v02 * cv.c02;
+                const float a01 = (v00 * cv.c01 + v01 * cv.c11) + v02 * cv.c12;
+                const float a02 = (v00 * cv.c02 + v01 * cv.c12) + v02 * cv.c22;
+                const float a10 = (v10 * cv.c00 + v11 * cv.c01) + v12 * cv.c02;
+                const float a11 = (v10 * cv.c01 + v11 * cv.c11) + v12 * cv.c12;
+                const float a12 = (v10 * cv.c02 + v11 * cv.c12) + v12 * cv.c22;
+                const float a20 = (v20 * cv.c00 + v21 * cv.c01) + v22 * cv.c02;
+                const float a21 = (v20 * cv.c01 + v21 * cv.c11) + v22 * cv.c12;
+                const float a22 = (v20 * cv.c02 + v21 * cv.c12) + v22 * cv.c22;
+                const float cc00 = (a00 * v00 + a01 * v01) + a02 * v02;
+                const float cc01 = (a00 * v10 + a01 * v11) + a02 * v12;
+                const float cc02 = (a00 * v20 + a01 * v21) + a02 * v22;
+                const float cc11 = (a10 * v10 + a11 * v11) + a12 * v12;
+                const float cc12 = (a10 * v20 + a11 * v21) + a12 * v22;
+                const float cc22 = (a20 * v20 + a21 * v21) + a22 * v22;
+                // EWA Jacobian as written (project.ts:128-149)
+                const float invZ = pdiv<kFma>(1.0f, pcz);
+                const float j00 = u.focal * invZ;
+                const float j02 = ((-u.focal * pcx) * invZ) * invZ;
+                const float j11 = u.focal * invZ;
+                const float j12 = ((-u.focal * pcy) * invZ) * invZ;
+                const float b00 = j00 * cc00 + j02 * cc02;
+                const float b01 = j00 * cc01 + j02 * cc12;
+                const float b02 = j00 * cc02 + j02 * cc22;
+                const float b11 = j11 * cc11 + j12 * cc12;
+                const float b12 = j11 * cc12 + j12 * cc22;
+                c00o = b00 * j00 + b02 * j02;
+                c01 = b01 * j11 + b02 * j12;
+                c11o = b11 * j11 + b12 * j12;
+            }
+            const float c01s = c01 * c01;
+            const float detOrig = kFma ? __fmaf_rn(c00o, c11o, -c01s) : c00o * c11o - c01s;
             const float c00 = c00o + DL_AA_DILATION;
             const float c11 = c11o + DL_AA_DILATION;
-            const float det = c00 * c11 - c01 * c01;
+            const float det = kFma ? __fmaf_rn(c00, c11, -c01s) : c00 * c11 - c01s;
             aaFactor = psqrt<kFma>(fmaxf(pdiv<kFma>(detOrig, det), 0.0f));
             if (det <= 1.0e-6f) {
                 culled = true;
@@ -385,7 +428,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
             }
             if (!culled) {
                 const float mid = 0.5f * (c00 + c11);
-                const float radiusEig = psqrt<kFma>(fmaxf(0.1f, mid * mid - det));
+                const float radiusEig = psqrt<kFma>(fmaxf(0.1f, kFma ? __fmaf_rn(mid, mid, -det) : mid * mid - det));
                 const float lambda1 = mid + radiusEig;
                 const float radiusRaw = DL_SIGMA_CUTOFF * psqrt<kFma>(lambda1);
                 const float fadeStart = DL_FADE_START_FRAC * u.height;
@@ -435,7 +478,7 @@ __global__ void __launch_bounds__(256, 3) project_k(ProjectArgs a) {
                 cB = __half2float(__float2half_rn(cB));
                 cC = __half2float(__float2half_rn(cC));
             }
-            const float ac = cA * cC, dt = ac - cB * cB;
+            const float ac = cA * cC, dt = kFma ? __fmaf_rn(-cB, cB, ac) : ac - cB * cB;
             if (dt > 0.0f && ac <= 1024.0f * dt) {
                 const float lx = DL_GAUSS_FLOOR + pdiv<kFma>(DL_MIN_ALPHA, alSt);
                 const float qa = -2.0f * (kFma ? __logf(lx) : logf(lx));
@@ -554,10 +597,8 @@ __global__ void __launch_bounds__(256) colour_k(ColourArgs a) {
         if ((v & 31u) == 0) m = __ldg(a.vis_mask + (uint64_t)(v >> 5) * a.sc.n + g);
         if (!((m >> (v & 31u)) & 1u)) continue;
         {
-            const float* V = vtab[v].view;
-            const float pcx = ((V[0] * pos[0] + V[4] * pos[1]) + V[8] * pos[2]) + V[12];
-            const float pcy = ((V[1] * pos[0] + V[5] * pos[1]) + V[9] * pos[2]) + V[13];
-            const float pcz = ((V[2] * pos[0] + V[6] * pos[1]) + V[10] * pos[2]) + V[14];
+            float pcx, pcy, pcz;
+            cam_pos<kFma>(vtab[v].view, pos, pcx, pcy, pcz);
             float c0, c1, c2;
             splat_colour<kFma>(a.sc, g, M, dc, pcx, pcy, pcz, c0, c1, c2);
             const uint64_t o = (uint64_t)v * a.view_stride + g;
