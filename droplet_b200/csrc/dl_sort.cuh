@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
     __shared__ uint32_t s_vals[kTile];
     __shared__ uint32_t s_hist[WARPS][RADIX];
     __shared__ uint32_t s_toff[RADIX];
-    __shared__ uint32_t s_glob[RADIX];
+    __shared__ uint32_t s_glob[RADIX];          // per digit: segment position of local slot i, minus i (mod 2^32)
     __shared__ uint32_t s_wsum[WARPS];
     __shared__ uint32_t s_tile, s_next;
     __shared__ uint32_t s_nkeep;                 // elements of the tile that are written
@@ -315,14 +315,14 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
                 }
                 if (publish) dl_st_volatile(p.status + (size_t)tile * RADIX + tid, kFlagPrefix | ((excl + cnt) & kValMask));
             }
-            s_glob[tid] = p.glob_off[((size_t)seg * p.passes + p.pass) * RADIX + tid] + excl;
+            s_glob[tid] = p.glob_off[((size_t)seg * p.passes + p.pass) * RADIX + tid] + excl - s_toff[tid];
         }
         __syncthreads();
         const uint32_t nKeep = DROP ? s_nkeep : nValid;
         for (uint32_t i = tid; i < nKeep; i += kThreads) {
             const uint32_t k = s_keys[i];
             const uint32_t d = (k >> p.shift) & MASK;
-            const uint64_t dst = base + s_glob[d] + (i - s_toff[d]);
+            const uint64_t dst = base + (uint32_t)(s_glob[d] + i);
             if (p.keys_out) p.keys_out[dst] = k;
             p.vals_out[dst] = s_vals[i];
         }

@@ -322,6 +322,14 @@ def test_offscreen_cull_changes_no_pixel(device, renderer, op_mu):
         b = r2.render_batch(sc, cams, flags=flags | _lib.DL_BATCH_CULL_OFFSCREEN)
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
+    # the cull mode's screen record (box half-extents) through the other fast rasterizers
+    fast = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
+    a = r2.render_batch(sc, cams, flags=fast)
+    for shape in ("tile", "8x4-f32x2", "8x4"):
+        r2.set_tuning(raster_shape=shape)
+        for x, y in zip(a, r2.render_batch(sc, cams, flags=fast | _lib.DL_BATCH_CULL_OFFSCREEN)):
+            assert np.array_equal(x, y), shape
+    r2.set_tuning()
     one = r2.render_batch(sc, cams[:1], flags=_lib.DL_BATCH_CULL_OFFSCREEN)[0]
     assert np.array_equal(one, renderer.render(d, cams[0]))
     assert int(r2.debug_get("nvis", np.uint64)[0]) < d.count
