@@ -47,7 +47,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-tune", action="store_true", help="skip the autotuner (default knobs)")
     p.add_argument("--raster-shape", default=None,
-                   help="with --no-tune: the rasterizer work item (8x4, 16x2, 4x8, 8x8x2, 8x4-f32x2)")
+                   help="with --no-tune: the rasterizer (8x4, 16x2, 4x8, 8x8x2, 8x4-f32x2, tile-f32x2, tile)")
+    p.add_argument("--pair-sort-bits", type=int, default=None, choices=[6, 7, 8],
+                   help="with --no-tune: the tile-pair sort's digit width")
     p.add_argument("--views", type=int, default=64)
     p.add_argument("--splats", type=int, default=3_000_000)
     p.add_argument("--no-e2e", action="store_true")
@@ -368,8 +370,8 @@ def run_ours(args, rank, world, local_rank):
         return ms
 
     # autotuner (untimed): pair-sort digit width, raster work-item shape, CTAs/SM
-    if args.no_tune and args.raster_shape:
-        r.set_tuning(raster_shape=args.raster_shape)
+    if args.no_tune and (args.raster_shape or args.pair_sort_bits):
+        r.set_tuning(raster_shape=args.raster_shape or "tile-f32x2", pair_sort_bits=args.pair_sort_bits or 8)
     tuning = None if args.no_tune else r.autotune(scene, cams, flags=FAST, reps=2)
 
     # the headline: tiles rasterized in the static (tile index) order, which

@@ -2,7 +2,8 @@
 //
 // One frame (any number of views of one device-resident scene):
 //   project_k -> depth sort (4 onesweep passes) -> emit_k -> pair_digits_k
-//   -> pair sort (1-3 onesweep passes) -> boundaries_k -> rasterize_k
+//   -> pair sort (1-3 onesweep passes; the last one lowers the tile offsets,
+//      bound_init_k / bound_fill_k around it) -> rasterize_k
 // No host synchronisation happens inside the frame: every size a later stage
 // needs (visible count, pair count, tile offsets) stays in device memory.
 // Pair buffers are sized from an upper bound; if a frame overflows them the
@@ -51,15 +52,17 @@ int ensure_pinned(void** p, size_t* cap, size_t need) {
 }
 
 template <int BITS>
-void launch_pass(const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
+void launch_pass(const dlsort::Pass& p, uint32_t grid, cudaStream_t st, const dlsort::Bound& b) {
     if (p.drop_max) dlsort::pass_k<BITS, true><<<dlsort::pass_grid(grid), dlsort::kThreads, 0, st>>>(p);
+    else if (b.bound) dlsort::pass_k<BITS, false, true><<<dlsort::pass_grid(grid), dlsort::kThreads, 0, st>>>(p, b);
     else dlsort::pass_k<BITS><<<dlsort::pass_grid(grid), dlsort::kThreads, 0, st>>>(p);
 }
 
-void launch_pass_bits(int bits, const dlsort::Pass& p, uint32_t grid, cudaStream_t st) {
-    if (bits == 8) launch_pass<8>(p, grid, st);
-    else if (bits == 7) launch_pass<7>(p, grid, st);
-    else launch_pass<6>(p, grid, st);
+void launch_pass_bits(int bits, const dlsort::Pass& p, uint32_t grid, cudaStream_t st,
+                      const dlsort::Bound& b = dlsort::Bound()) {
+    if (bits == 8) launch_pass<8>(p, grid, st, b);
+    else if (bits == 7) launch_pass<7>(p, grid, st, b);
+    else launch_pass<6>(p, grid, st, b);
 }
 
 // SH in 16 bits, repacked per Gaussian: in[g][c * M + k] (channel-major, as
@@ -550,16 +553,25 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
         dlsort::prepare_k<<<1, 32, 0, st>>>(ps);
         (*launches)++;
         uint32_t *kin = f.pkeys0, *kout = f.pkeys1, *vin = f.pvals0, *vout = f.pvals1;
+        // the last pass lowers the tile offsets itself (bound_init_k presets them)
+        dlr::BoundArgs bi;
+        bi.views = f.views; bi.keys = nullptr; bi.pair_base = f.pairBase; bi.seg_len = f.pairSegLen;
+        bi.tile_off = f.tileOff; bi.tile_stride = d.TS; bi.err = f.scr + SC_ERR;
+        dlr::bound_init_k<<<dim3((d.TS + 255) / 256, d.V), 256, 0, st>>>(bi);
+        (*launches)++;
         for (int p = 0; p < d.ppasses; p++) {
             DL_CK(cudaMemsetAsync(f.sortStatus, 0, 4ull * 256 * d.pairGrid, st));
             dlsort::Pass sp;
-            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = kout; sp.vals_out = vout;
+            const bool last = p + 1 == d.ppasses;
+            sp.keys_in = kin; sp.vals_in = vin; sp.keys_out = last ? nullptr : kout; sp.vals_out = vout;
+            dlsort::Bound bd;
+            if (last) { bd.bound = f.tileOff; bd.stride = d.TS; }
             sp.segs = ps; sp.glob_off = f.pairGlob;
             sp.status = f.sortStatus; sp.counter = f.scr + SC_PAIR_CTR + p; sp.err = f.scr + SC_ERR;
             sp.shift = d.pbits * p; sp.pass = p; sp.passes = d.ppasses;
             sp.spin_limit = g_dl_wait.spin_limit;
             if (p == 0) sp.withhold_tile = g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT);
-            launch_pass_bits(d.pbits, sp, d.pairGrid, st);
+            launch_pass_bits(d.pbits, sp, d.pairGrid, st, bd);
             (*launches)++;
             std::swap(kin, kout);
             std::swap(vin, vout);
@@ -576,8 +588,12 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ba.tile_off = f.tileOff;
     ba.tile_stride = d.TS;
     ba.err = f.scr + SC_ERR;
-    const uint32_t bgrid = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((d.cap + 256) / 256, 1), 2048);
-    dlr::boundaries_k<<<dim3(bgrid, d.V), 256, 0, st>>>(ba);
+    if (d.ppasses > 0) {
+        dlr::bound_fill_k<<<d.V, dlr::kFillThreads, 0, st>>>(ba);
+    } else {                            // one tile per view: the keys are all 0
+        const uint32_t bgrid = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((d.cap + 256) / 256, 1), 2048);
+        dlr::boundaries_k<<<dim3(bgrid, d.V), 256, 0, st>>>(ba);
+    }
     (*launches)++;
     DL_CK(cudaGetLastError());
 

@@ -860,6 +860,58 @@ __global__ void boundaries_k(BoundArgs a) {
     }
 }
 
+// The same offsets without the sorted tile ids: the pair sort's last pass
+// lowers tileOffsets[t] (atomicMin) to the position of the first pair of tile
+// t it writes; bound_init_k presets every entry of a view to its pair count
+// before that pass, and bound_fill_k then gives each empty tile the start of
+// the next non-empty one (a suffix minimum; positions grow with the tile id),
+// which is find-boundaries.ts's result: the first pair index with tile >= t.
+__global__ void bound_init_k(BoundArgs a) {
+    const uint32_t v = blockIdx.y;
+    const uint32_t n = a.seg_len[v];
+    const uint32_t T = a.views[v].numTiles;
+    uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= T; t += gridDim.x * blockDim.x) to[t] = n;
+}
+
+constexpr int kFillThreads = 1024;
+
+__global__ void __launch_bounds__(kFillThreads) bound_fill_k(BoundArgs a) {
+    __shared__ uint32_t s_w[kFillThreads / 32];
+    __shared__ uint32_t s_carry;
+    const uint32_t v = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t T = a.views[v].numTiles;
+    uint32_t* to = a.tile_off + (uint64_t)v * a.tile_stride;
+    // after a timed-out pair sort every view gets empty tiles
+    if (dl_ld_volatile(a.err) & DL_DEVERR_TIMEOUT) {
+        for (uint32_t t = tid; t <= T; t += kFillThreads) to[t] = 0u;
+        return;
+    }
+    if (tid == 0) s_carry = 0xffffffffu;
+    // chunks of kFillThreads entries from the end: suffix minimum inside the
+    // chunk, then with the minimum of everything after it
+    for (int64_t hi = (int64_t)T + 1; hi > 0; hi -= kFillThreads) {
+        const int64_t lo = hi - kFillThreads;
+        const int64_t t = lo + tid;
+        uint32_t x = t >= 0 ? to[t] : 0xffffffffu;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_down_sync(0xffffffffu, x, o);
+            if (lane + o < 32) x = min(x, y);
+        }
+        if (lane == 0) s_w[warp] = x;                 // minimum of the warp's entries
+        __syncthreads();
+        uint32_t later = s_carry;
+        for (int w = warp + 1; w < kFillThreads / 32; w++) later = min(later, s_w[w]);
+        x = min(x, later);
+        if (t >= 0) to[t] = x;
+        __syncthreads();                              // s_w and s_carry are rewritten next
+        if (tid == 0) s_carry = x;                    // the chunk's minimum: its first entry
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ tile features
 // The 12 inputs of the learned cost model for tile t of view u, from the tile
 // offsets alone (available after boundaries_k, before the rasterizer).

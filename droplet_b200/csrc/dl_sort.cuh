@@ -149,6 +149,16 @@ struct Pass {
     uint32_t withhold_tile = 0xffffffffu;  // test hook: this global tile publishes no status
 };
 
+// Optional table of the last pass of a sort whose keys index a table: the
+// first element of each run of equal keys in a CTA's tile lowers
+// bound[seg * stride + key] (atomicMin) to its position in the segment, so the
+// table ends with each present key's first position; the caller presets the
+// table, and keys_out is not written.  Launch pass_k<BITS, false, true> with it.
+struct Bound {
+    uint32_t* bound = nullptr;
+    uint32_t stride = 0;
+};
+
 constexpr int kLookback = 4;
 
 // Persistent passes: at most 4 resident CTAs per SM loop over the tiles.
@@ -162,9 +172,11 @@ inline uint32_t pass_grid(uint32_t tiles) {
     return tiles < (uint32_t)sms * 4u ? tiles : (uint32_t)sms * 4u;
 }                 // predecessor tiles read per look-back step
 
-// DROP: compiled in only for passes with Pass::drop_max set.
-template <int BITS, bool DROP = false>
-__global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
+// DROP: compiled in only for passes with Pass::drop_max set; BOUND: only for
+// a pass with Pass::bound set (either adds registers that other passes would
+// pay for in spills).
+template <int BITS, bool DROP = false, bool BOUND = false>
+__global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p, Bound bd = Bound()) {
     constexpr int RADIX = 1 << BITS;
     constexpr int WARPS = kThreads / 32;
     constexpr uint32_t MASK = RADIX - 1;
@@ -319,12 +331,24 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p) {
         }
         __syncthreads();
         const uint32_t nKeep = DROP ? s_nkeep : nValid;
-        for (uint32_t i = tid; i < nKeep; i += kThreads) {
-            const uint32_t k = s_keys[i];
-            const uint32_t d = (k >> p.shift) & MASK;
-            const uint64_t dst = base + (uint32_t)(s_glob[d] + i);
-            if (p.keys_out) p.keys_out[dst] = k;
-            p.vals_out[dst] = s_vals[i];
+        if constexpr (BOUND) {
+            uint32_t* const bnd = bd.bound + (size_t)seg * bd.stride;
+            for (uint32_t i = tid; i < nKeep; i += kThreads) {
+                const uint32_t k = s_keys[i];
+                const uint32_t pos = s_glob[(k >> p.shift) & MASK] + i;
+                p.vals_out[base + pos] = s_vals[i];
+                // the tile is sorted by the whole key here (the earlier passes
+                // sorted the lower digits): a run's first slot is its smallest position
+                if (i == 0 || s_keys[i - 1] != k) atomicMin(bnd + k, pos);
+            }
+        } else {
+            for (uint32_t i = tid; i < nKeep; i += kThreads) {
+                const uint32_t k = s_keys[i];
+                const uint32_t d = (k >> p.shift) & MASK;
+                const uint64_t dst = base + (uint32_t)(s_glob[d] + i);
+                if (p.keys_out) p.keys_out[dst] = k;
+                p.vals_out[dst] = s_vals[i];
+            }
         }
         // shared memory is reused by the next tile; a timed-out wait ends the CTA
         if (__syncthreads_or(tid == 0 && (dl_ld_volatile(p.err) & DL_DEVERR_TIMEOUT))) return;
