@@ -164,11 +164,13 @@ def peaks():
         return None
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the rasterizer from the committed ncu summary."""
+def profile_traffic(npairs):
+    """Per-launch DRAM bytes of the rasterizer: the committed ncu capture of the
+    full-size ring64 launch, scaled by tile pairs when this batch differs."""
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", "rasterize_ring64.json"))).get("dram_bytes_per_launch")
-    except (OSError, ValueError):
+        d = json.load(open(os.path.join(ROOT, "profiles", "rasterize_ring64.json")))
+        return d["dram_bytes_per_launch"] * npairs / d["pairs_per_launch"]
+    except (OSError, ValueError, KeyError, ZeroDivisionError):
         return None
 
 
@@ -457,8 +459,9 @@ def run_ours(args, rank, world, local_rank):
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     flops = evals * 20
     roof = {"kernel": "rasterizer (fused finalize)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-            "unit": "GB/s", "frac": achieved / hbm, "traffic": profile_traffic(),
-            "traffic_source": "ncu dram bytes of a 4-view capture of the same kernel, scaled by tile pairs",
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": profile_traffic(npairs),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size ring64 launch "
+                              "of this kernel (1-pass capture), scaled by tile pairs",
             "limiter": "instruction issue (FP32 / ALU pipes), not HBM: see compute",
             "peak_source": "measured" if pk else "fallback",
             "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": rast_ms,

@@ -335,6 +335,42 @@ def test_offscreen_cull_changes_no_pixel(device, renderer, op_mu):
     assert int(r2.debug_get("nvis", np.uint64)[0]) < d.count
 
 
+def test_cull_mode_near_the_image_edges(device, renderer):
+    # The cull mode drops splat-views whose tile box misses the image.  Splats
+    # straddling the frustum's edges, strongly anisotropic, with unnormalised
+    # rotations: the pixels are those of the frame without the cull mode and,
+    # in the exact arithmetic, of the oracle.
+    rng = np.random.default_rng(23)
+    n = 40_000
+    cam = synth.pinhole(640, 360, (0.0, 0.0, 4.0))
+    half_h = math.tan(math.pi / 6)
+    half_w = half_h * 640 / 360
+    z = rng.uniform(0.5, 8.0, n)                    # distance in front of the camera
+    side = rng.integers(0, 4, n)
+    u = rng.uniform(-1.3, 1.3, n)
+    edge = rng.uniform(0.9, 1.4, n)                 # in units of the half-width: inside and outside
+    x = np.where(side < 2, np.where(side == 0, -1, 1) * edge * half_w, u * half_w) * z
+    y = np.where(side >= 2, np.where(side == 2, -1, 1) * edge * half_h, u * half_h) * z
+    pos = np.stack([x, y, 4.0 - z], 1)
+    q = rng.normal(0.0, 1.0, (n, 4)) * rng.uniform(0.5, 2.0, (n, 1))
+    ls = np.stack([rng.uniform(math.log(0.05), math.log(0.6), n), rng.uniform(math.log(0.002), math.log(0.02), n),
+                   rng.uniform(math.log(0.002), math.log(0.05), n)], 1)
+    d = SplatData(n, pos.astype(np.float32), q.astype(np.float32), ls.astype(np.float32),
+                  rng.normal(1.0, 1.5, n).astype(np.float32), rng.normal(0.0, 0.5, (n, 3)).astype(np.float32))
+    r2 = dl.Renderer(device)
+    sc = r2.upload(d)
+    cams = [cam, synth.pinhole(333, 257, (0.5, -0.3, 3.0))]
+    fast = _lib.DL_BATCH_F16_RECORDS | _lib.DL_BATCH_FAST_EXP
+    for flags in (0, fast):
+        a = r2.render_batch(sc, cams, flags=flags)
+        b = r2.render_batch(sc, cams, flags=flags | _lib.DL_BATCH_CULL_OFFSCREEN)
+        for x0, y0 in zip(a, b):
+            assert np.array_equal(x0, y0), flags
+    exact = r2.render_batch(sc, cams, flags=_lib.DL_BATCH_CULL_OFFSCREEN)
+    for img, c in zip(exact, cams):
+        assert np.array_equal(img, O.render(d, c)["rgba"])
+
+
 def test_ply_parsed_into_pinned_memory_renders_like_its_data(renderer, tmp_path):
     # dl_ply_load parses the file into page-locked arrays; rendering them is
     # bit-exact with the same splats loaded by the Python loader, and with the oracle
