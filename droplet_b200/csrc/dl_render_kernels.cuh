@@ -8,7 +8,9 @@
 //   (pair-sort digit offsets)                    -> pair_digits_k
 //   emit-pairs.ts:28-57 emit                    -> emit_k (load-balanced emission)
 //   pipeline.ts:544-578 stable pair sort          -> dlsort passes on tile ids
-//   find-boundaries.ts:17-99 tile offsets         -> boundaries_k (direct writes, no atomics)
+//   find-boundaries.ts:17-99 tile offsets         -> lowered by the pair sort's last pass (dl_sort.cuh
+//                                                    Bound), bound_init_k / bound_fill_k; boundaries_k
+//                                                    (direct writes) when a view has one tile
 //   rasterize.ts:36-82 + finalize.ts:30-43    -> rasterize_k (fused)
 //
 // All f32 arithmetic that feeds an integer decision or an output byte is
@@ -914,7 +916,7 @@ __global__ void __launch_bounds__(kFillThreads) bound_fill_k(BoundArgs a) {
 
 // ------------------------------------------------------------------ tile features
 // The 12 inputs of the learned cost model for tile t of view u, from the tile
-// offsets alone (available after boundaries_k, before the rasterizer).
+// offsets alone (available after bound_fill_k, before the rasterizer).
 __device__ __forceinline__ void tile_features(const DlView& u, const uint32_t* to, uint32_t t, float* x) {
     const int tx = (int)(t % u.tilesX), ty = (int)(t / u.tilesX);
     auto cnt = [&](int cx, int cy) {
