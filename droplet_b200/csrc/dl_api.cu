@@ -110,6 +110,8 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
     r->tuneOut.release();
     if (r->copy_stream) { cudaStreamSynchronize(r->copy_stream); cudaStreamDestroy(r->copy_stream); }
     if (r->copy_event) cudaEventDestroy(r->copy_event);
+    if (r->raster_stream) { cudaStreamSynchronize(r->raster_stream); cudaStreamDestroy(r->raster_stream); }
+    for (auto& e : r->raster_ev) if (e) cudaEventDestroy(e);
     for (auto& e : r->upload_events) if (e) cudaEventDestroy(e);
     if (r->h_views) cudaFreeHost(r->h_views);
     if (r->h_u64) cudaFreeHost(r->h_u64);

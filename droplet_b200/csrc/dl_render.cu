@@ -267,6 +267,8 @@ struct FramePtrs {
     const uint32_t* rbTileBase;    // host [V+1] first global tile of each view
     cudaStream_t rbStream;
     cudaEvent_t rbEvent;
+    cudaStream_t rasterStream2;    // with rbGroups: the odd view ranges rasterize here (NULL: all on the frame's)
+    cudaEvent_t rasterEv[2];
     // learned schedule: features -> MLP -> longest-first tile order
     float* feat;                   // [total tiles][12], or NULL
     float* pred;
@@ -668,35 +670,35 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     ra.sub_lw = d.subLw;
     ra.rec_box = d.cullOff ? 1 : 0;
     ra.stage_pad = stage_pad();
-    auto raster = [&](const dlr::RasterArgs& x) {
+    auto raster = [&](const dlr::RasterArgs& x, cudaStream_t rs) {
         if (d.tileK && !count) {
             if (d.fastExp) {
-                if (x.tile_cycles) dlr::rasterize_tile_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-                else dlr::rasterize_tile_k<false, false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                if (x.tile_cycles) dlr::rasterize_tile_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+                else dlr::rasterize_tile_k<false, false><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
             } else {
-                if (x.tile_cycles) dlr::rasterize_tile_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-                else dlr::rasterize_tile_k<true, false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                if (x.tile_cycles) dlr::rasterize_tile_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+                else dlr::rasterize_tile_k<true, false><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
             }
         } else if (d.tileCta && !count) {
-            if (x.tile_cycles) dlr::rasterize_tile_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-            else dlr::rasterize_tile_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            if (x.tile_cycles) dlr::rasterize_tile_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+            else dlr::rasterize_tile_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
         } else if (d.x2 && !count) {
-            if (x.tile_cycles) dlr::rasterize_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-            else dlr::rasterize_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            if (x.tile_cycles) dlr::rasterize_x2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+            else dlr::rasterize_x2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
         } else if (d.ppl2) {
             if (d.fastExp) {
-                if (count) dlr::rasterize2_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-                else dlr::rasterize2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                if (count) dlr::rasterize2_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+                else dlr::rasterize2_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
             } else {
-                if (count) dlr::rasterize2_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-                else dlr::rasterize2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+                if (count) dlr::rasterize2_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+                else dlr::rasterize2_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
             }
         } else if (d.fastExp) {
-            if (count) dlr::rasterize_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-            else dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            if (count) dlr::rasterize_k<false, true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+            else dlr::rasterize_k<false><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
         } else {
-            if (count) dlr::rasterize_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
-            else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, st>>>(x);
+            if (count) dlr::rasterize_k<true, true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
+            else dlr::rasterize_k<true><<<d.rasterGrid, dlr::kRasterThreads, 0, rs>>>(x);
         }
         (*launches)++;
     };
@@ -708,22 +710,36 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
         const uint32_t ipt = 1u << iptLg;
         static_assert(SC_RASTER_CTR + kReadBackGroups <= kScratchWords, "scratch words");
         DL_CK(cudaMemsetAsync(f.scr + SC_RASTER_CTR, 0, 4ull * kReadBackGroups, st));
+        // Ranges alternate between the frame's stream and a second one, so
+        // that the next range's CTAs take the SMs that the current range's
+        // persistent CTAs leave at its end (ranges of one stream run in order;
+        // at most two ranges are in flight).
+        const bool two = f.rasterStream2 != nullptr;
+        if (two) {
+            DL_CK(cudaEventRecord(f.rasterEv[0], st));
+            DL_CK(cudaStreamWaitEvent(f.rasterStream2, f.rasterEv[0], 0));
+        }
         for (uint32_t v0 = 0, g = 0; v0 < d.V; v0 += per, g++) {
             const uint32_t v1 = std::min(d.V, v0 + per);
+            cudaStream_t rs = (two && (g & 1u)) ? f.rasterStream2 : st;
             dlr::RasterArgs x = ra;
             x.item_base = ipt * f.rbTileBase[v0];
             x.num_items = ipt * f.rbTileBase[v1];
             x.work_counter = f.scr + SC_RASTER_CTR + g;      // g < rbGroups <= kReadBackGroups
-            raster(x);
+            raster(x, rs);
             DL_CK(cudaGetLastError());
-            DL_CK(cudaEventRecord(f.rbEvent, st));
+            DL_CK(cudaEventRecord(f.rbEvent, rs));
             DL_CK(cudaStreamWaitEvent(f.rbStream, f.rbEvent, 0));
             for (uint32_t v = v0; v < v1; v++)
                 DL_CK(cudaMemcpyAsync(f.rbHost[v], f.rbDev[v], (uint64_t)f.rbViews[v].W * f.rbViews[v].H * 4,
                                       cudaMemcpyDeviceToHost, f.rbStream));
         }
+        if (two) {                       // the frame's stream continues after both
+            DL_CK(cudaEventRecord(f.rasterEv[1], f.rasterStream2));
+            DL_CK(cudaStreamWaitEvent(st, f.rasterEv[1], 0));
+        }
     } else {
-        raster(ra);
+        raster(ra, st);
     }
     DL_CK(cudaGetLastError());
     rec_event(ev, 7, st);
@@ -885,6 +901,12 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             f.rbTileBase = rbTileBase.data();
             f.rbStream = overlap->stream;
             f.rbEvent = overlap->event;
+            if (!r->raster_stream) DL_CK(cudaStreamCreateWithFlags(&r->raster_stream, cudaStreamNonBlocking));
+            for (auto& e : r->raster_ev)
+                if (!e) DL_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            f.rasterStream2 = r->raster_stream;
+            f.rasterEv[0] = r->raster_ev[0];
+            f.rasterEv[1] = r->raster_ev[1];
         }
     }
     const bool useGraph = !(flags & DL_BATCH_NO_GRAPH) && !(flags & DL_BATCH_PLAIN) && V > 1 && !r->profiling &&
