@@ -143,7 +143,8 @@ struct Pass {
     // 1: elements whose key is 0xffffffff are dropped (neither ranked nor
     // written); the others keep their relative order, so the output is the
     // stable pass over the remaining elements, compacted to the segment start.
-    // Launch pass_k<BITS, true> for such a pass.
+    // Launch pass_k<BITS, true> for such a pass; it ignores vals_in and takes
+    // the implicit values (each element's index in its segment).
     int drop_max = 0;
     uint32_t spin_limit = DL_SPIN_LIMIT;   // look-back polls before giving up
     uint32_t withhold_tile = 0xffffffffu;  // test hook: this global tile publishes no status
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p, Bound bd = Bound()
         const uint32_t e = warp * 32 * kItems + j * 32 + lane;
         const bool ok = e < nValid;
         key[j] = ok ? p.keys_in[base + t0 + e] : 0u;
-        val[j] = ok ? (p.vals_in ? p.vals_in[base + t0 + e] : t0 + e) : 0u;
+        if (!DROP) val[j] = ok ? (p.vals_in ? p.vals_in[base + t0 + e] : t0 + e) : 0u;
     }
 
     while (true) {
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p, Bound bd = Bound()
             if (dig[j] < RADIX) {
                 const uint32_t pos = s_toff[dig[j]] + s_hist[warp][dig[j]] + rank[j];
                 s_keys[pos] = key[j];
-                s_vals[pos] = val[j];
+                s_vals[pos] = DROP ? t0 + (uint32_t)(warp * 32 * kItems + j * 32 + lane) : val[j];
             }
         }
         // the next tile's elements: in flight during the look-back and the write-out
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_k(Pass p, Bound bd = Bound()
                 const uint32_t e = warp * 32 * kItems + j * 32 + lane;
                 const bool ok = e < nnv;
                 key[j] = ok ? p.keys_in[nbase + nt0 + e] : 0u;
-                val[j] = ok ? (p.vals_in ? p.vals_in[nbase + nt0 + e] : nt0 + e) : 0u;
+                if (!DROP) val[j] = ok ? (p.vals_in ? p.vals_in[nbase + nt0 + e] : nt0 + e) : 0u;
             }
         }
         // decoupled look-back for this digit's prefix over earlier tiles of the segment
