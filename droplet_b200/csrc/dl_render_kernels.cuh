@@ -1502,6 +1502,17 @@ __device__ __forceinline__ void pad_pair_slot(float* sp, uint32_t n) {
     P[14] = 0.0f; P[15] = 0.0f; P[17] = 0.0f;
 }
 
+// Writes a splat already in the packed form (negated, conic pre-scaled, colours
+// held finite: the values put_pair_slot computes) into slot `slot`.
+__device__ __forceinline__ void put_pair_slot_raw(float* sp, uint32_t slot, const float4& fa, const float4& fb,
+                                                  float fc) {
+    float* P = sp + (slot >> 1) * kPairFloats;
+    const uint32_t c = slot & 1u;
+    P[0 + c] = fa.x; P[2 + c] = fa.y; P[4 + c] = fa.z; P[6 + c] = fa.w;
+    P[8 + c] = fb.x; P[10 + c] = fb.y; P[12 + 2 * c] = fb.z; P[13 + 2 * c] = fb.w;
+    P[16 + c] = fc;
+}
+
 __device__ __forceinline__ uint32_t stage_chunk_x2(const RasterArgs& a, const uint32_t* vals, uint32_t b,
                                                    uint32_t end, uint64_t vo, float rx0, float rx1, float ry0,
                                                    float ry1, uint32_t lmask, float* sp) {
@@ -1677,7 +1688,11 @@ constexpr int kTileStage = kRasterThreads;     // pairs staged per batch
 
 template <bool kCycles>
 __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterArgs a) {
-    __shared__ float s_f[9][kTileStage];       // x, y, A, B, C, alpha, r, g, b of each staged pair
+    // each staged pair in the packed form of the pair buffers (put_pair_slot's
+    // values, computed once here instead of once per work item it reaches)
+    __shared__ float4 s_fa[kTileStage];        // -x, -y, -A log2(e)/2, -B log2(e)
+    __shared__ float4 s_fb[kTileStage];        // -C log2(e)/2, -alpha, -r, -g
+    __shared__ float s_fc[kTileStage];         // -b
     __shared__ uint8_t s_m[kTileStage];        // items the staged splat reaches (bit w: item w)
     __shared__ __align__(16) float s_p[kRasterWarps][32 * kPairFloats];
     __shared__ uint32_t s_tile;
@@ -1754,9 +1769,11 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterA
                                 mask = (1u << kRasterWarps) - 1u;   // a NaN extent reaches every item, as
                             }                                       // the comparisons it fails would say
                             if (mask) {
-                                s_f[0][tid] = ra.x; s_f[1][tid] = ra.y;
-                                s_f[2][tid] = A; s_f[3][tid] = B; s_f[4][tid] = C; s_f[5][tid] = al;
-                                s_f[6][tid] = cr; s_f[7][tid] = cg; s_f[8][tid] = cb;
+                                s_fa[tid] = make_float4(-ra.x, -ra.y, -0.72134752044448170f * A,
+                                                        -1.4426950408889634f * B);
+                                s_fb[tid] = make_float4(-0.72134752044448170f * C, -al, -fminf(cr, 3.402823466e38f),
+                                                        -fminf(cg, 3.402823466e38f));
+                                s_fc[tid] = -fminf(cb, 3.402823466e38f);
                             }
                         }
                     }
@@ -1774,9 +1791,7 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterA
                         const uint32_t i = c + (uint32_t)h * 32u + (uint32_t)lane;
                         const bool hit = i < nb && ((s_m[i] >> warp) & 1u);
                         const uint32_t m = __ballot_sync(0xffffffffu, hit);
-                        if (hit)
-                            put_pair_slot(sp, n + __popc(m & lmask), s_f[0][i], s_f[1][i], s_f[2][i], s_f[3][i],
-                                          s_f[4][i], s_f[5][i], s_f[6][i], s_f[7][i], s_f[8][i]);
+                        if (hit) put_pair_slot_raw(sp, n + __popc(m & lmask), s_fa[i], s_fb[i], s_fc[i]);
                         n += __popc(m);
                     }
                     if (n == 0u) continue;
