@@ -186,22 +186,22 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
             }
             if (M) {
                 // in the same ranges: copies issued later on other streams (a
-                // frame's view tables) queue behind one copy at most
+                // frame's view tables) queue behind one copy at most.  The
+                // copies run back to back; the 16-bit conversion of all splats
+                // follows them in one launch (a conversion between two copies
+                // would hold the next copy until it has run beside the frame)
                 for (int k = 0; k < kUploadChunks; k++) {
                     const uint64_t g0 = chunks->bounds[k], g1 = chunks->bounds[k + 1];
                     if (g1 == g0) continue;
                     const uint64_t e = 12ull * M;
-                    if (precision == DL_PREC_F32) {
-                        DL_CK(cudaMemcpyAsync(b + oSh + e * g0, (const char*)d->colors_sh + e * g0, e * (g1 - g0),
-                                              cudaMemcpyHostToDevice, st));
-                    } else {
-                        DL_CK(cudaMemcpyAsync(b + oTmp + e * g0, (const char*)d->colors_sh + e * g0, e * (g1 - g0),
-                                              cudaMemcpyHostToDevice, st));
-                        sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp) + 3ull * M * g0,
-                                                           (uint16_t*)(b + oSh) + (uint64_t)P16 * g0, g1 - g0, M,
-                                                           (int)P16, precision);
-                        DL_CK(cudaGetLastError());
-                    }
+                    DL_CK(cudaMemcpyAsync(b + (precision == DL_PREC_F32 ? oSh : oTmp) + e * g0,
+                                          (const char*)d->colors_sh + e * g0, e * (g1 - g0),
+                                          cudaMemcpyHostToDevice, st));
+                }
+                if (precision != DL_PREC_F32) {
+                    sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp), (uint16_t*)(b + oSh), n, M,
+                                                       (int)P16, precision);
+                    DL_CK(cudaGetLastError());
                 }
                 DL_CK(cudaEventRecord(chunks->sh_event, st));
             }
@@ -259,6 +259,8 @@ struct FramePtrs {
     // a scene upload still in flight: projection per splat range after its event
     const DlUploadChunks* upload;
     uint32_t* visMask;             // colours deferred until the SH has arrived (upload->sh_event)
+    cudaStream_t colStream;        // with visMask: colour_k runs there, beside the sorts and binning
+    cudaEvent_t colEv[2];          // [0] projection done (on the frame's stream), [1] colours done
     // host outputs read back per view range while the next range rasterizes
     int rbGroups;                  // 0: one rasterizer launch, no read-back here
     uint8_t* const* rbHost;        // [V] host destinations
@@ -455,6 +457,26 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
         (*launches)++;
     }
     DL_CK(cudaGetLastError());
+    // deferred colours, once the SH has arrived, on a stream of their own: they
+    // run while the frame's stream sorts and bins; the rasterizer waits for them
+    if (f.visMask && d.N) {
+        DL_CK(cudaEventRecord(f.colEv[0], st));
+        DL_CK(cudaStreamWaitEvent(f.colStream, f.colEv[0], 0));
+        DL_CK(cudaStreamWaitEvent(f.colStream, f.upload->sh_event, 0));
+        dlr::ColourArgs ca;
+        ca.sc = sc;
+        ca.views = f.views;
+        ca.num_views = d.V;
+        ca.view_stride = d.stride;
+        ca.vis_mask = f.visMask;
+        ca.recBC = d.f16rec ? nullptr : f.recBC;
+        ca.recH = d.f16rec ? f.recH : nullptr;
+        if (d.fastExp) dlr::colour_k<true><<<(d.N + 255) / 256, 256, 0, f.colStream>>>(ca);
+        else dlr::colour_k<false><<<(d.N + 255) / 256, 256, 0, f.colStream>>>(ca);
+        (*launches)++;
+        DL_CK(cudaGetLastError());
+        DL_CK(cudaEventRecord(f.colEv[1], f.colStream));
+    }
     rec_event(ev, 1, st);
     // depth sort: stable LSD, 4 x 8-bit digits, one segment per view
     if (d.N) {
@@ -599,22 +621,8 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     (*launches)++;
     DL_CK(cudaGetLastError());
 
-    // deferred colours, once the SH has arrived
-    if (f.visMask && d.N) {
-        DL_CK(cudaStreamWaitEvent(st, f.upload->sh_event, 0));
-        dlr::ColourArgs ca;
-        ca.sc = sc;
-        ca.views = f.views;
-        ca.num_views = d.V;
-        ca.view_stride = d.stride;
-        ca.vis_mask = f.visMask;
-        ca.recBC = d.f16rec ? nullptr : f.recBC;
-        ca.recH = d.f16rec ? f.recH : nullptr;
-        if (d.fastExp) dlr::colour_k<true><<<(d.N + 255) / 256, 256, 0, st>>>(ca);
-        else dlr::colour_k<false><<<(d.N + 255) / 256, 256, 0, st>>>(ca);
-        (*launches)++;
-        DL_CK(cudaGetLastError());
-    }
+    // the deferred colours (launched after the projection) are complete
+    if (f.visMask && d.N) DL_CK(cudaStreamWaitEvent(st, f.colEv[1], 0));
 
     // learned schedule: per-tile features, predicted cost, tiles in decreasing order
     const uint32_t* work = f.work;
@@ -891,6 +899,12 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         if (f.upload && f.upload->sh_separate) {
             DL_TRY(r->visMask.ensure(4ull * ((V + 31) / 32) * std::max<uint32_t>(N, 1)));
             f.visMask = r->visMask.as<uint32_t>();
+            if (!r->colour_stream) DL_CK(cudaStreamCreateWithFlags(&r->colour_stream, cudaStreamNonBlocking));
+            for (auto& e : r->colour_ev)
+                if (!e) DL_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            f.colStream = r->colour_stream;
+            f.colEv[0] = r->colour_ev[0];
+            f.colEv[1] = r->colour_ev[1];
         }
         if (overlap->groups > 1 && V > 1) {
             rbTileBase.assign(hTileBase, hTileBase + V + 1);
