@@ -410,6 +410,24 @@ class VoxelizeResult:
     stageTimes: Optional[dict] = None          # device ms per stage with opts["profile"]
 
 
+def voxelQuery(device: Device, result: VoxelizeResult, points) -> np.ndarray:
+    """Occupancy of points (n x 3 float32) against a voxelize result, on the device
+    (dl_vox_query; no counterpart in the reference, whose BlockMaskBuffer.get
+    answers one block at a time on the CPU).  Returns n uint8: 1 where the
+    point's voxel floor((p - bounds.min) / voxelResolution) is solid."""
+    pts = np.ascontiguousarray(np.asarray(points, np.float32).reshape(-1, 3))
+    out = np.zeros(len(pts), np.uint8)
+    buf = result.buffer
+    idx = np.ascontiguousarray(buf.blockIdx, np.uint32)
+    lo = np.ascontiguousarray(buf.maskLo, np.uint32)
+    hi = np.ascontiguousarray(buf.maskHi, np.uint32)
+    bmin = (ctypes.c_double * 3)(*[float(x) for x in result.bounds.min])
+    dims = (ctypes.c_double * 3)(float(result.numBlocksX), float(result.numBlocksY), float(result.numBlocksZ))
+    check(_lib.load().dl_vox_query(device.handle, idx.ctypes.data, lo.ctypes.data, hi.ctypes.data, len(idx), bmin,
+                                   float(result.voxelResolution), dims, pts.ctypes.data, len(pts), out.ctypes.data))
+    return out
+
+
 def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> VoxelizeResult:
     """voxelize.ts:59-248.  opts: {voxelResolution=0.05, opacityCutoff=0.1, bounds}.
 

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdroplet_b200.so")
-SOURCES = ["dl_api.cu", "dl_render.cu", "dl_voxel.cu", "dl_mlp.cu", "dl_sorter.cu", "dl_ply.cu"]
+SOURCES = ["dl_api.cu", "dl_render.cu", "dl_voxel.cu", "dl_mlp.cu", "dl_sorter.cu", "dl_ply.cu", "dl_query.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false",
               "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-ffp-contract=off"]
 

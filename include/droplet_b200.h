@@ -256,6 +256,20 @@ int dl_vox_result_info(const dl_vox_result* res, double bounds_min[3], double bo
  * flat block index, low 32 voxel bits, high 32 voxel bits. */
 int dl_vox_result_copy(const dl_vox_result* res, uint32_t* block_idx, uint32_t* mask_lo, uint32_t* mask_hi);
 int dl_vox_result_free(dl_vox_result* res);
+/* No counterpart in the reference (its BlockMaskBuffer answers get(blockIdx) one
+ * block at a time on the CPU, src/voxel/block-mask-buffer.ts:41-58): occupancy of
+ * npoints points (x, y, z f32, host memory) against a block-mask buffer (the
+ * arrays dl_vox_result_copy returns, or any BlockMaskBuffer's; a block listed
+ * twice is OR-merged as addBlock does), on the device — a collision test against
+ * the voxelizer's output.  A point lies in voxel floor((p - bounds_min) /
+ * voxel_resolution) per axis (f64); out[i] (host) = 1 when that voxel's bit is
+ * set in its block (flat index bx + by*dims[0] + bz*dims[0]*dims[1], bit
+ * (z&3)*16 + (y&3)*4 + (x&3) of the voxel in the block, lo = bits 0-31), else 0,
+ * also for points outside the 4*dims voxel grid, non-finite points and an
+ * empty grid.  Synchronous; device memory is allocated for the call. */
+int dl_vox_query(dl_device* dev, const uint32_t* block_idx, const uint32_t* mask_lo, const uint32_t* mask_hi,
+                 uint64_t nblocks, const double bounds_min[3], double voxel_resolution, const double dims[3],
+                 const float* points, uint64_t npoints, uint8_t* out);
 /* Learned block order (no reference counterpart: the reference evaluates
  * batches in dispatch order, voxelize.ts:186-248).  With a model attached,
  * dl_voxelize on this device evaluates blocks in decreasing cost predicted

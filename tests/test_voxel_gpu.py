@@ -147,3 +147,69 @@ def test_fast_exp_differs_only_near_the_cutoff(device):
         differing += bin(a[0] ^ b[0]).count("1") + bin(a[1] ^ b[1]).count("1")
     print(f"fast exp: {differing} bits differ from the canonical order, all within the {o['near_bits']} bits "
           f"with |alpha - cutoff| < {eps}")
+
+
+def _query_reference(idx, lo, hi, bmin, res, dims, pts):
+    """Occupancy of points by the BlockMaskBuffer rules (block-mask-buffer.ts:41-58,
+    duplicates OR-merged as addBlock does) and the voxel grid of voxelize.ts:160-179."""
+    table = {}
+    for b, l, h in zip(idx.tolist(), lo.tolist(), hi.tolist()):
+        ol, oh = table.get(b, (0, 0))
+        table[b] = (ol | l, oh | h)
+    out = np.zeros(len(pts), np.uint8)
+    if not all(math.isfinite(x) for x in list(bmin) + list(dims)) or min(dims) < 1:
+        return out
+    with np.errstate(invalid="ignore"):
+        v = np.floor((pts.astype(np.float64) - np.asarray(bmin, np.float64)) / res)
+        inside = np.all((v >= 0) & (v < 4 * np.asarray(dims, np.float64)), axis=1)
+    for i in np.nonzero(inside)[0]:
+        x, y, z = (int(c) for c in v[i])
+        flat = (x >> 2) + (y >> 2) * int(dims[0]) + (z >> 2) * int(dims[0]) * int(dims[1])
+        if flat in table:
+            bit = (z & 3) * 16 + (y & 3) * 4 + (x & 3)
+            l, h = table[flat]
+            out[i] = (l >> bit) & 1 if bit < 32 else (h >> (bit - 32)) & 1
+    return out
+
+
+def test_point_queries_match_the_block_mask_buffer(device):
+    # dl_vox_query (collision tests against the voxelizer's output) against the
+    # BlockMaskBuffer rules on the CPU: random points around the grid, the centres
+    # of listed blocks' voxels, non-finite points and the grid's edges
+    d = synth.voxel_1m(40_000)
+    res = dl.voxelize(device, d, {"voxelResolution": 0.1, "opacityCutoff": 0.1})
+    buf = res.buffer
+    assert buf.count > 1000
+    bmin, bmax = np.asarray(res.bounds.min, np.float64), np.asarray(res.bounds.max, np.float64)
+    dims = (res.numBlocksX, res.numBlocksY, res.numBlocksZ)
+    rng = np.random.default_rng(5)
+    span = bmax - bmin
+    p1 = rng.uniform(bmin - 0.1 * span, bmax + 0.1 * span, (60_000, 3))
+    pick = rng.integers(0, buf.count, 40_000)
+    b = buf.blockIdx[pick].astype(np.int64)
+    nx, ny = int(dims[0]), int(dims[1])
+    bx, by, bz = b % nx, (b // nx) % ny, b // (nx * ny)
+    local = rng.integers(0, 4, (40_000, 3))
+    vox = np.stack([bx, by, bz], 1) * 4 + local
+    p2 = bmin + (vox + 0.5) * 0.1
+    p3 = np.array([[np.nan, 0, 0], [np.inf, 0, 0], [0, -np.inf, 0], list(bmin), list(bmax)], np.float64)
+    pts = np.concatenate([p1, p2, p3]).astype(np.float32)
+    got = dl.voxelQuery(device, res, pts)
+    want = _query_reference(buf.blockIdx, buf.maskLo, buf.maskHi, bmin, 0.1, dims, pts)
+    assert np.array_equal(got, want)
+    assert 0 < got.sum() < len(pts)
+    # a buffer listing blocks twice, their bits split between the copies: OR-merged
+    k = min(500, buf.count)
+    split = dl.BlockMaskBuffer(np.concatenate([buf.blockIdx, buf.blockIdx[:k]]),
+                               np.concatenate([buf.maskLo & np.uint32(0x0000ffff), buf.maskLo[:k]]),
+                               np.concatenate([buf.maskHi, np.zeros(k, np.uint32)]))
+    merged = dl.BlockMaskBuffer(buf.blockIdx, np.concatenate([buf.maskLo[:k], buf.maskLo[k:] & np.uint32(0x0000ffff)]),
+                                buf.maskHi)
+    r2 = dl.VoxelizeResult(split, res.bounds, res.voxelResolution, *dims)
+    r3 = dl.VoxelizeResult(merged, res.bounds, res.voxelResolution, *dims)
+    assert np.array_equal(dl.voxelQuery(device, r2, pts), dl.voxelQuery(device, r3, pts))
+    assert np.array_equal(dl.voxelQuery(device, r2, pts),
+                          _query_reference(split.blockIdx, split.maskLo, split.maskHi, bmin, 0.1, dims, pts))
+    # an empty scene: bounds +-Infinity, nothing solid
+    empty = dl.voxelize(device, SplatData.empty(), {"voxelResolution": 0.1})
+    assert not dl.voxelQuery(device, empty, pts).any()
