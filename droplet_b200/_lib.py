@@ -45,7 +45,7 @@ EXPORTS = [
     "dl_renderer_set_tuning", "dl_renderer_get_tuning", "dl_renderer_autotune",
     "dl_device_set_voxel_scheduler", "dl_vox_result_block_log", "dl_test_set_wait_limit",
     "dl_test_withhold_status", "dl_test_fail_allocation", "dl_ply_load", "dl_ply_splats", "dl_ply_free",
-    "dl_vox_result_stage_times", "dl_vox_query",
+    "dl_vox_result_stage_times", "dl_vox_query", "dl_vox_carve",
 ]
 
 
@@ -146,6 +146,7 @@ def load():
         "dl_vox_result_stage_times": [vp, P(ctypes.c_double), i],
         "dl_vox_query": [vp, vp, vp, vp, ctypes.c_uint64, P(ctypes.c_double), ctypes.c_double, P(ctypes.c_double),
                          vp, ctypes.c_uint64, vp],
+        "dl_vox_carve": [vp, vp, vp, vp, ctypes.c_uint64, vp, vp, vp, ctypes.c_uint64, vp, vp, vp, P(ctypes.c_uint64)],
         "dl_renderer_autotune": [vp, vp, P(DlCamera), i, P(ctypes.c_float), ctypes.c_uint32, i, P(DlTuning),
                                  P(ctypes.c_double)],
     }

@@ -428,6 +428,25 @@ def voxelQuery(device: Device, result: VoxelizeResult, points) -> np.ndarray:
     return out
 
 
+def voxelCarve(device: Device, a: BlockMaskBuffer, b: BlockMaskBuffer) -> BlockMaskBuffer:
+    """A minus B, block by block, on the device (dl_vox_carve; voxelize.ts:1-14
+    names carve among the buffer's downstream stages, which the reference does not
+    build).  Each of A's blocks keeps the bits B's blocks with the same index do
+    not set; blocks left empty are dropped, the rest keep A's order."""
+    cols = []
+    for buf in (a, b):
+        cols.append([np.ascontiguousarray(c, np.uint32) for c in (buf.blockIdx, buf.maskLo, buf.maskHi)])
+    (ai, al, ah), (bi, bl, bh) = cols
+    na = len(ai)
+    oi, ol, oh = (np.zeros(max(na, 1), np.uint32) for _ in range(3))
+    n = ctypes.c_uint64(0)
+    check(_lib.load().dl_vox_carve(device.handle, ai.ctypes.data, al.ctypes.data, ah.ctypes.data, na,
+                                   bi.ctypes.data, bl.ctypes.data, bh.ctypes.data, len(bi),
+                                   oi.ctypes.data, ol.ctypes.data, oh.ctypes.data, ctypes.byref(n)))
+    k = n.value
+    return BlockMaskBuffer(oi[:k].copy(), ol[:k].copy(), oh[:k].copy())
+
+
 def voxelize(device: Device, data: SplatData, opts: Optional[dict] = None) -> VoxelizeResult:
     """voxelize.ts:59-248.  opts: {voxelResolution=0.05, opacityCutoff=0.1, bounds}.
 

@@ -162,3 +162,149 @@ extern "C" int dl_vox_query(dl_device* dev, const uint32_t* block_idx, const uin
     }
     return DL_OK;
 }
+
+// ---- carve: A minus B, block by block
+// Each listed block of A keeps the bits that B's blocks (OR-merged) do not
+// set; blocks left empty are dropped and the others keep A's order (the order
+// voxelize returns), so carving an empty B returns A's non-empty blocks as they
+// are.  Two kernels around one host scan of per-CTA counts: the first computes
+// every entry's carved masks and its CTA's count of non-empty entries, the
+// second writes the kept entries at their CTA's offset plus their rank in it.
+namespace {
+
+constexpr int kCarveThreads = 256;
+
+__device__ __forceinline__ void lookup_masks(uint32_t key, const uint32_t* keys, const uint32_t* tlo,
+                                             const uint32_t* thi, uint32_t mask, uint32_t& lo, uint32_t& hi) {
+    lo = 0u;
+    hi = 0u;
+    uint32_t s = slot_of(key, mask);
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+        const uint32_t k = keys[s];
+        if (k == key) { lo = tlo[s]; hi = thi[s]; return; }
+        if (k == kEmpty) return;
+        s = (s + 1u) & mask;
+    }
+}
+
+__global__ void __launch_bounds__(kCarveThreads) carve_count_k(const uint32_t* __restrict__ idx,
+                                                               uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
+                                                               uint64_t n, const uint32_t* keys, const uint32_t* tlo,
+                                                               const uint32_t* thi, uint32_t mask, uint32_t* counts) {
+    const uint64_t i = blockIdx.x * (uint64_t)kCarveThreads + threadIdx.x;
+    bool keep = false;
+    if (i < n) {
+        uint32_t bl, bh;
+        lookup_masks(idx[i], keys, tlo, thi, mask, bl, bh);
+        const uint32_t l = lo[i] & ~bl, h = hi[i] & ~bh;
+        lo[i] = l;
+        hi[i] = h;
+        keep = (l | h) != 0u;
+    }
+    const int c = __syncthreads_count(keep);
+    if (threadIdx.x == 0) counts[blockIdx.x] = (uint32_t)c;
+}
+
+__global__ void __launch_bounds__(kCarveThreads) carve_write_k(const uint32_t* __restrict__ idx,
+                                                               const uint32_t* __restrict__ lo,
+                                                               const uint32_t* __restrict__ hi, uint64_t n,
+                                                               const uint64_t* __restrict__ offs, uint32_t* oidx,
+                                                               uint32_t* olo, uint32_t* ohi) {
+    __shared__ uint32_t s_w[kCarveThreads / 32];
+    const uint64_t i = blockIdx.x * (uint64_t)kCarveThreads + threadIdx.x;
+    const bool keep = i < n && (lo[i] | hi[i]) != 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t b = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_w[warp] = (uint32_t)__popc(b);
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; w++) before += s_w[w];
+    if (keep) {
+        const uint64_t o = offs[blockIdx.x] + before + (uint32_t)__popc(b & dl_lanemask_lt());
+        oidx[o] = idx[i];
+        olo[o] = lo[i];
+        ohi[o] = hi[i];
+    }
+}
+
+}  // namespace
+
+extern "C" int dl_vox_carve(dl_device* dev, const uint32_t* a_idx, const uint32_t* a_lo, const uint32_t* a_hi,
+                            uint64_t na, const uint32_t* b_idx, const uint32_t* b_lo, const uint32_t* b_hi,
+                            uint64_t nb, uint32_t* out_idx, uint32_t* out_lo, uint32_t* out_hi, uint64_t* out_n) {
+    if (!dev || !out_n || (na && (!a_idx || !a_lo || !a_hi || !out_idx || !out_lo || !out_hi)) ||
+        (nb && (!b_idx || !b_lo || !b_hi))) {
+        dl_set_error("dl_vox_carve: NULL argument");
+        return DL_E_INVALID_ARG;
+    }
+    *out_n = 0;
+    if (na == 0) return DL_OK;
+    if (na >= (1ull << 30) || nb >= (1ull << 30)) { dl_set_error("dl_vox_carve: at most 2^30 - 1 blocks"); return DL_E_CAPACITY; }
+    DL_CK(cudaSetDevice(dev->ordinal));
+    cudaStream_t st = dev->stream;
+    uint32_t cap = 1;
+    while (cap < 2 * std::max<uint64_t>(nb, 1)) cap <<= 1;
+    const uint64_t ctas = (na + kCarveThreads - 1) / kCarveThreads;
+    DevBuf dAi, dAl, dAh, dBi, dBl, dBh, dKeys, dTlo, dThi, dCnt, dOff, dOi, dOl, dOh;
+    auto cleanup = [&]() {
+        for (DevBuf* b : {&dAi, &dAl, &dAh, &dBi, &dBl, &dBh, &dKeys, &dTlo, &dThi, &dCnt, &dOff, &dOi, &dOl, &dOh})
+            b->release();
+    };
+    int rc = DL_OK;
+    if ((rc = dAi.ensure(4 * na)) != DL_OK || (rc = dAl.ensure(4 * na)) != DL_OK || (rc = dAh.ensure(4 * na)) != DL_OK ||
+        (rc = dBi.ensure(4 * std::max<uint64_t>(nb, 1))) != DL_OK || (rc = dBl.ensure(4 * std::max<uint64_t>(nb, 1))) != DL_OK ||
+        (rc = dBh.ensure(4 * std::max<uint64_t>(nb, 1))) != DL_OK || (rc = dKeys.ensure(4ull * cap)) != DL_OK ||
+        (rc = dTlo.ensure(4ull * cap)) != DL_OK || (rc = dThi.ensure(4ull * cap)) != DL_OK ||
+        (rc = dCnt.ensure(4 * ctas)) != DL_OK || (rc = dOff.ensure(8 * ctas)) != DL_OK ||
+        (rc = dOi.ensure(4 * na)) != DL_OK || (rc = dOl.ensure(4 * na)) != DL_OK || (rc = dOh.ensure(4 * na)) != DL_OK) {
+        cleanup();
+        return rc;
+    }
+    cudaError_t e = cudaSuccess;
+    auto ck = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    ck(cudaMemcpyAsync(dAi.p, a_idx, 4 * na, cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(dAl.p, a_lo, 4 * na, cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(dAh.p, a_hi, 4 * na, cudaMemcpyHostToDevice, st));
+    if (nb) {
+        ck(cudaMemcpyAsync(dBi.p, b_idx, 4 * nb, cudaMemcpyHostToDevice, st));
+        ck(cudaMemcpyAsync(dBl.p, b_lo, 4 * nb, cudaMemcpyHostToDevice, st));
+        ck(cudaMemcpyAsync(dBh.p, b_hi, 4 * nb, cudaMemcpyHostToDevice, st));
+    }
+    ck(cudaMemsetAsync(dKeys.p, 0xff, 4ull * cap, st));
+    ck(cudaMemsetAsync(dTlo.p, 0, 4ull * cap, st));
+    ck(cudaMemsetAsync(dThi.p, 0, 4ull * cap, st));
+    if (nb) {
+        const uint32_t gi = (uint32_t)std::min<uint64_t>((nb + 255) / 256, 64ull * dev->sm_count);
+        query_insert_k<<<gi, 256, 0, st>>>(dBi.as<uint32_t>(), dBl.as<uint32_t>(), dBh.as<uint32_t>(), nb,
+                                           dKeys.as<uint32_t>(), dTlo.as<uint32_t>(), dThi.as<uint32_t>(), cap - 1);
+        ck(cudaGetLastError());
+    }
+    carve_count_k<<<(uint32_t)ctas, kCarveThreads, 0, st>>>(dAi.as<uint32_t>(), dAl.as<uint32_t>(), dAh.as<uint32_t>(),
+                                                           na, dKeys.as<uint32_t>(), dTlo.as<uint32_t>(),
+                                                           dThi.as<uint32_t>(), cap - 1, dCnt.as<uint32_t>());
+    ck(cudaGetLastError());
+    std::vector<uint32_t> cnt(ctas);
+    std::vector<uint64_t> off(ctas);
+    ck(cudaMemcpyAsync(cnt.data(), dCnt.p, 4 * ctas, cudaMemcpyDeviceToHost, st));
+    ck(cudaStreamSynchronize(st));
+    uint64_t total = 0;
+    for (uint64_t c = 0; c < ctas; c++) { off[c] = total; total += cnt[c]; }
+    if (e == cudaSuccess && total) {
+        ck(cudaMemcpyAsync(dOff.p, off.data(), 8 * ctas, cudaMemcpyHostToDevice, st));
+        carve_write_k<<<(uint32_t)ctas, kCarveThreads, 0, st>>>(dAi.as<uint32_t>(), dAl.as<uint32_t>(),
+                                                               dAh.as<uint32_t>(), na, dOff.as<uint64_t>(),
+                                                               dOi.as<uint32_t>(), dOl.as<uint32_t>(), dOh.as<uint32_t>());
+        ck(cudaGetLastError());
+        ck(cudaMemcpyAsync(out_idx, dOi.p, 4 * total, cudaMemcpyDeviceToHost, st));
+        ck(cudaMemcpyAsync(out_lo, dOl.p, 4 * total, cudaMemcpyDeviceToHost, st));
+        ck(cudaMemcpyAsync(out_hi, dOh.p, 4 * total, cudaMemcpyDeviceToHost, st));
+        ck(cudaStreamSynchronize(st));
+    }
+    cleanup();
+    if (e != cudaSuccess) {
+        dl_set_error(std::string("dl_vox_carve: ") + cudaGetErrorString(e));
+        return DL_E_CUDA;
+    }
+    *out_n = total;
+    return DL_OK;
+}

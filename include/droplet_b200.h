@@ -270,6 +270,16 @@ int dl_vox_result_free(dl_vox_result* res);
 int dl_vox_query(dl_device* dev, const uint32_t* block_idx, const uint32_t* mask_lo, const uint32_t* mask_hi,
                  uint64_t nblocks, const double bounds_min[3], double voxel_resolution, const double dims[3],
                  const float* points, uint64_t npoints, uint8_t* out);
+/* No counterpart in the reference (its voxelize.ts:1-14 names carve among the
+ * downstream stages of the block-mask buffer without building it): A minus B,
+ * block by block, on the device.  Each of A's na entries (host arrays as
+ * dl_vox_result_copy returns them) keeps the bits that B's entries with the same
+ * flat index (OR-merged) do not set; entries left empty are dropped and the rest
+ * keep A's order.  out_idx/out_lo/out_hi (host) hold na entries; *out_n gets the
+ * count written.  Synchronous; device memory is allocated for the call. */
+int dl_vox_carve(dl_device* dev, const uint32_t* a_idx, const uint32_t* a_lo, const uint32_t* a_hi, uint64_t na,
+                 const uint32_t* b_idx, const uint32_t* b_lo, const uint32_t* b_hi, uint64_t nb, uint32_t* out_idx,
+                 uint32_t* out_lo, uint32_t* out_hi, uint64_t* out_n);
 /* Learned block order (no reference counterpart: the reference evaluates
  * batches in dispatch order, voxelize.ts:186-248).  With a model attached,
  * dl_voxelize on this device evaluates blocks in decreasing cost predicted

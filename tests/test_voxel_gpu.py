@@ -213,3 +213,53 @@ def test_point_queries_match_the_block_mask_buffer(device):
     # an empty scene: bounds +-Infinity, nothing solid
     empty = dl.voxelize(device, SplatData.empty(), {"voxelResolution": 0.1})
     assert not dl.voxelQuery(device, empty, pts).any()
+
+
+def _carve_reference(a, b):
+    """A minus B block by block: B's entries OR-merged by index, each of A's entries
+    keeps the bits B's do not set, empty entries dropped, A's order kept."""
+    table = {}
+    for k, l, h in zip(b.blockIdx.tolist(), b.maskLo.tolist(), b.maskHi.tolist()):
+        ol, oh = table.get(k, (0, 0))
+        table[k] = (ol | l, oh | h)
+    out = ([], [], [])
+    for k, l, h in zip(a.blockIdx.tolist(), a.maskLo.tolist(), a.maskHi.tolist()):
+        bl, bh = table.get(k, (0, 0))
+        l, h = l & ~bl & 0xffffffff, h & ~bh & 0xffffffff
+        if l or h:
+            out[0].append(k)
+            out[1].append(l)
+            out[2].append(h)
+    return [np.asarray(c, np.uint32) for c in out]
+
+
+@pytest.mark.gpu
+def test_carve_matches_the_block_rules(device):
+    # dl_vox_carve against the CPU rules: the shell left when a high-cutoff
+    # voxelization is carved out of a low-cutoff one, a B with duplicate and
+    # absent blocks, and the empty cases
+    d = synth.voxel_1m(40_000)
+    lo_cut = dl.voxelize(device, d, {"voxelResolution": 0.1, "opacityCutoff": 0.1}).buffer
+    hi_cut = dl.voxelize(device, d, {"voxelResolution": 0.1, "opacityCutoff": 0.4}).buffer
+    assert lo_cut.count > 1000 and hi_cut.count > 100
+
+    def same(got, want):
+        assert np.array_equal(got.blockIdx, want[0])
+        assert np.array_equal(got.maskLo, want[1])
+        assert np.array_equal(got.maskHi, want[2])
+
+    shell = dl.voxelCarve(device, lo_cut, hi_cut)
+    same(shell, _carve_reference(lo_cut, hi_cut))
+    assert 0 < shell.count <= lo_cut.count
+    rng = np.random.default_rng(11)
+    n = lo_cut.count
+    pick = rng.integers(0, n, 3 * n // 2)
+    absent = np.arange(10**6, 10**6 + 300, dtype=np.uint32)
+    b = dl.BlockMaskBuffer(np.concatenate([lo_cut.blockIdx[pick], absent]),
+                           rng.integers(0, 2**32, len(pick) + 300, dtype=np.uint64).astype(np.uint32),
+                           rng.integers(0, 2**32, len(pick) + 300, dtype=np.uint64).astype(np.uint32))
+    same(dl.voxelCarve(device, lo_cut, b), _carve_reference(lo_cut, b))
+    empty = dl.BlockMaskBuffer()
+    same(dl.voxelCarve(device, lo_cut, empty), (lo_cut.blockIdx, lo_cut.maskLo, lo_cut.maskHi))
+    assert dl.voxelCarve(device, lo_cut, lo_cut).count == 0
+    assert dl.voxelCarve(device, empty, lo_cut).count == 0
