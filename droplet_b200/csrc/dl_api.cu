@@ -238,9 +238,12 @@ extern "C" int dl_render_many(dl_renderer* r, const dl_splats* data, const dl_ca
     // each range starts when it has arrived
     DL_TRY(ensure_copy_stream(r));
     DlUploadChunks up;
-    for (int k = 0; k <= kUploadChunks; k++)
-        if (!r->upload_events[k]) DL_CK(cudaEventCreateWithFlags(&r->upload_events[k], cudaEventDisableTiming));
-    for (int k = 0; k < kUploadChunks; k++) up.events[k] = r->upload_events[k];
+    for (auto& e : r->upload_events)
+        if (!e) DL_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (int k = 0; k < kUploadChunks; k++) {
+        up.events[k] = r->upload_events[k];
+        up.sh_events[k] = r->upload_events[kUploadChunks + 1 + k];
+    }
     up.sh_event = r->upload_events[kUploadChunks];
     // the previous frame's kernels may still read the scene buffer
     DL_CK(cudaEventRecord(r->copy_event, r->stream));
@@ -285,7 +288,10 @@ int render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, cons
     if (upload && !overlapped) {
         if (!upload->issued) DL_TRY(upload->issue());
         DL_CK(cudaStreamWaitEvent(r->stream, upload->events[upload->count - 1], 0));
-        if (upload->sh_separate) DL_CK(cudaStreamWaitEvent(r->stream, upload->sh_event, 0));
+        if (upload->sh_separate) {
+            DL_CK(cudaStreamWaitEvent(r->stream, upload->sh_event, 0));
+            DL_TRY(dl_upload_convert_sh(upload, 0, upload->bounds[upload->count], r->stream, nullptr));
+        }
     }
     if (flags & DL_BATCH_PLAIN) {
         for (int i = 0; i < n; i++) {

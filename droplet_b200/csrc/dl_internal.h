@@ -169,11 +169,11 @@ struct dl_renderer {
     cudaEvent_t copy_event = nullptr;
     // deferred colours run beside the sorts: their stream and events (projected, coloured)
     cudaStream_t colour_stream = nullptr;
-    cudaEvent_t colour_ev[2] = {nullptr, nullptr};
+    cudaEvent_t colour_ev[kUploadChunks + 1] = {};      // [c] splat range c projected, [last] colours done
     // host-output frames: the odd rasterizer view ranges run on a second stream
     cudaStream_t raster_stream = nullptr;
     cudaEvent_t raster_ev[2] = {nullptr, nullptr};
-    cudaEvent_t upload_events[kUploadChunks + 1] = {};   // geometry chunks, then the SH
+    cudaEvent_t upload_events[2 * kUploadChunks + 1] = {};   // geometry chunks, SH chunks, all SH
 };
 
 struct dl_mlp;
@@ -187,13 +187,20 @@ const void* dl_mlp_weights(const dl_mlp* mlp);   // device BF16 parameters
 // complete when sh_event has fired (sh_separate = 1), so that frames can defer
 // colours until then.  dl_upload_scene lays the scene out and returns; the
 // frame calls issue() once its own small host-to-device copies are queued, so
-// that they do not wait behind the upload.
+// that they do not wait behind the upload.  The SH arrives chunk by chunk as
+// f32 at sh_src (sh_events[c]: chunk c's coefficients are there); with a
+// 16-bit scene (sh_dst set) the frame converts them to the scene's layout
+// (sh_P halves per splat, dl_upload_convert_sh) once they have arrived.
 struct DlUploadChunks {
     int count;
     uint32_t bounds[kUploadChunks + 1];
     cudaEvent_t events[kUploadChunks];
     int sh_separate;
     cudaEvent_t sh_event;
+    cudaEvent_t sh_events[kUploadChunks];
+    const float* sh_src = nullptr;
+    uint16_t* sh_dst = nullptr;
+    int sh_M = 0, sh_P = 0, sh_kind = 0;
     std::function<int()> issue;
     bool issued = false;
 };
@@ -213,3 +220,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hviews, 
 int dl_upload_scene(dl_scene* s, const dl_splats* data, int precision, cudaStream_t stream,
                     DlUploadChunks* chunks = nullptr);
 int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlView* out);
+// Converts splats [g0, g1) of a chunked upload's SH to the scene's 16-bit
+// layout on st (nothing for an f32 scene); the caller orders it after the
+// chunks' sh_events.
+int dl_upload_convert_sh(const DlUploadChunks* up, uint32_t g0, uint32_t g1, cudaStream_t st, uint64_t* launches);

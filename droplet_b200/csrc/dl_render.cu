@@ -121,6 +121,16 @@ int dl_make_view(const dl_camera* cam, const float bg[4], uint32_t maxCov, DlVie
     return DL_OK;
 }
 
+int dl_upload_convert_sh(const DlUploadChunks* up, uint32_t g0, uint32_t g1, cudaStream_t st, uint64_t* launches) {
+    if (!up->sh_dst || g1 <= g0) return DL_OK;
+    sh_to_half_k<<<std::min<uint32_t>((g1 - g0 + 31) / 32, 1024), 256, 0, st>>>(
+        up->sh_src + 3ull * up->sh_M * g0, up->sh_dst + (uint64_t)up->sh_P * g0, g1 - g0, up->sh_M, up->sh_P,
+        up->sh_kind);
+    if (launches) (*launches)++;
+    DL_CK(cudaGetLastError());
+    return DL_OK;
+}
+
 int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t st, DlUploadChunks* chunks) {
     if (!d) { dl_set_error("splats is NULL"); return DL_E_INVALID_ARG; }
     if (d->sh_bands < 0 || d->sh_bands > 3) { dl_set_error("sh_bands must be 0..3"); return DL_E_INVALID_ARG; }
@@ -173,10 +183,16 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
     };
     if (chunks) {
         // the geometry in equal splat ranges, each followed by its event; then
-        // the SH of all splats (the bulk of the bytes), followed by sh_event
+        // the SH (the bulk of the bytes) in the same ranges, each followed by
+        // its event, and sh_event after all of them
         chunks->count = kUploadChunks;
         chunks->sh_separate = M > 0;
         chunks->issued = false;
+        chunks->sh_src = M ? (const float*)(b + (precision == DL_PREC_F32 ? oSh : oTmp)) : nullptr;
+        chunks->sh_dst = (M && precision != DL_PREC_F32) ? (uint16_t*)(b + oSh) : nullptr;
+        chunks->sh_M = M;
+        chunks->sh_P = (int)P16;
+        chunks->sh_kind = precision;
         for (int k = 0; k <= kUploadChunks; k++) chunks->bounds[k] = (uint32_t)(n * (uint64_t)k / kUploadChunks);
         chunks->issue = [=]() -> int {
             for (int k = 0; k < kUploadChunks; k++) {
@@ -187,21 +203,19 @@ int dl_upload_scene(dl_scene* s, const dl_splats* d, int precision, cudaStream_t
             if (M) {
                 // in the same ranges: copies issued later on other streams (a
                 // frame's view tables) queue behind one copy at most.  The
-                // copies run back to back; the 16-bit conversion of all splats
-                // follows them in one launch (a conversion between two copies
-                // would hold the next copy until it has run beside the frame)
+                // copies run back to back, each chunk followed by its event; the
+                // frame converts a chunk to 16 bits on its own stream (a
+                // conversion between two copies here would hold the next copy
+                // until it has run beside the frame's kernels)
                 for (int k = 0; k < kUploadChunks; k++) {
                     const uint64_t g0 = chunks->bounds[k], g1 = chunks->bounds[k + 1];
-                    if (g1 == g0) continue;
-                    const uint64_t e = 12ull * M;
-                    DL_CK(cudaMemcpyAsync(b + (precision == DL_PREC_F32 ? oSh : oTmp) + e * g0,
-                                          (const char*)d->colors_sh + e * g0, e * (g1 - g0),
-                                          cudaMemcpyHostToDevice, st));
-                }
-                if (precision != DL_PREC_F32) {
-                    sh_to_half_k<<<1024, 256, 0, st>>>((const float*)(b + oTmp), (uint16_t*)(b + oSh), n, M,
-                                                       (int)P16, precision);
-                    DL_CK(cudaGetLastError());
+                    if (g1 > g0) {
+                        const uint64_t e = 12ull * M;
+                        DL_CK(cudaMemcpyAsync(b + (precision == DL_PREC_F32 ? oSh : oTmp) + e * g0,
+                                              (const char*)d->colors_sh + e * g0, e * (g1 - g0),
+                                              cudaMemcpyHostToDevice, st));
+                    }
+                    DL_CK(cudaEventRecord(chunks->sh_events[k], st));
                 }
                 DL_CK(cudaEventRecord(chunks->sh_event, st));
             }
@@ -260,7 +274,7 @@ struct FramePtrs {
     const DlUploadChunks* upload;
     uint32_t* visMask;             // colours deferred until the SH has arrived (upload->sh_event)
     cudaStream_t colStream;        // with visMask: colour_k runs there, beside the sorts and binning
-    cudaEvent_t colEv[2];          // [0] projection done (on the frame's stream), [1] colours done
+    const cudaEvent_t* colEv;      // [c] splat range c projected (frame's stream), [upload->count] colours done
     // host outputs read back per view range while the next range rasterizes
     int rbGroups;                  // 0: one rasterizer launch, no read-back here
     uint8_t* const* rbHost;        // [V] host destinations
@@ -450,6 +464,7 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
                 (*launches)++;
                 DL_CK(cudaGetLastError());
             }
+            if (f.visMask) DL_CK(cudaEventRecord(f.colEv[k], st));
         }
     } else if (d.N) {
         if (d.fastExp) dlr::project_k<true><<<(d.N + 255) / 256, 256, 0, st>>>(pa);
@@ -457,12 +472,12 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
         (*launches)++;
     }
     DL_CK(cudaGetLastError());
-    // deferred colours, once the SH has arrived, on a stream of their own: they
-    // run while the frame's stream sorts and bins; the rasterizer waits for them
+    // deferred colours on a stream of their own, splat range by splat range as
+    // each range is projected and its SH has arrived (converted to 16 bits
+    // there first): they run beside the rest of the upload, the projection and
+    // the sorts; the rasterizer waits for them
     if (f.visMask && d.N) {
-        DL_CK(cudaEventRecord(f.colEv[0], st));
-        DL_CK(cudaStreamWaitEvent(f.colStream, f.colEv[0], 0));
-        DL_CK(cudaStreamWaitEvent(f.colStream, f.upload->sh_event, 0));
+        const DlUploadChunks& up = *f.upload;
         dlr::ColourArgs ca;
         ca.sc = sc;
         ca.views = f.views;
@@ -471,11 +486,20 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
         ca.vis_mask = f.visMask;
         ca.recBC = d.f16rec ? nullptr : f.recBC;
         ca.recH = d.f16rec ? f.recH : nullptr;
-        if (d.fastExp) dlr::colour_k<true><<<(d.N + 255) / 256, 256, 0, f.colStream>>>(ca);
-        else dlr::colour_k<false><<<(d.N + 255) / 256, 256, 0, f.colStream>>>(ca);
-        (*launches)++;
-        DL_CK(cudaGetLastError());
-        DL_CK(cudaEventRecord(f.colEv[1], f.colStream));
+        for (int k = 0; k < up.count; k++) {
+            const uint32_t g0 = up.bounds[k], g1 = up.bounds[k + 1];
+            DL_CK(cudaStreamWaitEvent(f.colStream, f.colEv[k], 0));
+            DL_CK(cudaStreamWaitEvent(f.colStream, up.sh_events[k], 0));
+            if (g1 == g0) continue;
+            DL_TRY(dl_upload_convert_sh(&up, g0, g1, f.colStream, launches));
+            ca.g_begin = g0;
+            ca.g_end = g1;
+            if (d.fastExp) dlr::colour_k<true><<<(g1 - g0 + 255) / 256, 256, 0, f.colStream>>>(ca);
+            else dlr::colour_k<false><<<(g1 - g0 + 255) / 256, 256, 0, f.colStream>>>(ca);
+            (*launches)++;
+            DL_CK(cudaGetLastError());
+        }
+        DL_CK(cudaEventRecord(f.colEv[up.count], f.colStream));
     }
     rec_event(ev, 1, st);
     // depth sort: stable LSD, 4 x 8-bit digits, one segment per view
@@ -622,7 +646,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     DL_CK(cudaGetLastError());
 
     // the deferred colours (launched after the projection) are complete
-    if (f.visMask && d.N) DL_CK(cudaStreamWaitEvent(st, f.colEv[1], 0));
+    if (f.visMask && d.N) DL_CK(cudaStreamWaitEvent(st, f.colEv[f.upload->count], 0));
 
     // learned schedule: per-tile features, predicted cost, tiles in decreasing order
     const uint32_t* work = f.work;
@@ -903,8 +927,7 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
             for (auto& e : r->colour_ev)
                 if (!e) DL_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             f.colStream = r->colour_stream;
-            f.colEv[0] = r->colour_ev[0];
-            f.colEv[1] = r->colour_ev[1];
+            f.colEv = r->colour_ev;
         }
         if (overlap->groups > 1 && V > 1) {
             rbTileBase.assign(hTileBase, hTileBase + V + 1);

@@ -572,6 +572,7 @@ struct ColourArgs {
     const uint32_t* vis_mask;
     float4* recBC;
     uint4* recH;
+    uint32_t g_begin, g_end;       // the splat range coloured by this launch
 };
 
 template <bool kFma>
@@ -586,8 +587,8 @@ __global__ void __launch_bounds__(256) colour_k(ColourArgs a) {
     }
     __syncthreads();
     const DlView* vtab = staged ? s_views : a.views;
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= a.sc.n) return;
+    const uint32_t g = a.g_begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.g_end) return;
     const int M = a.sc.bands == 0 ? 0 : a.sc.bands == 1 ? 3 : a.sc.bands == 2 ? 8 : 15;
     float pos[3], dc[3];
     pos[0] = __ldg(a.sc.pos + 3ull * g); pos[1] = __ldg(a.sc.pos + 3ull * g + 1); pos[2] = __ldg(a.sc.pos + 3ull * g + 2);

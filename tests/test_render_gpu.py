@@ -279,7 +279,7 @@ def test_other_binning_tiles_keep_the_coverage_truncation(device):
 
 
 def test_render_many_groups_and_sh16_match_the_batch(device):
-    # host outputs of 8+ views: the scene uploads in four splat ranges, each
+    # host outputs of 8+ views: the scene uploads in eight splat ranges, each
     # projected when it has arrived, and the rasterizer runs per view range with
     # overlapped read-back; DL_BATCH_SH16 keeps the uploaded SH in f16 like a
     # Scene uploaded as "f16".  The splat count is not a multiple of 4.
@@ -304,6 +304,15 @@ def test_render_many_groups_and_sh16_match_the_batch(device):
     got = r2.render_many(d, cams, flags=fl | _lib.DL_BATCH_SH16)
     for a, b in zip(ref16, got):
         assert np.array_equal(a, b)
+    # fewer splats than upload ranges: empty ranges are skipped
+    tiny = synth.cluster_scene(5, seed=18, clusters=2, extent=1.0, bands=3)
+    cams8 = synth.ring_cameras(8, radius=4.0, resolutions=[(160, 96)])
+    st = r2.upload(tiny, "f16")
+    ref = r2.render_batch(st, cams8[:4], flags=fl) + r2.render_batch(st, cams8[4:], flags=fl)
+    got = r2.render_many(tiny, cams8, flags=fl | _lib.DL_BATCH_SH16)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+    assert any(np.asarray(a).reshape(-1, 4)[:, 3].any() for a in ref)
 
 
 @pytest.mark.parametrize("op_mu", [0.0, -3.0])
