@@ -148,8 +148,10 @@ __device__ __forceinline__ void eval_sh(const DlSceneDev& sc, uint64_t base, int
 }
 
 // evalSH on the 16-bit SH block of one Gaussian (same basis, same summation
-// order as eval_sh): the block is read with 128-bit loads.
-template <int BANDS, bool kFma>
+// order as eval_sh): the block is read with 128-bit loads.  kHalf: FP16
+// coefficients, else BF16 (a compile-time choice, so that each coefficient
+// costs one conversion and no select).
+template <int BANDS, bool kFma, bool kHalf>
 __device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, float x, float y, float z,
                                           float& r, float& gr, float& b) {
     constexpr int M = BANDS == 1 ? 3 : BANDS == 2 ? 8 : 15;
@@ -161,11 +163,11 @@ __device__ __forceinline__ void eval_sh16(const DlSceneDev& sc, uint32_t g, floa
         const uint4 q = __ldg(blk + c);
         w[4 * c] = q.x; w[4 * c + 1] = q.y; w[4 * c + 2] = q.z; w[4 * c + 3] = q.w;
     }
-    const bool isHalf = sc.sh_kind == 1;
     auto coef = [&](int k, int ch) -> float {
         const int e = 3 * k + ch;
-        const uint16_t bits = (uint16_t)(w[e >> 1] >> ((e & 1) * 16));
-        return isHalf ? __half2float(__ushort_as_half(bits)) : __bfloat162float(__ushort_as_bfloat16(bits));
+        const uint32_t word = w[e >> 1];
+        if (kHalf) return __half2float(__ushort_as_half((uint16_t)(word >> ((e & 1) * 16))));
+        return __uint_as_float((e & 1) ? (word & 0xffff0000u) : (word << 16));   // BF16: the high half of an f32
     };
     const float SH1 = 0.4886025119029199f, nSH1 = -0.4886025119029199f;
     const float b1[3] = {nSH1 * y, SH1 * z, nSH1 * x};
@@ -239,10 +241,14 @@ __device__ __forceinline__ void splat_colour(const DlSceneDev& sc, uint32_t g, i
                                            : (pcx * pcx + pcy * pcy) + pcz * pcz);
         float sr, sg, sb;
         const float dxn = pdiv<kFma>(pcx, len), dyn = pdiv<kFma>(pcy, len), dzn = pdiv<kFma>(pcz, len);
-        if (sc.sh16) {
-            if (sc.bands == 1) eval_sh16<1, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
-            else if (sc.bands == 2) eval_sh16<2, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
-            else eval_sh16<3, kFma>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+        if (sc.sh16 && sc.sh_kind == 1) {
+            if (sc.bands == 1) eval_sh16<1, kFma, true>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else if (sc.bands == 2) eval_sh16<2, kFma, true>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else eval_sh16<3, kFma, true>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+        } else if (sc.sh16) {
+            if (sc.bands == 1) eval_sh16<1, kFma, false>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else if (sc.bands == 2) eval_sh16<2, kFma, false>(sc, g, dxn, dyn, dzn, sr, sg, sb);
+            else eval_sh16<3, kFma, false>(sc, g, dxn, dyn, dzn, sr, sg, sb);
         } else {
             eval_sh<kFma>(sc, (uint64_t)g * 3 * M, M, dxn, dyn, dzn, sr, sg, sb);
         }
