@@ -31,6 +31,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -106,19 +107,62 @@ def config(args, cams, extra=None, data=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    polled every 10 ms from a thread (the GPU found by the CUDA device's UUID),
+    or nvidia-smi at 100 ms where NVML is unavailable.  Read-only: no setting
+    of the GPU is touched."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.f = None
         self.p = None
+        self.nv = None
+        self.sm, self.mx, self.reasons = [], None, set()
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.idx).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+        return pynvml, h
+
+    def _poll(self):
+        nv, h = self.nv
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        while not self.stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                self.mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for n, b in zip(self.NAMES, bits):
+                    if r & b:
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            self.stop.wait(0.01)
 
     def __enter__(self):
         try:
+            self.nv = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nv = None
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
@@ -128,6 +172,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.p:
             self.p.terminate()
             try:
@@ -136,25 +183,27 @@ class ClockSampler:
                 self.p.kill()
 
     def summary(self):
-        self.f.flush()
-        self.f.seek(0)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f.read().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        os.unlink(self.f.name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.f is not None:
+            self.f.flush()
+            self.f.seek(0)
+            for line in self.f.read().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    self.sm.append(float(parts[1]))
+                    self.mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(self.NAMES, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        self.reasons.add(n)
+            os.unlink(self.f.name)
+            self.f = None
+        sm = self.sm
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.mx,
+                "reasons": sorted(self.reasons), "samples": len(sm),
+                "source": "nvml, 10 ms" if self.nv else "nvidia-smi, 100 ms"}
 
 
 def peaks():
