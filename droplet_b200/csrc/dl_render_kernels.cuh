@@ -672,6 +672,7 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
     __shared__ unsigned long long s_prefix;
     __shared__ uint32_t s_skip;
     __shared__ uint32_t s_dh[4 * 256];
+    __shared__ uint32_t s_own[kEmitThreads / 32][32];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // after a timed-out depth sort the sorted indices may hold unwritten slots
@@ -779,13 +780,52 @@ __global__ void __launch_bounds__(kEmitThreads, 8) emit_k(EmitArgs a) {
     if (s_skip) return;
     const uint64_t outBase = a.pair_base[v] + s_prefix;
     const uint32_t dmask = (1u << a.bits) - 1u;
-    for (uint32_t o = tid; o < total; o += kEmitThreads) {
-        // last rank slot whose exclusive offset is <= o
-        uint32_t lo = 0, hi = kEmitRanks;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_excl[mid] <= o) lo = mid; else hi = mid;
+    // Each warp walks a contiguous share of the CTA's pairs, 32 at a time.  A
+    // pair o belongs to the last rank slot whose exclusive offset is <= o: one
+    // binary search finds the slot of the warp's first pair, then each window
+    // of 32 pairs takes its slots from the 32 slots after the previous one —
+    // each marks the window position where it starts (the last of equal
+    // starts: slots without pairs are passed over) and a max-scan over the
+    // lanes counts the slots starting at or before each pair (another 32 slots
+    // when all of them do).
+    constexpr uint32_t kEmitWarps = kEmitThreads / 32;
+    const uint32_t per = ((total + kEmitWarps - 1u) / kEmitWarps + 31u) & ~31u;
+    const uint32_t wb = min(total, (uint32_t)warp * per), we = min(total, wb + per);
+    uint32_t* own = s_own[warp];
+    uint32_t base = 0;
+    if (wb < we) {
+        uint32_t hi = kEmitRanks;
+        while (hi - base > 1) {
+            const uint32_t mid = (base + hi) >> 1;
+            if (s_excl[mid] <= wb) base = mid; else hi = mid;
         }
+    }
+    for (uint32_t o0 = wb; o0 < we; o0 += 32u) {
+        const uint32_t o = o0 + (uint32_t)lane;
+        uint32_t lo = base, b = base;
+        bool resolved = false;
+        while (true) {
+            own[lane] = 0u;
+            __syncwarp();
+            // slot b + 1 + lane starts at o0 + q (q >= 0: slot b ends at or after o0)
+            const uint32_t idx = b + 1u + (uint32_t)lane;
+            const uint32_t q = idx <= (uint32_t)kEmitRanks ? s_excl[idx] - o0 : 0xffffffffu;
+            const uint32_t qn = __shfl_down_sync(0xffffffffu, q, 1);
+            if (q < 32u && (lane == 31 || qn != q)) own[q] = (uint32_t)lane + 1u;
+            __syncwarp();
+            uint32_t m = own[lane];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, m, d);
+                if (lane >= d) m = max(m, t);
+            }
+            if (!resolved && m < 32u) { lo = b + m; resolved = true; }
+            if (!__any_sync(0xffffffffu, o < we && !resolved)) break;
+            b += 32u;
+            __syncwarp();                                   // own[] is cleared next
+        }
+        base = __shfl_sync(0xffffffffu, lo, 31);
+        if (o >= we) continue;
         const uint32_t w = o - s_excl[lo];
         const uint32_t span = s_span[lo];
         const uint32_t mn = s_min[lo];

@@ -527,7 +527,6 @@ struct EvalArgs {
     const uint32_t* nblocks;
     uint2* masks;
     uint32_t* counter;
-    unsigned long long* evals;
     const uint32_t* work;          // optional block order (learned); NULL: block order
     uint32_t* cycles;              // optional [block] SM cycles / 16 spent on the block
     const uint32_t* err;           // DL_DEVERR_TIMEOUT: the block lists are not complete
@@ -574,7 +573,6 @@ __global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
     // linear bit index = z*16 + y*4 + x (shaders/voxelize.ts:137)
     const uint32_t lx = tid & 3, ly = (tid >> 2) & 3, lz = tid >> 4;
     const int64_t NX = a.p.NB[0], NY = a.p.NB[1], NBX = a.p.NBB[0], NBY = a.p.NBB[1];
-    uint64_t evals = 0;
     while (true) {
         if (tid == 0) {
             const uint32_t k = atomicAdd(a.counter, 1u);
@@ -607,7 +605,6 @@ __global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
             if (sigma < 7.0f) {
                 for (uint32_t j = 0; j < m; j++) {
                     sigma = sigma + eval_gaussian<kFast>(vc, a.p.half, s_g[j]);
-                    evals++;
                     if (sigma >= 7.0f) break;
                 }
             }
@@ -622,9 +619,6 @@ __global__ void __launch_bounds__(64, 32) vox_eval_k(EvalArgs a) {
             a.masks[b] = make_uint2(s_mask[0], s_mask[1]);
             if (a.cycles) a.cycles[b] = (uint32_t)((clock64() - t0) >> 4);
         }
-    }
-    if (a.evals) {
-        if (evals) atomicAdd(a.evals, (unsigned long long)evals);
     }
 }
 
@@ -1210,7 +1204,7 @@ extern "C" int dl_voxelize(dl_device* dev, const dl_splats* data, const dl_vox_o
         EvalArgs va;
         va.p = p; va.rec = B.rec.as<VoxRec>(); va.vals = valsF; va.bkey = B.bkey.as<uint32_t>();
         va.bstart = B.bstart.as<uint32_t>(); va.nblocks = scr + VS_NBLK; va.masks = B.masks.as<uint2>();
-        va.counter = scr + VS_EVAL; va.evals = nullptr;
+        va.counter = scr + VS_EVAL;
         va.work = work; va.cycles = logBlocks ? B.scycles.as<uint32_t>() : nullptr; va.err = scr + VS_ERR;
         if (fastExp) vox_eval_k<true><<<dev->sm_count * 32, 64, 0, st>>>(va);
         else vox_eval_k<false><<<dev->sm_count * 32, 64, 0, st>>>(va);
