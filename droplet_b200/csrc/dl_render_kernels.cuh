@@ -1771,12 +1771,16 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_x2_k(RasterA
         const float pad = a.stage_pad;
         float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
         bool done = !inImage;
+        // the thread's pair value of the next batch is loaded while this batch
+        // is composited (one dependent load fewer before the staging barrier)
+        uint32_t gNext = start + (uint32_t)tid < end ? __ldg(vals + start + tid) : 0u;
         for (uint32_t b = start; b < end; b += kTileStage) {
             // ---- stage one pair per thread
             uint32_t mask = 0;
             const uint32_t e = b + (uint32_t)tid;
+            const uint32_t g = gNext;
+            if (e + kTileStage < end) gNext = __ldg(vals + e + kTileStage);
             if (e < end) {
-                const uint32_t g = __ldg(vals + e);
                 if (!(g & kPhantomBit)) {
                     const float4 ra = __ldg(a.recA + vo + g);
                     float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
@@ -1917,12 +1921,16 @@ __global__ void __launch_bounds__(kRasterThreads, 5) rasterize_tile_k(RasterArgs
         const float pad = a.stage_pad;
         float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, T = 1.0f;
         bool done = !inImage;
+        // the thread's pair value of the next batch is loaded while this batch
+        // is composited (one dependent load fewer before the staging barrier)
+        uint32_t gNext = start + (uint32_t)tid < end ? __ldg(vals + start + tid) : 0u;
         for (uint32_t b = start; b < end; b += kTileStage) {
             // ---- stage one pair per thread
             uint32_t mask = 0;
             const uint32_t e = b + (uint32_t)tid;
+            const uint32_t g = gNext;
+            if (e + kTileStage < end) gNext = __ldg(vals + e + kTileStage);
             if (e < end) {
-                const uint32_t g = __ldg(vals + e);
                 if (!(g & kPhantomBit)) {
                     const float4 ra = __ldg(a.recA + vo + g);
                     float ex = ra.z, ey = a.rec_box ? ra.w : ra.z;
