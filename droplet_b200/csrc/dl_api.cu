@@ -110,8 +110,6 @@ extern "C" int dl_renderer_destroy(dl_renderer* r) {
     r->tuneOut.release();
     if (r->copy_stream) { cudaStreamSynchronize(r->copy_stream); cudaStreamDestroy(r->copy_stream); }
     if (r->copy_event) cudaEventDestroy(r->copy_event);
-    if (r->colour_stream) { cudaStreamSynchronize(r->colour_stream); cudaStreamDestroy(r->colour_stream); }
-    for (auto& e : r->colour_ev) if (e) cudaEventDestroy(e);
     if (r->raster_stream) { cudaStreamSynchronize(r->raster_stream); cudaStreamDestroy(r->raster_stream); }
     for (auto& e : r->raster_ev) if (e) cudaEventDestroy(e);
     for (auto& e : r->upload_events) if (e) cudaEventDestroy(e);

@@ -167,9 +167,6 @@ struct dl_renderer {
     // read-back of host-output batches, overlapped with rendering
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_event = nullptr;
-    // deferred colours run beside the sorts: their stream and events (projected, coloured)
-    cudaStream_t colour_stream = nullptr;
-    cudaEvent_t colour_ev[kUploadChunks + 1] = {};      // [c] splat range c projected, [last] colours done
     // host-output frames: the odd rasterizer view ranges run on a second stream
     cudaStream_t raster_stream = nullptr;
     cudaEvent_t raster_ev[2] = {nullptr, nullptr};

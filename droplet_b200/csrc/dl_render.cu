@@ -272,9 +272,7 @@ struct FramePtrs {
     uint32_t* tileCycles;
     // a scene upload still in flight: projection per splat range after its event
     const DlUploadChunks* upload;
-    uint32_t* visMask;             // colours deferred until the SH has arrived (upload->sh_event)
-    cudaStream_t colStream;        // with visMask: colour_k runs there, beside the sorts and binning
-    const cudaEvent_t* colEv;      // [c] splat range c projected (frame's stream), [upload->count] colours done
+    uint32_t* visMask;             // colours deferred until each SH range has arrived (upload->sh_events)
     // host outputs read back per view range while the next range rasterizes
     int rbGroups;                  // 0: one rasterizer launch, no read-back here
     uint8_t* const* rbHost;        // [V] host destinations
@@ -434,6 +432,37 @@ inline void rec_event(cudaEvent_t* ev, int i, cudaStream_t st) {
 
 // project + depth sort.  Expects views, segment tables, nvis and scratch words
 // already uploaded / cleared on the stream.
+// Deferred colours of upload ranges [k0, k1) on the frame's stream, each once
+// its SH range has arrived (converted to 16 bits first).  The frame launches
+// them between its later stages, so that they neither wait behind persistent
+// kernels that hold every SM nor hold back the rasterizer.
+int launch_colours(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cudaStream_t st, int k0, int k1,
+                   uint64_t* launches) {
+    if (!f.visMask || !d.N) return DL_OK;
+    const DlUploadChunks& up = *f.upload;
+    dlr::ColourArgs ca;
+    ca.sc = sc;
+    ca.views = f.views;
+    ca.num_views = d.V;
+    ca.view_stride = d.stride;
+    ca.vis_mask = f.visMask;
+    ca.recBC = d.f16rec ? nullptr : f.recBC;
+    ca.recH = d.f16rec ? f.recH : nullptr;
+    for (int k = std::max(k0, 0); k < std::min(k1, up.count); k++) {
+        const uint32_t g0 = up.bounds[k], g1 = up.bounds[k + 1];
+        DL_CK(cudaStreamWaitEvent(st, up.sh_events[k], 0));
+        if (g1 == g0) continue;
+        DL_TRY(dl_upload_convert_sh(&up, g0, g1, st, launches));
+        ca.g_begin = g0;
+        ca.g_end = g1;
+        if (d.fastExp) dlr::colour_k<true><<<(g1 - g0 + 255) / 256, 256, 0, st>>>(ca);
+        else dlr::colour_k<false><<<(g1 - g0 + 255) / 256, 256, 0, st>>>(ca);
+        (*launches)++;
+        DL_CK(cudaGetLastError());
+    }
+    return DL_OK;
+}
+
 int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cudaStream_t st, cudaEvent_t* ev,
                  uint64_t* launches) {
     rec_event(ev, 0, st);
@@ -464,7 +493,6 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
                 (*launches)++;
                 DL_CK(cudaGetLastError());
             }
-            if (f.visMask) DL_CK(cudaEventRecord(f.colEv[k], st));
         }
     } else if (d.N) {
         if (d.fastExp) dlr::project_k<true><<<(d.N + 255) / 256, 256, 0, st>>>(pa);
@@ -472,35 +500,6 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
         (*launches)++;
     }
     DL_CK(cudaGetLastError());
-    // deferred colours on a stream of their own, splat range by splat range as
-    // each range is projected and its SH has arrived (converted to 16 bits
-    // there first): they run beside the rest of the upload, the projection and
-    // the sorts; the rasterizer waits for them
-    if (f.visMask && d.N) {
-        const DlUploadChunks& up = *f.upload;
-        dlr::ColourArgs ca;
-        ca.sc = sc;
-        ca.views = f.views;
-        ca.num_views = d.V;
-        ca.view_stride = d.stride;
-        ca.vis_mask = f.visMask;
-        ca.recBC = d.f16rec ? nullptr : f.recBC;
-        ca.recH = d.f16rec ? f.recH : nullptr;
-        for (int k = 0; k < up.count; k++) {
-            const uint32_t g0 = up.bounds[k], g1 = up.bounds[k + 1];
-            DL_CK(cudaStreamWaitEvent(f.colStream, f.colEv[k], 0));
-            DL_CK(cudaStreamWaitEvent(f.colStream, up.sh_events[k], 0));
-            if (g1 == g0) continue;
-            DL_TRY(dl_upload_convert_sh(&up, g0, g1, f.colStream, launches));
-            ca.g_begin = g0;
-            ca.g_end = g1;
-            if (d.fastExp) dlr::colour_k<true><<<(g1 - g0 + 255) / 256, 256, 0, f.colStream>>>(ca);
-            else dlr::colour_k<false><<<(g1 - g0 + 255) / 256, 256, 0, f.colStream>>>(ca);
-            (*launches)++;
-            DL_CK(cudaGetLastError());
-        }
-        DL_CK(cudaEventRecord(f.colEv[up.count], f.colStream));
-    }
     rec_event(ev, 1, st);
     // depth sort: stable LSD, 4 x 8-bit digits, one segment per view
     if (d.N) {
@@ -537,6 +536,9 @@ int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, c
         }
         DL_CK(cudaGetLastError());
     }
+    // deferred colours: the first half of the upload ranges (their SH has
+    // arrived by the end of the depth sort on the headline batch)
+    if (f.visMask) DL_TRY(launch_colours(f, d, sc, st, 0, f.upload->count / 2, launches));
     rec_event(ev, 2, st);
     // after 4 passes keys0 / vals0 hold the sorted keys / splat indices
     return DL_OK;
@@ -575,6 +577,11 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     dlr::emit_k<<<d.V * d.emitTilesPerView, dlr::kEmitThreads, 0, st>>>(ea);
     (*launches)++;
     DL_CK(cudaGetLastError());
+    // deferred colours: the next three eighths of the upload ranges after the
+    // emission, the rest after the first pair-sort pass
+    const int colMid = f.visMask ? f.upload->count / 2 : 0;
+    const int colLate = f.visMask ? f.upload->count * 7 / 8 : 0;
+    if (f.visMask) DL_TRY(launch_colours(f, d, sc, st, colMid, colLate, launches));
     rec_event(ev, 4, st);
 
     dlr::PairDigitArgs pd;
@@ -621,6 +628,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
             if (p == 0) sp.withhold_tile = g_dl_wait.withheld(DL_WAIT_STAGE_PAIR_SORT);
             launch_pass_bits(d.pbits, sp, d.pairGrid, st, bd);
             (*launches)++;
+            if (p == 0 && f.visMask) DL_TRY(launch_colours(f, d, sc, st, colLate, f.upload->count, launches));
             std::swap(kin, kout);
             std::swap(vin, vout);
         }
@@ -645,8 +653,7 @@ int launch_back(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cu
     (*launches)++;
     DL_CK(cudaGetLastError());
 
-    // the deferred colours (launched after the projection) are complete
-    if (f.visMask && d.N) DL_CK(cudaStreamWaitEvent(st, f.colEv[f.upload->count], 0));
+    if (d.ppasses == 0 && f.visMask) DL_TRY(launch_colours(f, d, sc, st, colLate, f.upload->count, launches));
 
     // learned schedule: per-tile features, predicted cost, tiles in decreasing order
     const uint32_t* work = f.work;
@@ -923,11 +930,6 @@ int dl_render_views(dl_renderer* r, const DlSceneDev& sc, const DlView* hv, uint
         if (f.upload && f.upload->sh_separate) {
             DL_TRY(r->visMask.ensure(4ull * ((V + 31) / 32) * std::max<uint32_t>(N, 1)));
             f.visMask = r->visMask.as<uint32_t>();
-            if (!r->colour_stream) DL_CK(cudaStreamCreateWithFlags(&r->colour_stream, cudaStreamNonBlocking));
-            for (auto& e : r->colour_ev)
-                if (!e) DL_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-            f.colStream = r->colour_stream;
-            f.colEv = r->colour_ev;
         }
         if (overlap->groups > 1 && V > 1) {
             rbTileBase.assign(hTileBase, hTileBase + V + 1);
