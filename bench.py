@@ -423,7 +423,9 @@ def run_ours(args, rank, world, local_rank):
     # autotuner (untimed): pair-sort digit width, raster work-item shape, CTAs/SM
     if args.no_tune and (args.raster_shape or args.pair_sort_bits):
         r.set_tuning(raster_shape=args.raster_shape or "tile-f32x2", pair_sort_bits=args.pair_sort_bits or 8)
-    tuning = None if args.no_tune else r.autotune(scene, cams, flags=FAST, reps=2)
+    # five frames per candidate: 7- and 8-bit pair-sort digits are within a few
+    # percent of each other on this batch, closer than two frames' noise
+    tuning = None if args.no_tune else r.autotune(scene, cams, flags=FAST, reps=5)
 
     # the headline: tiles rasterized in the static (tile index) order, which
     # the learned cost order does not beat on this GPU; the learned arm is
