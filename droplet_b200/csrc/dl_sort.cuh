@@ -94,14 +94,21 @@ __global__ void __launch_bounds__(kThreads) hist_k(const uint32_t* __restrict__ 
         const uint32_t lt = tile - s.tile_base[seg];
         const uint32_t len = s.len[seg];
         const uint64_t base = s.start[seg];
+        // all of the thread's keys are loaded before the first count, so that
+        // the loads are in flight together rather than one per shared atomic
+        uint32_t kk[kItems];
+#pragma unroll
         for (int j = 0; j < kItems; j++) {
             const uint32_t e = lt * kTile + j * kThreads + threadIdx.x;
-            if (e < len) {
-                const uint32_t k = keys[base + e];
-                if (drop_max && k == 0xffffffffu) continue;
-                for (int p = 0; p < passes; p++)
-                    atomicAdd(&sh[p * RADIX + ((k >> (first_shift + p * BITS)) & (RADIX - 1))], 1u);
-            }
+            kk[j] = e < len ? __ldg(keys + base + e) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kItems; j++) {
+            const uint32_t e = lt * kTile + j * kThreads + threadIdx.x;
+            const uint32_t k = kk[j];
+            if (e >= len || (drop_max && k == 0xffffffffu)) continue;
+            for (int p = 0; p < passes; p++)
+                atomicAdd(&sh[p * RADIX + ((k >> (first_shift + p * BITS)) & (RADIX - 1))], 1u);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < passes * RADIX; i += kThreads)
