@@ -1,4 +1,5 @@
-// dl_query.cu — point occupancy against a sparse block-mask buffer, on the device.
+// dl_query.cu — point occupancy against a sparse block-mask buffer, and one
+// buffer carved out of another, on the device.
 //
 // A downstream stage of the voxelizer (collision tests against its output), with
 // no counterpart in the reference, whose BlockMaskBuffer answers one block at a

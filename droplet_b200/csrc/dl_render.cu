@@ -430,8 +430,6 @@ inline void rec_event(cudaEvent_t* ev, int i, cudaStream_t st) {
     if (ev) cudaEventRecord(ev[i], st);
 }
 
-// project + depth sort.  Expects views, segment tables, nvis and scratch words
-// already uploaded / cleared on the stream.
 // Deferred colours of upload ranges [k0, k1) on the frame's stream, each once
 // its SH range has arrived (converted to 16 bits first).  The frame launches
 // them between its later stages, so that they neither wait behind persistent
@@ -463,6 +461,8 @@ int launch_colours(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc,
     return DL_OK;
 }
 
+// project + depth sort.  Expects views, segment tables, nvis and scratch words
+// already uploaded / cleared on the stream.
 int launch_front(const FramePtrs& f, const FrameDims& d, const DlSceneDev& sc, cudaStream_t st, cudaEvent_t* ev,
                  uint64_t* launches) {
     rec_event(ev, 0, st);
