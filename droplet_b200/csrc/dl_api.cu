@@ -302,8 +302,24 @@ int render_batch(dl_renderer* r, dl_scene* s, const dl_camera* cams, int n, cons
         // ranges; each range is copied back on a second stream while the next
         // rasterizes
         DL_TRY(ensure_copy_stream(r));
-        const DlOverlap ov = {kReadBackGroups, outs, r->copy_stream, r->copy_event, upload};
-        const int rc = dl_render_views(r, s->d, views.data(), (uint32_t)n, dOuts.data(), flags, &ov);
+        // the frame takes the views largest first, so that the last range,
+        // whose read-back nothing overlaps, holds the smallest images (each
+        // view is rendered on its own: the order changes no pixel)
+        std::vector<int> ord((size_t)n);
+        for (int i = 0; i < n; i++) ord[i] = i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+            return (uint64_t)views[x].W * views[x].H > (uint64_t)views[y].W * views[y].H;
+        });
+        std::vector<DlView> pv((size_t)n);
+        std::vector<uint32_t*> pdOuts((size_t)n);
+        std::vector<uint8_t*> pOuts((size_t)n);
+        for (int i = 0; i < n; i++) {
+            pv[i] = views[ord[i]];
+            pdOuts[i] = dOuts[ord[i]];
+            pOuts[i] = outs[ord[i]];
+        }
+        const DlOverlap ov = {kReadBackGroups, pOuts.data(), r->copy_stream, r->copy_event, upload};
+        const int rc = dl_render_views(r, s->d, pv.data(), (uint32_t)n, pdOuts.data(), flags, &ov);
         const cudaError_t ce = cudaStreamSynchronize(r->copy_stream);
         if (rc != DL_OK) return rc;
         DL_CK(ce);
