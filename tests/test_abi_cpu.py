@@ -1,6 +1,7 @@
 """CPU tests of the C-ABI boundary: the library loads, exports every function
 include/droplet_b200.h declares, and reports errors as the reference would
 (a status + message, raised as an exception by the host API)."""
+import ctypes
 import os
 import re
 
@@ -42,6 +43,14 @@ def test_null_arguments_are_rejected_without_a_device():
     assert L.dl_render(None, None, None, None, None, 0) == _lib.DL_E_INVALID_ARG
     assert "NULL" in L.dl_last_error().decode()
     assert L.dl_voxelize(None, None, None, None) == _lib.DL_E_INVALID_ARG
+    # the block-mask buffer stages refuse a missing device before any device work
+    bmin, dims = (ctypes.c_double * 3)(0.0, 0.0, 0.0), (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    assert L.dl_vox_query(None, None, None, None, 0, bmin, 0.1, dims, None, 0, None) == _lib.DL_E_INVALID_ARG
+    assert "dl_vox_query" in L.dl_last_error().decode()
+    n = ctypes.c_uint64(7)
+    assert L.dl_vox_carve(None, None, None, None, 0, None, None, None, 0, None, None, None,
+                          ctypes.byref(n)) == _lib.DL_E_INVALID_ARG
+    assert "dl_vox_carve" in L.dl_last_error().decode()
 
 
 def test_splatdata_validates_lengths():
